@@ -1,0 +1,360 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 query-execution core.
+
+Default workload: the pricing-summary scan (60,000,000 rows in 2^20-row segments; filter + dense
+GROUP BY over 2 one-byte dictionary-coded flags; exact int128 sums of price and price expressions),
+the configuration the headline metric is quoted on.  One step = one query: build the aggregator,
+add the 58 segment batches, one fused scan kernel, compaction and download of the 6 groups.
+
+  value   device-timed throughput (G rows/s) with the table resident in HBM (2.28 GB of inputs, far
+          larger than the 126 MB L2, so no flush between steps is needed)
+  e2e     the same query through the C ABI from pinned host buffers: every step copies the segment
+          columns host -> device and reads the groups back
+  roofline  the scan kernel's algorithmic bytes (38 B/row) per launch / its CUDA-event duration
+  cpu_baseline  the CPU oracle (C++ restatement, all host threads) on a bounded sample
+
+`--impl reference` times the reference's CPU path: the reference has no CPU implementation of these
+operators, so the CPU oracle port stands in (kind "port").
+Multi-GPU (torchrun): every rank runs its own replica of the workload (the operators do not shard a
+query across GPUs); value = rows of all ranks / max step time over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAK_FALLBACK_GBS = 6650.0
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return PEAK_FALLBACK_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = [l.split(",") for l in open(self.f.name).read().strip().splitlines() if l.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                for i, nm in enumerate(names):
+                    if r[5 + i].strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(n_gpus: int):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def reduce_max(x: float, ws: int) -> float:
+    if ws <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws: int):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ------------------------------------------------------------------ CPU baseline (oracle)
+def cpu_oracle_rate(table, env, plan, budget_s: float, max_segments: int = 8):
+    """Rows/s of the oracle over the first segments of the table, repeated for about budget_s."""
+    from oracle import oracle
+    nseg = min(max_segments, table.nseg)
+    batches = table.batches(False)[:nseg]
+    rows = sum(b[0] for b in batches)
+    done, t0 = 0, time.perf_counter()
+    while True:
+        oracle.aggregate(env.env, plan, batches, env.ncols)
+        done += rows
+        el = time.perf_counter() - t0
+        if el >= budget_s:
+            break
+    return done / el, rows, os.cpu_count() or 1
+
+
+# ------------------------------------------------------------------ workloads
+def make_workload(name: str, rank: int):
+    from warpstore_b200 import workloads as W
+    if name == "pricing_summary_60m":
+        t = W.pricing_summary(W.PRICING_ROWS, seed=2 + rank)
+        e, aq, ds = W.pricing_summary_query(t)
+        return t, e, aq, ds, W.PRICING_BYTES_PER_ROW, 1024, {
+            "workload": "pricing_summary_60m", "rows": t.n, "segments": t.nseg, "segment_rows": t.seg_rows,
+            "columns": "ship_date i32, quantity/price/discount/tax i64, flag1/flag2 u8-encoded",
+            "groups": 6, "aggregation": "dense", "l2": "inputs 2.28 GB >> 126 MB L2 (no flush needed)"}
+    if name == "filter_groupby_1m":
+        t = W.filter_groupby_1m(1 << 20, seed=0 + rank)
+        e, aq = W.filter_groupby_1m_query(t)
+        return t, e, aq, None, W.FILTER_GROUPBY_BYTES_PER_ROW, 1024, {
+            "workload": "filter_groupby_1m", "rows": t.n, "groups": 16, "aggregation": "hash",
+            "l2": "inputs 21 MB fit in L2: L2 flushed between steps"}
+    raise SystemExit(f"unknown workload {name}")
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+
+    from warpstore_b200 import abi, ops
+
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+    ops.lib().ws_set_stream(stream.cuda_stream)
+    ops.gpu_init()
+    table, env, aq, ds, bpr, cap, cfg = make_workload(args.workload, rank)
+    table.to_device()
+    ops.jit_set_mode(abi.JIT_SYNC)
+    fn = abi.JF_NOKEYS if aq.plan.nkeys == 0 else abi.JF_DENSE if ds is not None else abi.JF_GROUPED
+    prog = ops.jit_get(env.env, env.ncols, aq.plan, fn, cfg["workload"])
+    if not prog:
+        raise SystemExit("codegen failed")
+    flush = None
+    if table.nbytes() < 512 << 20:  # small inputs: write a buffer larger than L2 between steps
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    batches = table.batches(True)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+
+    def step(i=None):
+        agg = ops.GpuAggregator(aq.plan, cap, ds)
+        for n, _, views in batches:
+            for c, v in enumerate(views):
+                env.env.cols[c] = v
+            agg.add_batch(env.env, env.ncols, n)
+        with torch.cuda.stream(stream):
+            if i is not None:
+                ev[i][0].record(stream)
+            agg.run(env.env, prog)
+            if i is not None:
+                ev[i][1].record(stream)
+        keys, accs, exact = agg.fetch()
+        agg.close()
+        return keys.shape[0]
+
+    def maybe_flush():
+        if flush is not None:
+            with torch.cuda.stream(stream):
+                flush.fill_(1)
+
+    for _ in range(args.warmup):
+        maybe_flush()
+        step()
+    stream.synchronize()
+    barrier(ws)
+    clocks = ClockSampler(local)
+    clocks.start()
+    t_total = 0.0
+    launches0 = ops.kernel_launches()
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    for i in range(args.steps):
+        maybe_flush()
+        if i == 0:
+            s0.record(stream)
+        step(i)
+    s1.record(stream)
+    s1.synchronize()
+    launches = ops.kernel_launches() - launches0
+    total_ms = s0.elapsed_time(s1)
+    if flush is not None:  # the flush kernels are not query work
+        total_ms = sum(a.elapsed_time(b) for a, b in ev) + 0.0
+    barrier(ws)
+    clk = clocks.stop()
+    kernel_ms = float(np.mean([a.elapsed_time(b) for a, b in ev]))
+    ms_step = reduce_max(total_ms / args.steps, ws)
+    rows_all = table.n * ws
+    value = rows_all / (ms_step / 1e3) / 1e9
+
+    # end to end from pinned host buffers through the C ABI
+    e2e_steps = max(1, min(args.steps, 5))
+    hosts = [torch.from_numpy(c.host).pin_memory() for c in table.cols]
+    devs = [torch.empty(c.host.size, dtype=torch.uint8, device="cuda") for c in table.cols]
+    e2e_batches = []
+    for s in range(table.nseg):
+        views = table.views(s, True)
+        for c, v in enumerate(views):
+            v.p = devs[c].data_ptr() + table.cols[c].offsets[s]
+        e2e_batches.append((table.seg_len(s), 0, views))
+    d2h = 0
+
+    def e2e_step():
+        nonlocal d2h
+        with torch.cuda.stream(stream):
+            for h, d in zip(hosts, devs):
+                d.copy_(h, non_blocking=True)
+        agg = ops.GpuAggregator(aq.plan, cap, ds)
+        for n, _, views in e2e_batches:
+            for c, v in enumerate(views):
+                env.env.cols[c] = v
+            agg.add_batch(env.env, env.ncols, n)
+        agg.run(env.env, prog)
+        keys, accs, exact = agg.fetch()
+        d2h = keys.nbytes + exact.nbytes
+        agg.close()
+
+    e2e_step()
+    stream.synchronize()
+    barrier(ws)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = reduce_max(e0.elapsed_time(e1) / e2e_steps, ws)
+    e2e_value = rows_all / (e2e_ms / 1e3) / 1e9
+
+    peak, peak_kind = measured_peak()
+    algo_bytes = bpr * table.n
+    achieved = algo_bytes / (kernel_ms / 1e3) / 1e9
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        rate, rows, cores = cpu_oracle_rate(table, env, aq.plan, args.cpu_seconds)
+        cpu = {"value": rate / 1e9, "unit": "G rows/s", "cores": cores, "kind": "port",
+               "sample": f"{rows} rows (first segments of the same table), repeated for ~{args.cpu_seconds:.0f} s"}
+    if rank == 0:
+        line = {
+            "metric": "scan_filter_aggregate_throughput", "value": round(value, 4), "unit": "G rows/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+            "data": "synthetic (seeded numpy)", "config": dict(cfg, parallelism=f"replicas{ws}"),
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": args.traffic, "peak_kind": f"{peak_kind} hbm_gbs",
+                         "kernel_ms": round(kernel_ms, 4), "algorithmic_bytes": algo_bytes},
+            "e2e": {"value": round(e2e_value, 4), "unit": "G rows/s", "h2d_bytes_per_step": table.nbytes(),
+                    "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_ms, 3)},
+            "gpu_launches": int(launches), "clocks": clk, "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    table.free_device()
+
+
+def run_reference(args, ws, rank, local):
+    if rank != 0:
+        return
+    from warpstore_b200 import workloads as W
+    name = args.workload
+    if name == "pricing_summary_60m":
+        # the per-step sample: 8 segments (8.4M rows) of the same table
+        t = W.pricing_summary(8 * W.SEG_ROWS, seed=2)
+        e, aq, ds = W.pricing_summary_query(t)
+        cfg = {"workload": "pricing_summary_60m", "rows": W.PRICING_ROWS, "sample_rows": t.n}
+    else:
+        t = W.filter_groupby_1m(1 << 20, seed=0)
+        e, aq = W.filter_groupby_1m_query(t)
+        cfg = {"workload": "filter_groupby_1m", "rows": t.n, "sample_rows": t.n}
+    from oracle import oracle
+    batches = t.batches(False)
+    for _ in range(args.warmup):
+        oracle.aggregate(e.env, aq.plan, batches, e.ncols)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        oracle.aggregate(e.env, aq.plan, batches, e.ncols)
+    el = time.perf_counter() - t0
+    rate = t.n * args.steps / el / 1e9
+    cores = os.cpu_count() or 1
+    line = {"metric": "scan_filter_aggregate_throughput", "value": round(rate, 4), "unit": "G rows/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(el / args.steps * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+            "data": "synthetic (seeded numpy)", "config": cfg, "impl": "reference",
+            "cpu_baseline": {"value": round(rate, 4), "unit": "G rows/s", "cores": cores, "kind": "port",
+                             "sample": f"{t.n} rows per step"},
+            "e2e": {"value": round(rate, 4), "unit": "G rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="pricing_summary_60m", choices=["pricing_summary_60m", "filter_groupby_1m"])
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--traffic", type=float, default=None, help="ncu dram bytes per launch, when known")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        ws = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        run_reference(args, ws, rank, 0)
+        return
+    ws, rank, local = dist_setup(args.gpus)
+    try:
+        run_ours(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,157 @@
+/* libwarpstore_b200 — C ABI of the B200 query-execution core.
+ *
+ * These entry points replace the GPU operator layer of the Warpstore engine: src/gpu.h (allocation,
+ * aggregation, selection, gathers, joins) and src/jit.h (per-query compiled plans and the plan cache).
+ * Each declaration names the reference interface it stands in for.  The C++ engine keeps calling the
+ * same C++ signatures through the header-only shim ws_gpu.hpp, which forwards here.
+ *
+ * Conventions
+ *  - Every function returns WS_OK (0) or an error code; the message of the calling thread's last
+ *    error is ws_last_error().  Codes are the engine's SQL error numbers: WS_ERR_OOM (1041) means
+ *    "GPU out of memory" (the engine retries the query alone), WS_ERR_PLAN (1235) a plan the
+ *    interpreter cannot run, WS_ERR_INTERNAL (1105) everything else.
+ *  - Device pointers are plain CUDA device addresses.  Work is issued on the calling thread's stream
+ *    (ws_set_stream; default: the per-thread default stream, as the engine is built with
+ *    --default-stream per-thread).  Functions that return a count synchronize that stream.
+ *  - Buffers returned through T** are stream-ordered pool allocations: release them with ws_tmp_free.
+ *  - All entry points are re-entrant across threads.
+ */
+#ifndef WS_B200_H
+#define WS_B200_H
+#include "ws_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WS_OK 0
+#define WS_ERR_OOM 1041
+#define WS_ERR_INTERNAL 1105
+#define WS_ERR_PLAN 1235
+#define WS_ERR_SIZE 1206     /* an output buffer is too small: the needed size is returned */
+#define WS_ERR_ARG 1210      /* invalid argument */
+#define WS_ERR_RANGE 1264    /* a dense GROUP BY key outside its declared range */
+
+/* ---- errors */
+const char* ws_last_error(void);
+int ws_last_error_code(void);
+
+/* ---- device runtime (src/gpu.h:12-56: gpuInit, gpuSmCount, gpuArch, gpuDescribe, devAlloc/devFree,
+ *      tmpAlloc/tmpFree, h2d/d2h/d2d, gpuSync, gpuTrimPool) */
+int ws_gpu_init(void);
+int ws_gpu_sm_count(void);
+int ws_gpu_arch(void);
+int ws_gpu_describe(char* buf, size_t size);
+int ws_set_stream(void* stream); /* cudaStream_t for this thread; NULL restores the default */
+void* ws_get_stream(void);
+int ws_dev_alloc(size_t bytes, void** out);
+int ws_dev_free(void* p);
+int ws_tmp_alloc(size_t bytes, void** out);
+int ws_tmp_free(void* p);
+int ws_h2d(void* dst, const void* src, size_t bytes);
+int ws_d2h(void* dst, const void* src, size_t bytes);
+int ws_d2d(void* dst, const void* src, size_t bytes);
+int ws_gpu_sync(void);
+int ws_gpu_trim_pool(void);
+
+/* ---- aggregation (src/gpu.h:84-130, class GpuAggregator).
+ * Batches (segments, write buffers or a joined relation) are collected with ws_agg_add_batch and
+ * aggregated by ws_agg_run in one pass.  Without GROUP BY there is one result row; with a dense spec
+ * (G > 0) groups index arrays directly; otherwise an open-addressing hash table of `capacity` rows
+ * (rounded up to a power of two) is used, and ws_agg_overflowed reports when it filled up (the
+ * caller retries bigger, as the engine does). */
+typedef struct ws_aggregator ws_aggregator;
+typedef struct ws_jit_program ws_jit_program;
+int ws_agg_create(const ws_agg_plan* plan, int64_t capacity, const ws_dense_spec* dense, ws_aggregator** out);
+void ws_agg_destroy(ws_aggregator* agg);
+int ws_agg_add_batch(ws_aggregator* agg, const ws_expr_env* env, int ncols, int64_t n, const uint32_t* del);
+int ws_agg_run(ws_aggregator* agg, const ws_expr_env* env, const ws_jit_program* jit);
+int ws_agg_run_window(ws_aggregator* agg, const ws_expr_env* env, const ws_jit_program* jit);
+int ws_agg_batches(const ws_aggregator* agg);
+int ws_agg_windows(const ws_aggregator* agg);
+int64_t ws_agg_rows_in(const ws_aggregator* agg);
+int ws_agg_is_dense(const ws_aggregator* agg);
+int64_t ws_agg_capacity(const ws_aggregator* agg);
+int ws_agg_overflowed(ws_aggregator* agg, int* out);
+int ws_agg_group_count(ws_aggregator* agg, int64_t* out);
+/* Groups in host memory (GpuAggregator::fetch): keys[g * nkeys + k], accs[g * naggs + a] in the engine's
+ * format (int64 bits for integer keys and aggBits slots; a split BIGINT SUM as its 2^32-weighted high
+ * and low parts; doubles otherwise).  exact (optional) receives [g][naggs][2] int64 words: (lo, hi) of
+ * the exact int128 integer SUM, (value, 0) for COUNT / integer MIN / MAX, (bits, 0) for doubles.
+ * max_groups < groups: WS_ERR_SIZE with *ngroups set. */
+int ws_agg_fetch(ws_aggregator* agg, int64_t max_groups, double* keys, double* accs, int64_t* exact, int64_t* ngroups);
+/* Without GROUP BY: which slots hold exact int64 bits (GpuAggregator::sumBitsSlots) and the high 64 bits
+ * of the exact integer sums (GpuAggregator::sumHigh; valid after ws_agg_fetch). */
+int ws_agg_sum_bits_slots(const ws_aggregator* agg, uint8_t* out);
+int ws_agg_sum_high(const ws_aggregator* agg, int64_t* out);
+/* Groups left in device memory, column-major (GpuAggregator::compact): keys[k * g + i], accs[a * g + i]. */
+int ws_agg_compact(ws_aggregator* agg, double** keys, double** accs, int64_t* ngroups);
+
+/* ---- selection and gathers (src/gpu.h:132-143, :170-172) */
+int ws_select(const ws_expr_env* env, int has_where, ws_prog where, int64_t n, const uint32_t* del, int32_t* out_idx,
+              const ws_jit_program* jit, int64_t* count);
+int ws_select_multi(const ws_expr_env* env, int has_where, ws_prog where, int nb, const int64_t* bn,
+                    const uint32_t* const* bdel, const ws_col_view* bcols, int ncols, int32_t** out_idx,
+                    int64_t* per_batch, const ws_jit_program* jit, int64_t* count);
+int ws_gather_multi(const ws_col_view* src, const int64_t* boff, int nb, int ptype, int esize, const int32_t* idx,
+                    int64_t m, void* dst);
+int ws_gather(const void* src, int ptype, const int32_t* idx, int64_t m, void* dst);
+
+/* ---- joins (src/gpu.h:178-186: gpuHashJoin, gpuHashJoinParts).  Output pairs (build row, probe row)
+ * are grouped by probe partition; out_off (optional, npparts + 1) receives each partition's first pair. */
+int ws_hash_join_parts(ws_col_view build_key, const int64_t* boff, int nbparts, ws_col_view probe_key,
+                       const int64_t* poff, int npparts, int32_t** out_build, int32_t** out_probe, int64_t* out_off,
+                       int64_t* m);
+int ws_hash_join(ws_col_view build_key, int64_t nb, ws_col_view probe_key, int64_t np, int32_t** out_build,
+                 int32_t** out_probe, int64_t* m);
+
+/* ---- compiled plans (src/jit.h:33-75) */
+typedef struct ws_jit_info {
+  int id;
+  int fn_kind;
+  int state;       /* 0 compiling, 1 ready, 2 failed */
+  int from_disk;
+  double compile_ms;
+  int64_t execs;
+  double total_ms, last_ms;
+  int64_t source_bytes;
+} ws_jit_info;
+typedef struct ws_jit_query_info {
+  int compiled, hits, from_disk, background;
+  double compile_ms;
+} ws_jit_query_info;
+int ws_jit_set_mode(int mode);          /* this thread: WS_JIT_OFF / ON / SYNC */
+int ws_jit_mode(void);
+int ws_jit_set_default_mode(int mode);
+int ws_jit_set_cache_dir(const char* dir);
+/* The compiled plan for `fn` over the plan's expressions (nullptr in *out: run interpreted). */
+int ws_jit_get(const ws_expr_env* env, int ncols, const ws_agg_plan* plan, int fn, const char* kind,
+               const ws_jit_program** out);
+int ws_prog_is_int(const ws_expr_env* env, ws_prog p);
+int ws_jit_program_info(const ws_jit_program* p, ws_jit_info* info);
+int ws_jit_source_of(int id, char* buf, size_t size, size_t* needed);
+int ws_jit_plan_cache_count(void);
+int ws_jit_plan_cache_row(int i, ws_jit_info* info);
+int ws_jit_clear_cache(void);
+int ws_jit_begin_query(const char* sql);
+int ws_jit_end_query(double query_ms, ws_jit_query_info* info);
+
+/* Generated evaluator source of a plan (what ws_jit_get compiles; host only, no device needed). */
+int ws_codegen_source(const ws_expr_env* env, int ncols, const ws_agg_plan* plan, int fn, char* buf, size_t size,
+                      size_t* needed);
+/* Compiles a plan's module with NVRTC for sm_<arch_sm> without loading it (host only, no device):
+ * a build check of the generated code.  dense_groups > 0 also compiles the register-accumulator
+ * dense kernel for that many groups. */
+int ws_codegen_compile_check(const ws_expr_env* env, int ncols, const ws_agg_plan* plan, int fn, int dense_groups,
+                             int arch_sm, size_t* cubin_bytes);
+
+/* ---- introspection */
+/* Layout check: out[0..] = sizeof / offsetof values of the ABI structs as this library sees them. */
+int ws_abi_layout(int64_t* out, int n);
+/* Kernels this library has launched since it was loaded (all threads). */
+int64_t ws_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WS_B200_H */

@@ -1,0 +1,150 @@
+"""Parity of selection (ascending row indices + per-batch counts), gathers and inner hash joins with
+the CPU oracle: indices bit-exact and in order; join pairs compared as sorted multisets."""
+import numpy as np
+import pytest
+
+from oracle import oracle
+from warpstore_b200 import abi, ops
+from warpstore_b200 import query as q
+from warpstore_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def run_select(t, e, where, jit, deleted=None):
+    t.to_device()
+    ops.jit_set_mode(abi.JIT_SYNC if jit else abi.JIT_OFF)
+    try:
+        prog = None
+        if jit:
+            fp = abi.AggPlan()
+            fp.hasWhere = 1 if where is not None else 0
+            if where is not None:
+                fp.where = where
+            fp.naggs = 1
+            fp.ops[0] = abi.AGG_COUNT
+            prog = ops.jit_get(e.env, e.ncols, fp, abi.JF_FLAGM, "filter")
+            assert prog
+        ptr, m, per = ops.select_multi(e.env, where, t.batches(True, [d.ptr for d in deleted] if deleted else None),
+                                       e.ncols, prog)
+        idx = ops.device_to_array(ptr, np.int32, m)
+        ops.tmp_free(ptr)
+        return idx, per
+    finally:
+        ops.jit_set_mode(-1)
+
+
+@pytest.mark.parametrize("n", [0, 1, 1000, 1025, 3 * (1 << 20) + 17])
+def test_select_multi(n):
+    rng = np.random.default_rng(n)
+    t = W.Table(max(n, 0))
+    t.add("a", abi.T_I32, rng.integers(0, 2406, n, dtype=np.int32))
+    t.add("b", abi.T_F64, rng.random(n))
+    e = W.env_for(t)
+    where = e.compile(q.and_(q.col(0).lt(1203), q.col(1).lt(q.lit(0.9))))
+    if n == 0:
+        ptr, m, per = ops.select_multi(e.env, where, [], e.ncols)
+        assert m == 0
+        ops.tmp_free(ptr)
+        return
+    oi, op = oracle.select(e.env, where, t.batches(False), e.ncols)
+    for jit in (True, False):
+        gi, gp = run_select(t, e, where, jit)
+        assert np.array_equal(gi, oi)
+        assert list(gp) == list(op)
+
+
+def test_select_with_deletes_and_gather():
+    n = 2 * (1 << 20) + 999
+    rng = np.random.default_rng(1)
+    t = W.Table(n)
+    t.add("a", abi.T_I32, rng.integers(0, 100, n, dtype=np.int32))
+    t.add("v", abi.T_I64, rng.integers(-2**40, 2**40, n, dtype=np.int64), enc=0)
+    t.add("c", abi.T_I64, rng.integers(1000, 1200, n, dtype=np.int64), enc=1)
+    e = W.env_for(t)
+    where = e.compile(q.col(0).ge(50))
+    dh, dd = [], []
+    for s in range(t.nseg):
+        m = t.seg_len(s)
+        bits = rng.integers(0, 2**32, (m + 31) // 32, dtype=np.uint32) & rng.integers(0, 2**32, (m + 31) // 32, dtype=np.uint32)
+        dh.append(bits)
+        dd.append(ops.DeviceBuffer.from_array(bits))
+    oi, op = oracle.select(e.env, where, t.batches(False, [d.ctypes.data for d in dh]), e.ncols)
+    gi, gp = run_select(t, e, where, True, dd)
+    assert np.array_equal(gi, oi) and list(gp) == list(op)
+    # gathers of the selected rows: raw and encoded columns
+    boff = [s * t.seg_rows for s in range(t.nseg)]
+    idx = ops.DeviceBuffer.from_array(gi)
+    for c, pt, es in ((1, abi.PT_I64, 8), (2, abi.PT_I64, 8), (0, abi.PT_I32, 4)):
+        views = [t.views(s, True)[c] for s in range(t.nseg)]
+        out = ops.DeviceBuffer(len(gi) * es)
+        ops.gather_multi(views, boff, pt, es, idx.ptr, len(gi), out.ptr)
+        got = out.to_array(np.int64 if es == 8 else np.int32)
+        hv = [t.views(s, False)[c] for s in range(t.nseg)]
+        want = np.empty(len(gi), dtype=got.dtype)
+        oracle.gather_multi(hv, boff, pt, es, gi, want)
+        assert np.array_equal(got, want)
+        assert np.array_equal(got, t.cols[c].data[gi].astype(got.dtype))
+
+
+def join_case(nb, np_, key_space, seed, dup=False, nulls=False, i32=False):
+    rng = np.random.default_rng(seed)
+    dt = np.int32 if i32 else np.int64
+    if dup:
+        bk = rng.integers(0, key_space, nb).astype(dt)
+    else:
+        bk = rng.permutation(key_space)[:nb].astype(dt)
+    pk = rng.integers(0, key_space, np_).astype(dt)
+    if nulls:
+        null = abi.NULL_I32 if i32 else abi.NULL_I64
+        bk[rng.random(nb) < 0.05] = null
+        pk[rng.random(np_) < 0.05] = null
+    return bk, pk
+
+
+@pytest.mark.parametrize("nb,np_,space,dup,nulls,i32", [
+    (1000, 5000, 1000, False, False, False),
+    (100_000, 1_000_000, 400_000, False, False, False),
+    (50_000, 200_000, 10_000, True, True, False),     # duplicate build keys: many matches per probe
+    (30_000, 100_000, 30_000, False, True, True),     # int32 keys with NULLs
+    (1, 1, 1, False, False, False),
+])
+def test_hash_join(nb, np_, space, dup, nulls, i32):
+    bk, pk = join_case(nb, np_, space, nb + np_, dup, nulls, i32)
+    t = abi.T_I32N if i32 else abi.T_I64N
+    db, dp = ops.DeviceBuffer.from_array(bk), ops.DeviceBuffer.from_array(pk)
+    ob, op, m = ops.hash_join(abi.ColView(db.ptr, t, 0, 0, 0), nb, abi.ColView(dp.ptr, t, 0, 0, 0), np_)
+    gb, gp = ops.device_to_array(ob, np.int32, m), ops.device_to_array(op, np.int32, m)
+    ops.tmp_free(ob)
+    ops.tmp_free(op)
+    wb, wp = oracle.hash_join(abi.ColView(bk.ctypes.data, t, 0, 0, 0), nb, abi.ColView(pk.ctypes.data, t, 0, 0, 0), np_)
+    assert m == len(wb)
+    g = np.lexsort((gb, gp))
+    w = np.lexsort((wb, wp))
+    assert np.array_equal(gp[g], wp[w]) and np.array_equal(gb[g], wb[w])
+
+
+def test_hash_join_partitions():
+    rng = np.random.default_rng(4)
+    P = 4
+    bks, pks = [], []
+    for p in range(P):  # co-located: partition p's keys are == p mod P
+        bks.append((rng.permutation(20_000)[:5_000] * P + p).astype(np.int64))
+        pks.append((rng.integers(0, 20_000, 30_000) * P + p).astype(np.int64))
+    bk, pk = np.concatenate(bks), np.concatenate(pks)
+    boff = [0] + list(np.cumsum([len(x) for x in bks]))
+    poff = [0] + list(np.cumsum([len(x) for x in pks]))
+    db, dp = ops.DeviceBuffer.from_array(bk), ops.DeviceBuffer.from_array(pk)
+    ob, op, m, outoff = ops.hash_join_parts(abi.ColView(db.ptr, abi.T_I64, 0, 0, 0), [int(x) for x in boff],
+                                            abi.ColView(dp.ptr, abi.T_I64, 0, 0, 0), [int(x) for x in poff])
+    gb, gp = ops.device_to_array(ob, np.int32, m), ops.device_to_array(op, np.int32, m)
+    ops.tmp_free(ob)
+    ops.tmp_free(op)
+    wb, wp = oracle.hash_join(abi.ColView(bk.ctypes.data, abi.T_I64, 0, 0, 0), len(bk),
+                              abi.ColView(pk.ctypes.data, abi.T_I64, 0, 0, 0), len(pk))
+    assert m == len(wb)
+    for p in range(P):  # pairs grouped by probe partition
+        seg = gp[outoff[p]:outoff[p + 1] if p + 1 < P else m]
+        assert np.all((seg >= poff[p]) & (seg < poff[p + 1]))
+    g, w = np.lexsort((gb, gp)), np.lexsort((wb, wp))
+    assert np.array_equal(gp[g], wp[w]) and np.array_equal(gb[g], wb[w])

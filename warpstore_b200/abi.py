@@ -1,0 +1,88 @@
+"""ctypes mirror of the ABI structs in include/ws_types.h (the engine's Instr / ColView / ExprEnv /
+AggPlan / DenseSpec layout, src/devtypes.h:64-547)."""
+from __future__ import annotations
+
+import ctypes as C
+
+MAX_STACK, MAX_COLS, MAX_CODE, MAX_CONSTS, MAX_SETS, MAX_KEYS, MAX_AGGS = 16, 128, 320, 96, 16, 8, 64
+INTERP_KEYS, INTERP_AGGS = 4, 16
+ENC_HEADER = 16
+NULL_I32 = -(1 << 31)
+NULL_I64 = -(1 << 63)
+
+# opcodes (enum ws_op)
+(OP_COL, OP_CONST, OP_ADD, OP_SUB, OP_MUL, OP_DIV, OP_MOD, OP_NEG, OP_EQ, OP_NE, OP_LT, OP_LE, OP_GT, OP_GE,
+ OP_AND, OP_OR, OP_NOT, OP_INSET, OP_SELECT, OP_YEAR, OP_ISNULL, OP_COALESCE, OP_NULLIF, OP_CALL1, OP_CALL2,
+ OP_DICTMAP, OP_INSORTED, OP_VDOT, OP_VEUC, OP_COLRAW) = range(30)
+
+# scalar function ids (enum ws_fn)
+FN = {name: i for i, name in enumerate(
+    "ABS CEIL FLOOR ROUND SQRT EXP LN LOG10 LOG2 SIN COS TAN SIGN MONTH DAY DAYOFWEEK DAYOFYEAR QUARTER WEEKDAY "
+    "LAST_DAY DT_DATE DT_HOUR DT_MINUTE DT_SECOND DATE_TO_DT DT_UNIX UNIX_DT DT_YEAR DT_MONTH DT_DAY ASIN ACOS ATAN "
+    "DEGREES RADIANS WEEK TO_DAYS FROM_DAYS DT_MICRO YEARWEEK".split())}
+FN.update({name: 100 + i for i, name in enumerate(
+    "ROUND2 POW ATAN2 LEAST GREATEST TRUNCATE2 ADD_MONTHS DT_ADD_MONTHS LOG_B IDIV DATE_TRUNC_MONTH DT_DIFF_UNIT".split())})
+
+AGG_SUM, AGG_COUNT, AGG_MIN, AGG_MAX = 0, 1, 2, 3
+DK_COUNT, DK_SUM_I, DK_SUM_D, DK_MIN_I, DK_MAX_I, DK_MIN_D, DK_MAX_D = range(7)
+PT_I32, PT_I64, PT_F64, PT_VEC = 0, 1, 2, 5
+JF_NOKEYS, JF_GROUPED, JF_DENSE, JF_FLAG, JF_FLAGM = range(5)
+JIT_OFF, JIT_ON, JIT_SYNC = 0, 1, 2
+
+# column view types (ColView.t)
+T_I32, T_I64, T_F64, T_I32N, T_I64N, T_VEC, T_DEC = 0, 1, 2, 3, 4, 5, 6
+
+
+class Instr(C.Structure):
+    _fields_ = [("op", C.c_uint8), ("isInt", C.c_uint8), ("arg", C.c_uint16)]
+
+
+class ColView(C.Structure):
+    _fields_ = [("p", C.c_void_p), ("t", C.c_uint8), ("scale", C.c_uint8), ("enc", C.c_uint8), ("off", C.c_int32)]
+
+
+class Prog(C.Structure):
+    _fields_ = [("start", C.c_int16), ("len", C.c_int16)]
+
+
+class ExprEnv(C.Structure):
+    _fields_ = [("code", Instr * MAX_CODE), ("consts", C.c_double * MAX_CONSTS), ("sets", C.c_void_p * MAX_SETS),
+                ("setSize", C.c_int32 * MAX_SETS), ("maps", C.c_void_p * MAX_SETS), ("mapSize", C.c_int32 * MAX_SETS),
+                ("cols", ColView * MAX_COLS), ("ovf", C.c_void_p)]
+
+
+class AggPlan(C.Structure):
+    _fields_ = [("hasWhere", C.c_uint8), ("where", Prog), ("nkeys", C.c_int32), ("keys", Prog * MAX_KEYS),
+                ("naggs", C.c_int32), ("aggs", Prog * MAX_AGGS), ("ops", C.c_uint8 * MAX_AGGS),
+                ("aggInt", C.c_uint8 * MAX_AGGS), ("aggBits", C.c_uint8 * MAX_AGGS), ("aggPart", C.c_uint8 * MAX_AGGS),
+                ("aggNull", C.c_uint8 * MAX_AGGS), ("densePriv", C.c_uint8), ("keyInt", C.c_uint8 * MAX_KEYS),
+                ("genv", C.c_void_p)]
+
+
+class DenseSpec(C.Structure):
+    _fields_ = [("G", C.c_int64), ("copies", C.c_int32), ("copyBytes", C.c_int32), ("priv", C.c_int32),
+                ("kmin", C.c_int64 * MAX_KEYS), ("range", C.c_int64 * MAX_KEYS), ("stride", C.c_int64 * MAX_KEYS),
+                ("slotOff", C.c_int32 * MAX_AGGS), ("kind", C.c_uint8 * MAX_AGGS)]
+
+
+class JitInfo(C.Structure):
+    _fields_ = [("id", C.c_int), ("fn_kind", C.c_int), ("state", C.c_int), ("from_disk", C.c_int),
+                ("compile_ms", C.c_double), ("execs", C.c_int64), ("total_ms", C.c_double), ("last_ms", C.c_double),
+                ("source_bytes", C.c_int64)]
+
+
+class JitQueryInfo(C.Structure):
+    _fields_ = [("compiled", C.c_int), ("hits", C.c_int), ("from_disk", C.c_int), ("background", C.c_int),
+                ("compile_ms", C.c_double)]
+
+
+def layout() -> list[int]:
+    """sizeof / offsetof values in the order of ws_abi_layout() (runtime side of the layout check)."""
+    o = C.sizeof
+    return [o(Instr), o(ColView), ColView.off.offset, o(ExprEnv), ExprEnv.consts.offset, ExprEnv.sets.offset,
+            ExprEnv.setSize.offset, ExprEnv.maps.offset, ExprEnv.mapSize.offset, ExprEnv.cols.offset,
+            ExprEnv.ovf.offset, o(AggPlan), AggPlan.where.offset, AggPlan.nkeys.offset, AggPlan.keys.offset,
+            AggPlan.naggs.offset, AggPlan.aggs.offset, AggPlan.ops.offset, AggPlan.aggInt.offset,
+            AggPlan.aggBits.offset, AggPlan.aggPart.offset, AggPlan.aggNull.offset, AggPlan.densePriv.offset,
+            AggPlan.keyInt.offset, AggPlan.genv.offset, o(DenseSpec), DenseSpec.kmin.offset, DenseSpec.range.offset,
+            DenseSpec.stride.offset, DenseSpec.slotOff.offset, DenseSpec.kind.offset]

@@ -1,0 +1,574 @@
+// Scan kernel bodies, templated over a row evaluator `Ev`.  The library instantiates them with the
+// on-device interpreter (InterpEv, ws_interp.cuh); every query plan instantiates them again with its
+// own generated evaluator, compiled by NVRTC for sm_100a (ws_codegen.cpp).  No host headers.
+//
+// Evaluator contract (all row indices are within the current batch):
+//   static constexpr int NK, NA;            loop bounds (>= nk(), na())
+//   Ev(const Launch&);  void bind(const Launch&, int batch);  bool fastOk;
+//   int nk(), na(), rowWords(), kind(a), woff(a); bool keyInt(k);
+//   void load(i64 r0, bool fast, int nv);   rows r0 .. r0+3 (nv valid) into registers
+//   bool where(i); i64 ikey(k, i); double dkey(k, i); bool ival(a, i, i64&); double dval(a, i)
+//
+// Work decomposition: a batch (segment / write buffer) is cut into tiles of kTile rows; a CTA of
+// kThreads threads takes one tile per iteration, each thread 4 consecutive rows (128-bit loads of
+// 4-byte columns, 2 x 128-bit of 8-byte columns).  Grids are persistent (a multiple of the SM count);
+// CTAs stride over the tiles of all batches of the launch.
+#pragma once
+#include "ws_dev.cuh"
+
+namespace ws {
+
+constexpr int kThreads = 256;
+constexpr int kTile = kThreads * 4;
+constexpr u64 kEmpty = ~0ull;
+constexpr int kMaxRowWords = 1 + 2 * WS_MAX_AGGS;
+
+WS_DI u64 mix64(u64 x) {  // splitmix64 finalizer (Steele, Lea, Flood 2014)
+  x ^= x >> 30;
+  x *= 0xbf58476d1ce4e5b9ull;
+  x ^= x >> 27;
+  x *= 0x94d049bb133111ebull;
+  x ^= x >> 31;
+  return x;
+}
+
+// Visits every live row (not deleted, passing the filter) of the tiles this CTA owns.
+// f(i, batch, row) is called with i = the row's position (0..3) in the evaluator's 4-row group.
+template <class Ev, class F>
+WS_DI void forEachRow(const Launch& L, Ev& ev, F&& f) {
+  int b = 0, bound = -1;
+  for (i64 t = blockIdx.x; t < L.ntiles; t += gridDim.x) {
+    while (t >= __ldg(L.tileStart + b + 1)) ++b;
+    if (b != bound) {
+      ev.bind(L, b);
+      bound = b;
+    }
+    const i64 n = __ldg(L.n + b);
+    const i64 r0 = (t - __ldg(L.tileStart + b)) * kTile + threadIdx.x * 4;
+    const i64 left = n - r0;
+    if (left <= 0) continue;
+    const int nv = left >= 4 ? 4 : (int)left;
+    ev.load(r0, ev.fastOk && nv == 4, nv);
+    unsigned live = (1u << nv) - 1;
+    const uint32_t* del = L.del[b];
+    if (del) live &= ~(__ldg(del + (r0 >> 5)) >> (r0 & 31)) & 0xfu;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+      if (((live >> i) & 1u) && ev.where(i)) f(i, b, r0 + i);
+  }
+}
+
+// ------------------------------------------------------------------ row words
+// A group's accumulator row: word 0 = key word, then each slot's words at woff(a) (slot kinds in
+// SlotKind).  DMIN / DMAX words hold dord(value) so that integer min / max orders them.
+template <class Ev>
+WS_DI void rowIdentity(const Ev& ev, u64* w) {
+#pragma unroll
+  for (int a = 0; a < Ev::NA; ++a) {
+    if (a >= ev.na()) break;
+    const int o = ev.woff(a);
+    switch (ev.kind(a)) {
+      case SK_COUNT: w[o] = 0; break;
+      case SK_ISUM: w[o] = 0, w[o + 1] = 0; break;
+      case SK_IMIN: w[o] = (u64)0x7fffffffffffffffll; break;
+      case SK_IMAX: w[o] = (u64)0x8000000000000000ll; break;
+      case SK_DSUM: w[o] = 0; break;
+      case SK_DMIN: w[o] = (u64)dord(__longlong_as_double(0x7ff0000000000000ll)); break;
+      case SK_DMAX: w[o] = (u64)dord(__longlong_as_double((i64)0xfff0000000000000ull)); break;
+      default: break;
+    }
+  }
+}
+// Adds row `i` of the current 4-row group into accumulator words w (registers).
+template <class Ev>
+WS_DI void rowAccumulate(const Ev& ev, int i, u64* w) {
+#pragma unroll
+  for (int a = 0; a < Ev::NA; ++a) {
+    if (a >= ev.na()) break;
+    const int o = ev.woff(a);
+    switch (ev.kind(a)) {
+      case SK_COUNT: w[o] += 1; break;
+      case SK_ISUM: {
+        i64 v;
+        if (ev.ival(a, i, v)) add128(w[o], *(i64*)&w[o + 1], v);
+        break;
+      }
+      case SK_IMIN: {
+        i64 v;
+        if (ev.ival(a, i, v) && v < (i64)w[o]) w[o] = (u64)v;
+        break;
+      }
+      case SK_IMAX: {
+        i64 v;
+        if (ev.ival(a, i, v) && v > (i64)w[o]) w[o] = (u64)v;
+        break;
+      }
+      case SK_DSUM: {
+        const double v = ev.dval(a, i);
+        if (v == v) w[o] = (u64)__double_as_longlong(__longlong_as_double((i64)w[o]) + v);
+        break;
+      }
+      case SK_DMIN: {
+        const double v = ev.dval(a, i);
+        if (v == v && dord(v) < (i64)w[o]) w[o] = (u64)dord(v);
+        break;
+      }
+      case SK_DMAX: {
+        const double v = ev.dval(a, i);
+        if (v == v && dord(v) > (i64)w[o]) w[o] = (u64)dord(v);
+        break;
+      }
+      default: break;
+    }
+  }
+}
+// w += x (both accumulator rows, same layout)
+template <class Ev>
+WS_DI void rowCombine(const Ev& ev, u64* w, const u64* x) {
+#pragma unroll
+  for (int a = 0; a < Ev::NA; ++a) {
+    if (a >= ev.na()) break;
+    const int o = ev.woff(a);
+    switch (ev.kind(a)) {
+      case SK_COUNT: w[o] += x[o]; break;
+      case SK_ISUM: add128w(w[o], *(i64*)&w[o + 1], x[o], (i64)x[o + 1]); break;
+      case SK_IMIN: case SK_DMIN: if ((i64)x[o] < (i64)w[o]) w[o] = x[o]; break;
+      case SK_IMAX: case SK_DMAX: if ((i64)x[o] > (i64)w[o]) w[o] = x[o]; break;
+      case SK_DSUM:
+        w[o] = (u64)__double_as_longlong(__longlong_as_double((i64)w[o]) + __longlong_as_double((i64)x[o]));
+        break;
+      default: break;
+    }
+  }
+}
+// Atomic w += x into a row in shared or global memory (generic addressing).
+template <class Ev>
+WS_DI void rowAtomicCombine(const Ev& ev, u64* w, const u64* x) {
+#pragma unroll
+  for (int a = 0; a < Ev::NA; ++a) {
+    if (a >= ev.na()) break;
+    const int o = ev.woff(a);
+    switch (ev.kind(a)) {
+      case SK_COUNT: if (x[o]) atomicAdd(w + o, x[o]); break;
+      case SK_ISUM: if (x[o] || x[o + 1]) atomicAdd128(w + o, (i64*)(w + o + 1), x[o], (i64)x[o + 1]); break;
+      case SK_IMIN: case SK_DMIN: if ((i64)x[o] < (i64)*(volatile u64*)(w + o)) atomicMin((i64*)(w + o), (i64)x[o]); break;
+      case SK_IMAX: case SK_DMAX: if ((i64)x[o] > (i64)*(volatile u64*)(w + o)) atomicMax((i64*)(w + o), (i64)x[o]); break;
+      case SK_DSUM: {
+        const double v = __longlong_as_double((i64)x[o]);
+        if (v != 0.0) atomicAdd((double*)(w + o), v);
+        break;
+      }
+      default: break;
+    }
+  }
+}
+// The accumulator row of a single input row (count 1, each argument once; NULL arguments neutral).
+template <class Ev>
+WS_DI void rowOfInput(const Ev& ev, int i, u64* w) {
+  rowIdentity(ev, w);
+  rowAccumulate(ev, i, w);
+}
+
+// Warp + block reduction of one accumulator row per thread into `out` (thread 0's view).
+template <class Ev, int RW>
+WS_DI void blockReduceRow(const Ev& ev, u64 (&w)[RW], u64* sred /* [kThreads/32][RW] */) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int rw = ev.rowWords();
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    u64 x[RW];
+#pragma unroll
+    for (int j = 0; j < RW; ++j) x[j] = j < rw ? __shfl_down_sync(0xffffffffu, w[j], off) : 0;
+    rowCombine(ev, w, x);
+  }
+  if (lane == 0)
+#pragma unroll
+    for (int j = 0; j < RW; ++j)
+      if (j < rw) sred[warp * RW + j] = w[j];
+  __syncthreads();
+  if (warp == 0) {
+    if (lane < kThreads / 32) {
+#pragma unroll
+      for (int j = 0; j < RW; ++j)
+        if (j < rw) w[j] = sred[lane * RW + j];
+    } else {
+      rowIdentity(ev, w);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      u64 x[RW];
+#pragma unroll
+      for (int j = 0; j < RW; ++j) x[j] = j < rw ? __shfl_down_sync(0xffffffffu, w[j], off) : 0;
+      rowCombine(ev, w, x);
+    }
+  }
+  __syncthreads();
+}
+
+// After every CTA wrote its partial rows part[cta][nrows][rw]: the last CTA to finish reduces them
+// into rows[nrows][rw] (word 0 of each row = its key word, left as is).  Thread t folds CTAs t,
+// t + blockDim, ... in order, then a fixed-shape tree combines the threads: deterministic.
+template <class Ev, int RW>
+WS_DI void lastCtaReduce(const Launch& L, const Ev& ev, int nrows, u64* sred) {
+  __shared__ bool amLast;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) amLast = atomicAdd(L.ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!amLast) return;
+  __threadfence();
+  const int rw = ev.rowWords();
+  for (int g = 0; g < nrows; ++g) {
+    u64 w[RW];
+    rowIdentity(ev, w);
+    for (unsigned c = threadIdx.x; c < gridDim.x; c += blockDim.x) {
+      const u64* p = L.part + ((size_t)c * nrows + g) * rw;
+      u64 x[RW];
+#pragma unroll
+      for (int j = 1; j < RW; ++j) x[j] = j < rw ? __ldcg(p + j) : 0;
+      rowCombine(ev, w, x);
+    }
+    blockReduceRow(ev, w, sred);
+    if (threadIdx.x == 0) {  // rows accumulate across launches (scan windows): combine into them
+      u64* out = L.rows + (size_t)g * rw;
+      u64 x[RW];
+#pragma unroll
+      for (int j = 1; j < RW; ++j) x[j] = j < rw ? out[j] : 0;
+      rowCombine(ev, x, w);
+#pragma unroll
+      for (int j = 1; j < RW; ++j)
+        if (j < rw) out[j] = x[j];
+    }
+  }
+}
+
+// ------------------------------------------------------------------ no GROUP BY
+template <class Ev>
+__device__ void aggNoKeys(const Launch& L) {
+  constexpr int RW = Ev::RW;
+  __shared__ u64 sred[(kThreads / 32) * RW];
+  Ev ev(L);
+  u64 w[RW];
+  rowIdentity(ev, w);
+  forEachRow(L, ev, [&](int i, int, i64) { rowAccumulate(ev, i, w); });
+  blockReduceRow(ev, w, sred);
+  const int rw = ev.rowWords();
+  if (threadIdx.x == 0)
+    for (int j = 1; j < rw; ++j) L.part[(size_t)blockIdx.x * rw + j] = w[j];
+  lastCtaReduce<Ev, RW>(L, ev, 1, sred);
+}
+
+// ------------------------------------------------------------------ dense GROUP BY
+template <class Ev>
+WS_DI bool denseIndex(const Launch& L, const Ev& ev, int i, i64& g) {
+  g = 0;
+#pragma unroll
+  for (int k = 0; k < Ev::NK; ++k) {
+    if (k >= ev.nk()) break;
+    const i64 d = ev.ikey(k, i) - L.kmin[k];
+    if ((u64)d >= (u64)L.range[k]) return false;
+    g += d * L.stride[k];
+  }
+  return true;
+}
+
+// Few groups: every thread keeps all G accumulator rows in registers (GR = G, compile-time), rows
+// of one 4-row group are added with predication, no atomics.  Partials per CTA, last CTA reduces.
+template <class Ev, int GR>
+__device__ void aggDenseReg(const Launch& L) {
+  constexpr int RW = Ev::RW;
+  __shared__ u64 sred[(kThreads / 32) * RW];
+  Ev ev(L);
+  u64 w[GR][RW];
+#pragma unroll
+  for (int g = 0; g < GR; ++g) rowIdentity(ev, w[g]);
+  forEachRow(L, ev, [&](int i, int, i64) {
+    i64 gi;
+    if (!denseIndex(L, ev, i, gi)) {
+      L.err[0] = 1;
+      return;
+    }
+    u64 x[RW];
+    rowOfInput(ev, i, x);
+#pragma unroll
+    for (int g = 0; g < GR; ++g)
+      if (gi == g) rowCombine(ev, w[g], x);
+  });
+  const int rw = ev.rowWords();
+#pragma unroll
+  for (int g = 0; g < GR; ++g) {
+    blockReduceRow(ev, w[g], sred);
+    if (threadIdx.x == 0)
+      for (int j = 1; j < rw; ++j) L.part[((size_t)blockIdx.x * GR + g) * rw + j] = w[g][j];
+  }
+  lastCtaReduce<Ev, RW>(L, ev, GR, sred);
+}
+
+// Medium G: the CTA's rows [G][rw] live in shared memory (rows' key words unused) and take shared
+// atomics; at the end each non-empty group is merged into the global rows with global atomics.
+template <class Ev>
+__device__ void aggDenseShared(const Launch& L) {
+  extern __shared__ __align__(16) u64 wsSmem[];
+  Ev ev(L);
+  const int rw = ev.rowWords();
+  const i64 G = L.G;
+  for (i64 g = threadIdx.x; g < G; g += blockDim.x) rowIdentity(ev, wsSmem + g * rw);
+  __syncthreads();
+  forEachRow(L, ev, [&](int i, int, i64) {
+    i64 gi;
+    if (!denseIndex(L, ev, i, gi)) {
+      L.err[0] = 1;
+      return;
+    }
+    u64 x[kMaxRowWords];
+    rowOfInput(ev, i, x);
+    rowAtomicCombine(ev, wsSmem + gi * rw, x);
+  });
+  __syncthreads();
+  for (i64 g = threadIdx.x; g < G; g += blockDim.x) {
+    const u64* s = wsSmem + g * rw;
+    if (s[ev.woff(0)] == 0) continue;  // slot 0 is COUNT(*): no rows of this group in this CTA
+    rowAtomicCombine(ev, L.rows + g * rw, s);
+  }
+}
+
+// Large G: rows go straight to the global rows with atomics.
+template <class Ev>
+__device__ void aggDenseGlobal(const Launch& L) {
+  Ev ev(L);
+  const int rw = ev.rowWords();
+  forEachRow(L, ev, [&](int i, int, i64) {
+    i64 gi;
+    if (!denseIndex(L, ev, i, gi)) {
+      L.err[0] = 1;
+      return;
+    }
+    u64 x[kMaxRowWords];
+    rowOfInput(ev, i, x);
+    rowAtomicCombine(ev, L.rows + gi * rw, x);
+  });
+}
+
+// ------------------------------------------------------------------ hash GROUP BY
+// Key word of a row: a single integer key is its own key word, a single double key its canonical
+// bits (both exact); several keys are folded into a 64-bit hash that identifies the group, and their
+// values are stored beside the table.
+template <class Ev>
+WS_DI u64 keyWord(const Ev& ev, int i, double* kv) {
+  if (ev.nk() == 1) {
+    const u64 w = ev.keyInt(0) ? (u64)ev.ikey(0, i) : (u64)dkeyBits(ev.dkey(0, i));
+    kv[0] = __longlong_as_double((i64)w);
+    return w;
+  }
+  u64 h = 0x9e3779b97f4a7c15ull;
+#pragma unroll
+  for (int k = 0; k < Ev::NK; ++k) {
+    if (k >= ev.nk()) break;
+    const u64 b = ev.keyInt(k) ? (u64)ev.ikey(k, i) : (u64)dkeyBits(ev.dkey(k, i));
+    kv[k] = __longlong_as_double((i64)b);
+    h = mix64(h ^ b) + (u64)k;
+  }
+  return h == kEmpty ? (h ^ 1) : h;
+}
+
+// Inserts accumulator row x under key word kw into the global table (linear probing, bounded).
+template <class Ev>
+WS_DI void globalInsert(const Launch& L, const Ev& ev, u64 kw, const double* kv, const u64* x) {
+  if (*(volatile int*)(L.err + 1)) return;  // the table overflowed: the caller reruns with a bigger one
+  const int rw = ev.rowWords();
+  if (kw == kEmpty) {  // the EMPTY key word itself has a dedicated row after the table
+    u64* row = L.table + (L.mask + 1) * rw;
+    if (atomicCAS(row, 0ull, 1ull) == 0ull)
+      for (int k = 0; k < ev.nk(); ++k) L.tkeys[(L.mask + 1) * ev.nk() + k] = kv[k];
+    rowAtomicCombine(ev, row, x);
+    return;
+  }
+  u64 s = mix64(kw) & L.mask;
+  for (int p = 0; p < L.probeLimit; ++p) {
+    u64* row = L.table + s * rw;
+    u64 prev = *(volatile u64*)row;
+    if (prev == kEmpty) {
+      prev = atomicCAS(row, kEmpty, kw);
+      if (prev == kEmpty) {
+        if (ev.nk() > 1)
+          for (int k = 0; k < ev.nk(); ++k) L.tkeys[s * ev.nk() + k] = kv[k];
+        const u64 c = atomicAdd(L.count, 1ull) + 1;
+        if (c * 10 > (L.mask + 1) * 7) L.err[1] = 1;  // fuller than 70%: the caller retries bigger
+        prev = kw;
+      }
+    }
+    if (prev == kw) {
+      rowAtomicCombine(ev, row, x);
+      return;
+    }
+    s = (s + 1) & L.mask;
+  }
+  L.err[1] = 1;  // no free slot within the probe limit
+}
+
+// Rows are pre-aggregated in a per-CTA shared-memory table (smemSlots rows, bounded probing), which
+// absorbs hot keys; a row that finds no slot goes to the global table directly.  The shared table is
+// merged into the global table when the CTA finishes.
+template <class Ev>
+__device__ void aggHash(const Launch& L) {
+  extern __shared__ __align__(16) u64 wsSmem[];
+  Ev ev(L);
+  const int rw = ev.rowWords();
+  const int S = L.smemSlots;
+  for (int s = threadIdx.x; s < S; s += blockDim.x) {
+    u64* row = wsSmem + (size_t)s * rw;
+    rowIdentity(ev, row);
+    row[0] = kEmpty;
+  }
+  double* skv = (double*)(wsSmem + (size_t)S * rw);  // [S][nk] key values of multi-key groups
+  __syncthreads();
+  forEachRow(L, ev, [&](int i, int, i64) {
+    double kv[Ev::NK];
+    const u64 kw = keyWord(ev, i, kv);
+    u64 x[kMaxRowWords];
+    rowOfInput(ev, i, x);
+    if (kw != kEmpty && S > 0) {
+      unsigned s = (unsigned)(mix64(kw) & (u64)(S - 1));
+#pragma unroll 1
+      for (int p = 0; p < 8; ++p) {
+        u64* row = wsSmem + (size_t)s * rw;
+        u64 prev = row[0];
+        if (prev == kEmpty) {
+          prev = atomicCAS(row, kEmpty, kw);
+          if (prev == kEmpty) {
+            if (ev.nk() > 1)
+              for (int k = 0; k < ev.nk(); ++k) skv[(size_t)s * ev.nk() + k] = kv[k];
+            prev = kw;
+          }
+        }
+        if (prev == kw) {
+          rowAtomicCombine(ev, row, x);
+          return;
+        }
+        s = (s + 1) & (S - 1);
+      }
+    }
+    globalInsert(L, ev, kw, kv, x);
+  });
+  __syncthreads();
+  for (int s = threadIdx.x; s < S; s += blockDim.x) {
+    const u64* row = wsSmem + (size_t)s * rw;
+    if (row[0] == kEmpty) continue;
+    double kv[WS_MAX_KEYS];
+    if (ev.nk() > 1)
+      for (int k = 0; k < ev.nk(); ++k) kv[k] = skv[(size_t)s * ev.nk() + k];
+    else
+      kv[0] = __longlong_as_double((i64)row[0]);
+    globalInsert(L, ev, row[0], kv, row);
+  }
+}
+
+// ------------------------------------------------------------------ selection
+// Pass 1: selected rows per tile.  Pass 2 (after an exclusive scan of the tile counts): each warp
+// ranks its rows with ballot / popc and writes ascending global row indices.
+template <class Ev>
+__device__ void selectCount(const Launch& L) {
+  __shared__ int wcount[kThreads / 32];
+  Ev ev(L);
+  int b = 0, bound = -1;
+  for (i64 t = blockIdx.x; t < L.ntiles; t += gridDim.x) {
+    while (t >= __ldg(L.tileStart + b + 1)) ++b;
+    if (b != bound) {
+      ev.bind(L, b);
+      bound = b;
+    }
+    const i64 n = __ldg(L.n + b);
+    const i64 r0 = (t - __ldg(L.tileStart + b)) * kTile + threadIdx.x * 4;
+    int c = 0;
+    if (r0 < n) {
+      const int nv = n - r0 >= 4 ? 4 : (int)(n - r0);
+      ev.load(r0, ev.fastOk && nv == 4, nv);
+      unsigned live = (1u << nv) - 1;
+      const uint32_t* del = L.del[b];
+      if (del) live &= ~(__ldg(del + (r0 >> 5)) >> (r0 & 31)) & 0xfu;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) c += ((live >> i) & 1u) && ev.where(i);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0) wcount[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int s = 0;
+      for (int w = 0; w < kThreads / 32; ++w) s += wcount[w];
+      L.tileCount[t] = s;
+    }
+    __syncthreads();
+  }
+}
+
+template <class Ev>
+__device__ void selectWrite(const Launch& L) {
+  __shared__ int woff[kThreads / 32];
+  Ev ev(L);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int b = 0, bound = -1;
+  for (i64 t = blockIdx.x; t < L.ntiles; t += gridDim.x) {
+    while (t >= __ldg(L.tileStart + b + 1)) ++b;
+    if (b != bound) {
+      ev.bind(L, b);
+      bound = b;
+    }
+    const i64 n = __ldg(L.n + b);
+    const i64 r0 = (t - __ldg(L.tileStart + b)) * kTile + threadIdx.x * 4;
+    unsigned sel = 0;
+    if (r0 < n) {
+      const int nv = n - r0 >= 4 ? 4 : (int)(n - r0);
+      ev.load(r0, ev.fastOk && nv == 4, nv);
+      unsigned live = (1u << nv) - 1;
+      const uint32_t* del = L.del[b];
+      if (del) live &= ~(__ldg(del + (r0 >> 5)) >> (r0 & 31)) & 0xfu;
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        if (((live >> i) & 1u) && ev.where(i)) sel |= 1u << i;
+    }
+    // rank = selected rows of lower lanes (ballot per row position) + own earlier rows
+    const unsigned lower = (1u << lane) - 1;
+    int before = 0, total = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const unsigned m = __ballot_sync(0xffffffffu, (sel >> i) & 1u);
+      before += __popc(m & lower);
+      total += __popc(m);
+    }
+    if (lane == 0) woff[warp] = total;
+    __syncthreads();
+    int base = 0;
+    for (int w = 0; w < warp; ++w) base += woff[w];
+    const i64 out0 = L.tileCount[t] + base + before;
+    const i64 g0 = __ldg(L.rowStart + b) + r0;
+    int k = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+      if ((sel >> i) & 1u) L.outIdx[out0 + k++] = (int32_t)(g0 + i);
+    __syncthreads();
+  }
+}
+
+}  // namespace ws
+
+// Kernel entry points (extern "C" names so generated modules can be looked up by name).  The Launch
+// descriptor is a __grid_constant__ parameter: the evaluator keeps a reference to it without forcing a
+// per-thread copy.
+#define WS_K_ENTRY(PREFIX, NAME, BODY)                                                                    \
+  extern "C" __global__ void __launch_bounds__(ws::kThreads) PREFIX##_##NAME(const __grid_constant__ ws::Launch L) { \
+    BODY(L);                                                                                               \
+  }
+#define WS_K_NOKEYS(EV, PREFIX) WS_K_ENTRY(PREFIX, nokeys, ws::aggNoKeys<EV>)
+#define WS_K_DENSE_SHARED(EV, PREFIX) WS_K_ENTRY(PREFIX, dense_shared, ws::aggDenseShared<EV>)
+#define WS_K_DENSE_GLOBAL(EV, PREFIX) WS_K_ENTRY(PREFIX, dense_global, ws::aggDenseGlobal<EV>)
+#define WS_K_HASH(EV, PREFIX) WS_K_ENTRY(PREFIX, hash, ws::aggHash<EV>)
+#define WS_K_SELECT_COUNT(EV, PREFIX) WS_K_ENTRY(PREFIX, select_count, ws::selectCount<EV>)
+#define WS_K_SELECT_WRITE(EV, PREFIX) WS_K_ENTRY(PREFIX, select_write, ws::selectWrite<EV>)
+#define WS_DEFINE_SCAN_KERNELS(EV, PREFIX) \
+  WS_K_NOKEYS(EV, PREFIX)                  \
+  WS_K_DENSE_SHARED(EV, PREFIX)            \
+  WS_K_DENSE_GLOBAL(EV, PREFIX)            \
+  WS_K_HASH(EV, PREFIX)                    \
+  WS_K_SELECT_COUNT(EV, PREFIX)            \
+  WS_K_SELECT_WRITE(EV, PREFIX)

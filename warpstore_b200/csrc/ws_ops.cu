@@ -1,0 +1,725 @@
+// Operators of libwarpstore_b200: aggregation (GpuAggregator), selection, gathers and hash joins
+// (reference: src/gpu.cu:393-800, :1089-1316).  Scan kernels come from ws_kern.cuh, instantiated here
+// with the interpreter and per plan by the code generator; the helper kernels below are plain CUDA.
+#include <cstring>
+
+#include "ws_internal.h"
+#include "ws_interp.cuh"
+
+// Interpreter instantiations of every scan kernel (prefix wsi).
+WS_DEFINE_SCAN_KERNELS(ws::InterpEv, wsi)
+
+namespace ws {
+
+const KernelSet& interpKernels() {
+  static KernelSet ks = [] {
+    KernelSet k;
+    const void* syms[K_COUNT_] = {(const void*)wsi_nokeys, (const void*)wsi_dense_shared, (const void*)wsi_dense_global,
+                                  (const void*)wsi_hash, (const void*)wsi_select_count, (const void*)wsi_select_write};
+    for (int i = 0; i < K_COUNT_; ++i) {
+      cudaFunction_t f;
+      WS_CK(cudaGetFuncBySymbol(&f, syms[i]));
+      k.fn[i] = (CUfunction)f;
+    }
+    k.interp = true;
+    return k;
+  }();
+  return ks;
+}
+
+namespace {
+
+int gridFor(int64_t n, int block = 256, int perSm = 8) {
+  int64_t g = (n + block - 1) / block;
+  const int64_t cap = (int64_t)smCount() * perSm;
+  if (g > cap) g = cap;
+  return (int)(g < 1 ? 1 : g);
+}
+#define WS_LAUNCH(kernel, grid, block, smem, ...)                 \
+  do {                                                            \
+    kernel<<<(grid), (block), (smem), stream()>>>(__VA_ARGS__);   \
+    WS_CK(cudaGetLastError());                                    \
+    countLaunch();                                                \
+  } while (0)
+
+// ---------------------------------------------------------------- helper kernels
+}  // namespace
+// Identity values of one accumulator row (by value as a kernel parameter).
+struct RowTemplate {
+  u64 w[kMaxRowWords];
+};
+namespace {
+__global__ void kFillRows(u64* rows, int64_t nrows, int rw, RowTemplate t, int64_t emptyRows) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nrows; i += (int64_t)gridDim.x * blockDim.x) {
+    u64* r = rows + i * rw;
+    for (int j = 1; j < rw; ++j) r[j] = t.w[j];
+    r[0] = i < emptyRows ? kEmpty : 0ull;
+  }
+}
+
+// Exclusive scan of n counts in place (one CTA); counts[n] receives the total.
+__global__ void kScanExclusive(int64_t* counts, int64_t n) {
+  __shared__ int64_t part[1024];
+  const int t = threadIdx.x, T = blockDim.x;
+  const int64_t per = (n + T - 1) / T;
+  const int64_t lo = min((int64_t)t * per, n), hi = min(lo + per, n);
+  int64_t s = 0;
+  for (int64_t i = lo; i < hi; ++i) s += counts[i];
+  part[t] = s;
+  __syncthreads();
+  for (int off = 1; off < T; off <<= 1) {  // Hillis-Steele inclusive scan of the thread sums
+    const int64_t v = t >= off ? part[t - off] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  int64_t run = t ? part[t - 1] : 0;
+  for (int64_t i = lo; i < hi; ++i) {
+    const int64_t c = counts[i];
+    counts[i] = run;
+    run += c;
+  }
+  if (t == T - 1) counts[n] = part[T - 1];
+}
+
+__global__ void kGatherI64(const int64_t* src, const int64_t* idx, int n, int64_t* dst) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = src[idx[i]];
+}
+
+// Occupied result rows: hash rows [0, cap) by their key word, the extra row (cap) by its claim flag,
+// dense rows by slot 0 (COUNT(*)) being non-zero.
+struct OccSpec {
+  int rw, mode;  // mode 1 dense, 2 hash
+  int cnt0;      // word of slot 0
+  int64_t cap;   // hash: index of the extra row
+};
+__device__ __forceinline__ bool occupied(const u64* rows, int64_t i, const OccSpec& s) {
+  const u64* r = rows + i * s.rw;
+  if (s.mode == 1) return r[s.cnt0] != 0;
+  if (i == s.cap) return r[0] != 0;
+  return r[0] != kEmpty;
+}
+constexpr int kOccChunk = 2048;
+__global__ void kOccCount(const u64* rows, int64_t nrows, OccSpec s, int64_t* counts) {
+  __shared__ int wc[32];
+  const int64_t c0 = (int64_t)blockIdx.x * kOccChunk;
+  int c = 0;
+  for (int64_t i = c0 + threadIdx.x; i < min(c0 + kOccChunk, nrows); i += blockDim.x) c += occupied(rows, i, s);
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0) wc[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += wc[w];
+    counts[blockIdx.x] = t;
+  }
+}
+__global__ void kOccWrite(const u64* rows, int64_t nrows, OccSpec s, const int64_t* offs, int64_t* idx) {
+  __shared__ int wbase[32];
+  __shared__ int64_t run;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int64_t c0 = (int64_t)blockIdx.x * kOccChunk;
+  if (threadIdx.x == 0) run = offs[blockIdx.x];
+  __syncthreads();
+  for (int64_t b = c0; b < min(c0 + kOccChunk, nrows); b += blockDim.x) {
+    const int64_t i = b + threadIdx.x;
+    const bool occ = i < nrows && i < c0 + kOccChunk && occupied(rows, i, s);
+    const unsigned m = __ballot_sync(0xffffffffu, occ);
+    if (lane == 0) wbase[warp] = __popc(m);
+    __syncthreads();
+    int before = 0, total = 0;
+    for (int w = 0; w < nw; ++w) {
+      if (w < warp) before += wbase[w];
+      total += wbase[w];
+    }
+    if (occ) idx[run + before + __popc(m & ((1u << lane) - 1))] = i;
+    __syncthreads();
+    if (threadIdx.x == 0) run += total;
+    __syncthreads();
+  }
+}
+
+// Result rows -> keys (engine format) and exact words per group.
+struct EmitSpec {
+  int nk, na, rw, mode;  // mode 0 no keys, 1 dense, 2 hash
+  uint8_t kind[WS_MAX_AGGS];
+  int16_t woff[WS_MAX_AGGS];
+  int16_t partner[WS_MAX_AGGS];
+  uint8_t keyInt[WS_MAX_KEYS];
+  int64_t kmin[WS_MAX_KEYS], range[WS_MAX_KEYS], stride[WS_MAX_KEYS];
+  const double* tkeys;
+  int64_t cap;
+};
+__global__ void kEmit(const u64* rows, const int64_t* idx, int64_t m, EmitSpec s, double* keys, int64_t* exact,
+                      int colMajor) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < m; j += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = idx ? idx[j] : j;
+    const u64* r = rows + i * s.rw;
+    for (int k = 0; k < s.nk; ++k) {
+      double kv;
+      if (s.mode == 1) {
+        const long long v = s.kmin[k] + (i / s.stride[k]) % s.range[k];
+        kv = s.keyInt[k] ? __longlong_as_double(v) : (double)v;
+      } else if (s.nk == 1 && i != s.cap) {
+        kv = __longlong_as_double((long long)r[0]);
+      } else {
+        kv = s.tkeys[i * s.nk + k];
+      }
+      keys[colMajor ? k * m + j : j * s.nk + k] = kv;
+    }
+    for (int a = 0; a < s.na; ++a) {
+      const int src = s.kind[a] == SK_NONE ? s.partner[a] : a;
+      const int o = s.woff[src];
+      long long w0 = (long long)r[o], w1 = 0;
+      const uint8_t k = s.kind[src];
+      if (k == SK_ISUM) w1 = (long long)r[o + 1];
+      else if (k == SK_DMIN || k == SK_DMAX) w0 = __double_as_longlong(dunord(w0));
+      exact[(j * s.na + a) * 2] = w0;
+      exact[(j * s.na + a) * 2 + 1] = w1;
+    }
+  }
+}
+
+// Exact words -> the engine's double slot format, on the device (for compact()).
+struct DblSpec {
+  int na, nokeys;
+  uint8_t kind[WS_MAX_AGGS], aggBits[WS_MAX_AGGS], aggPart[WS_MAX_AGGS];
+};
+__device__ __host__ inline double bitsToD(long long v) {
+  double d;
+  memcpy(&d, &v, 8);
+  return d;
+}
+__device__ __host__ inline double slotDouble(const DblSpec& s, int a, long long w0, long long w1, bool srcIsNone,
+                                             uint8_t srcKind) {
+  const uint8_t k = srcKind;
+  if (k == SK_COUNT) return (double)w0;
+  if (k == SK_ISUM) {
+    const __int128 T = (__int128)(((unsigned __int128)(unsigned long long)w1 << 64) | (unsigned long long)w0);
+    if (s.nokeys) {
+      long long lo = w0;
+      double d;
+      memcpy(&d, &lo, 8);
+      return d;
+    }
+    if (s.aggBits[a]) {
+      long long v = s.aggPart[a] == 2 || srcIsNone ? (long long)(T >> 32) : s.aggPart[a] == 1 ? (long long)(T & 0xffffffff) : w0;
+      double d;
+      memcpy(&d, &v, 8);
+      return d;
+    }
+    return (double)T;
+  }
+  if (k == SK_IMIN || k == SK_IMAX) {
+    if (s.nokeys || s.aggBits[a]) {
+      double d;
+      memcpy(&d, &w0, 8);
+      return d;
+    }
+    if (k == SK_IMIN && w0 == 0x7fffffffffffffffll) return bitsToD(0x7ff0000000000000ll);
+    if (k == SK_IMAX && w0 == (long long)0x8000000000000000ull) return bitsToD((long long)0xfff0000000000000ull);
+    return (double)w0;
+  }
+  double d;
+  memcpy(&d, &w0, 8);
+  return d;
+}
+__global__ void kExactToDouble(const int64_t* exact, int64_t m, DblSpec s, const int16_t* partnerKinds, double* accs) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < m; j += (int64_t)gridDim.x * blockDim.x)
+    for (int a = 0; a < s.na; ++a) {
+      const bool none = s.kind[a] == SK_NONE;
+      const uint8_t sk = none ? (uint8_t)partnerKinds[a] : s.kind[a];
+      accs[a * m + j] = slotDouble(s, a, exact[(j * s.na + a) * 2], exact[(j * s.na + a) * 2 + 1], none, sk);
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- batch descriptor
+// Device copy of the batches of one launch: [cols nb*ncols][n nb][del nb][tileStart nb+1][rowStart nb+1]
+// followed, for interpreted plans, by the typed programs and slot tables.
+struct BatchDesc {
+  DBuf<uint8_t> buf;
+  int64_t ntiles = 0, rows = 0;
+  const ws_col_view* cols = nullptr;
+  const int64_t* n = nullptr;
+  const uint32_t* const* del = nullptr;
+  const int64_t* tileStart = nullptr;
+  const int64_t* rowStart = nullptr;
+  const TProgs* progs = nullptr;
+  const uint8_t* kinds = nullptr;
+  const int* woff = nullptr;
+  const uint8_t* aggNull = nullptr;
+  const uint8_t* keyInt = nullptr;
+};
+
+static BatchDesc uploadBatches(int nb, int ncols, const int64_t* bn, const uint32_t* const* bdel, const ws_col_view* bcols,
+                               const TProgs* progs, const SlotLayout* lay, const ws_agg_plan* plan) {
+  BatchDesc d;
+  const size_t colBytes = (size_t)nb * ncols * sizeof(ws_col_view);
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t o = (off + 15) & ~(size_t)15;
+    off = o + bytes;
+    return o;
+  };
+  const size_t oCols = take(colBytes), oN = take(8 * nb), oDel = take(8 * nb), oTile = take(8 * (nb + 1)),
+               oRow = take(8 * (nb + 1));
+  size_t oProg = 0, oKinds = 0, oWoff = 0, oNull = 0, oKeyInt = 0;
+  if (progs) {
+    oProg = take(sizeof(TProgs));
+    oKinds = take(WS_MAX_AGGS);
+    oWoff = take(4 * WS_MAX_AGGS);
+    oNull = take(WS_MAX_AGGS);
+    oKeyInt = take(WS_MAX_KEYS);
+  }
+  uint8_t* st = pinnedStage(off);
+  memcpy(st + oCols, bcols, colBytes);
+  int64_t* n = (int64_t*)(st + oN);
+  const uint32_t** del = (const uint32_t**)(st + oDel);
+  int64_t* ts = (int64_t*)(st + oTile);
+  int64_t* rs = (int64_t*)(st + oRow);
+  ts[0] = 0;
+  rs[0] = 0;
+  for (int b = 0; b < nb; ++b) {
+    n[b] = bn[b];
+    del[b] = bdel ? bdel[b] : nullptr;
+    ts[b + 1] = ts[b] + (bn[b] + kTile - 1) / kTile;
+    rs[b + 1] = rs[b] + bn[b];
+  }
+  d.ntiles = ts[nb];
+  d.rows = rs[nb];
+  if (progs) {
+    memcpy(st + oProg, progs, sizeof(TProgs));
+    memcpy(st + oKinds, lay->kind, WS_MAX_AGGS);
+    memcpy(st + oWoff, lay->woff, 4 * WS_MAX_AGGS);
+    memcpy(st + oNull, plan->aggNull, WS_MAX_AGGS);
+    memcpy(st + oKeyInt, plan->keyInt, WS_MAX_KEYS);
+  }
+  d.buf = DBuf<uint8_t>((int64_t)off);
+  h2dAsync(d.buf.p, st, off);
+  stageCopied();
+  uint8_t* p = d.buf.p;
+  d.cols = (const ws_col_view*)(p + oCols);
+  d.n = (const int64_t*)(p + oN);
+  d.del = (const uint32_t* const*)(p + oDel);
+  d.tileStart = (const int64_t*)(p + oTile);
+  d.rowStart = (const int64_t*)(p + oRow);
+  if (progs) {
+    d.progs = (const TProgs*)(p + oProg);
+    d.kinds = p + oKinds;
+    d.woff = (const int*)(p + oWoff);
+    d.aggNull = p + oNull;
+    d.keyInt = p + oKeyInt;
+  }
+  return d;
+}
+
+static void fillLaunch(Launch& L, const BatchDesc& d, int nb, int ncols, const ws_expr_env& env, const ws_agg_plan* plan,
+                       const SlotLayout* lay) {
+  memset(&L, 0, sizeof L);
+  L.cols = d.cols;
+  L.n = (const i64*)d.n;
+  L.del = d.del;
+  L.tileStart = (const i64*)d.tileStart;
+  L.rowStart = (const i64*)d.rowStart;
+  L.nb = nb;
+  L.ncols = ncols;
+  L.ntiles = d.ntiles;
+  L.env = envK(env);
+  L.progs = d.progs;
+  L.kinds = d.kinds;
+  L.woff = d.woff;
+  L.aggNull = d.aggNull;
+  L.keyInt = d.keyInt;
+  if (plan) {
+    L.nkeys = plan->nkeys;
+    L.naggs = plan->naggs;
+  }
+  if (lay) L.rowWords = lay->rw;
+}
+
+// A compiled plan can only run batches whose columns it was generated for: one generated for raw
+// columns cannot decode an encoded segment (the engine's hint, env.cols[c].enc, says which may be).
+static bool planCovers(const ws_expr_env& env, int nb, int ncols, const ws_col_view* bcols) {
+  for (int b = 0; b < nb; ++b)
+    for (int c = 0; c < ncols; ++c)
+      if (bcols[(int64_t)b * ncols + c].enc && !env.cols[c].enc) return false;
+  return true;
+}
+
+}  // namespace ws
+
+using namespace ws;
+
+// ================================================================ aggregation
+struct ws_aggregator {
+  ws_agg_plan plan{};
+  ws_dense_spec dense{};
+  bool isDense = false;
+  SlotLayout lay;
+  int64_t cap = 1;  // hash rows (power of two) / dense groups / 1
+  int ncols = 0;
+  std::vector<int64_t> bn;
+  std::vector<const uint32_t*> bdel;
+  std::vector<ws_col_view> bcols;
+  int64_t rowsDone = 0;
+  int batchesDone = 0, windows = 0;
+  DBuf<u64> rows;
+  DBuf<double> tkeys;
+  DBuf<uint8_t> ctl;  // [count u64][err int x2][ticket]
+  bool fetched = false;
+  std::vector<int64_t> hi;
+  int64_t lastGroups = -1;
+
+  u64* count() { return (u64*)ctl.p; }
+  int* err() { return (int*)(ctl.p + 8); }
+  unsigned* ticket() { return (unsigned*)(ctl.p + 16); }
+  int64_t nrows() const { return isDense ? dense.G : plan.nkeys ? cap + 1 : 1; }
+};
+
+namespace ws {
+
+static RowTemplate rowTemplate(const SlotLayout& lay) {
+  RowTemplate t{};
+  for (int a = 0; a < lay.na; ++a) {
+    const int o = lay.woff[a];
+    switch (lay.kind[a]) {
+      case SK_IMIN: t.w[o] = (u64)0x7fffffffffffffffll; break;
+      case SK_IMAX: t.w[o] = (u64)0x8000000000000000ll; break;
+      case SK_DMIN: {
+        double inf = __builtin_inf();
+        long long b;
+        memcpy(&b, &inf, 8);
+        t.w[o] = (u64)(b >= 0 ? b : (b ^ 0x7fffffffffffffffll));
+        break;
+      }
+      case SK_DMAX: {
+        double inf = -__builtin_inf();
+        long long b;
+        memcpy(&b, &inf, 8);
+        t.w[o] = (u64)(b >= 0 ? b : (b ^ 0x7fffffffffffffffll));
+        break;
+      }
+      default: break;
+    }
+  }
+  return t;
+}
+
+static void aggInitRows(ws_aggregator& A) {
+  const int64_t nr = A.nrows();
+  A.rows = DBuf<u64>(nr * A.lay.rw);
+  const int64_t emptyRows = A.plan.nkeys && !A.isDense ? A.cap : 0;
+  WS_LAUNCH(kFillRows, gridFor(nr), 256, 0, A.rows.p, nr, A.lay.rw, rowTemplate(A.lay), emptyRows);
+  if (A.plan.nkeys && !A.isDense) {
+    A.tkeys = DBuf<double>((A.cap + 1) * std::max(A.plan.nkeys, 1));
+  }
+  A.ctl = DBuf<uint8_t>(32);
+  WS_CK(cudaMemsetAsync(A.ctl.p, 0, 32, stream()));
+}
+
+static size_t hashSmemSlots(const ws_aggregator& A, size_t budget) {
+  const size_t per = (size_t)A.lay.rw * 8 + (A.plan.nkeys > 1 ? (size_t)A.plan.nkeys * 8 : 0);
+  size_t s = 4096;
+  while (s > 64 && s * per > budget) s >>= 1;
+  return s * per > budget ? 0 : s;
+}
+
+static void aggRun(ws_aggregator& A, const ws_expr_env& env, const ws_jit_program* jit) {
+  const int nb = (int)A.bn.size();
+  if (nb == 0) return;
+  A.fetched = false;
+  A.lastGroups = -1;
+  const bool useJit = jit && jit->state.load() == 1 && planCovers(env, nb, A.ncols, A.bcols.data());
+  if (!useJit && (A.plan.naggs > WS_INTERP_AGGS || A.plan.nkeys > WS_INTERP_KEYS))
+    throw Error("this aggregation needs a compiled plan (more than 16 aggregates or 4 GROUP BY keys); codegen failed or is off", WS_ERR_PLAN);
+  std::unique_ptr<TProgs> progs;
+  if (!useJit) {
+    progs.reset(new TProgs);
+    buildTProgs(env, A.ncols, A.plan, A.plan.hasWhere, *progs);
+  }
+  BatchDesc d = uploadBatches(nb, A.ncols, A.bn.data(), A.bdel.data(), A.bcols.data(), progs.get(), &A.lay, &A.plan);
+  if (d.ntiles == 0) return;
+  Launch L;
+  fillLaunch(L, d, nb, A.ncols, env, &A.plan, &A.lay);
+  L.rows = A.rows.p;
+  L.err = A.err();
+  L.ticket = A.ticket();
+  const KernelSet& ks = useJit ? jit->kernels : interpKernels();
+  if (A.plan.nkeys == 0) {
+    CUfunction f = ks.fn[K_NOKEYS];
+    if (!f) throw Error("compiled plan has no aggregation kernel", WS_ERR_INTERNAL);
+    const unsigned grid = persistentGrid(f, 0, d.ntiles);
+    DBuf<u64> part((int64_t)grid * A.lay.rw);
+    L.part = part.p;
+    WS_CK(cudaMemsetAsync(A.ticket(), 0, 4, stream()));
+    launchScan(f, grid, 0, L);
+    return;
+  }
+  if (A.isDense) {
+    for (int k = 0; k < A.plan.nkeys; ++k) {
+      L.kmin[k] = A.dense.kmin[k];
+      L.range[k] = A.dense.range[k];
+      L.stride[k] = A.dense.stride[k];
+    }
+    L.G = A.dense.G;
+    const int64_t G = A.dense.G;
+    if (useJit && G <= 32 && G <= denseRegMaxGroups(A.plan)) {
+      CUfunction f = denseRegKernel(const_cast<ws_jit_program*>(jit), (int)G);
+      if (f) {
+        const unsigned grid = persistentGrid(f, 0, d.ntiles);
+        DBuf<u64> part((int64_t)grid * G * A.lay.rw);
+        L.part = part.p;
+        WS_CK(cudaMemsetAsync(A.ticket(), 0, 4, stream()));
+        launchScan(f, grid, 0, L);
+        return;
+      }
+    }
+    const size_t smem = (size_t)G * A.lay.rw * 8;
+    if (smem <= 96 * 1024 && ks.fn[K_DENSE_SHARED]) {
+      CUfunction f = ks.fn[K_DENSE_SHARED];
+      launchScan(f, persistentGrid(f, smem, d.ntiles), smem, L);
+    } else {
+      CUfunction f = ks.fn[K_DENSE_GLOBAL];
+      if (!f) throw Error("compiled plan has no dense kernel", WS_ERR_INTERNAL);
+      launchScan(f, persistentGrid(f, 0, d.ntiles), 0, L);
+    }
+    return;
+  }
+  CUfunction f = ks.fn[K_HASH];
+  if (!f) throw Error("compiled plan has no hash aggregation kernel", WS_ERR_INTERNAL);
+  L.table = A.rows.p;
+  L.tkeys = A.tkeys.p;
+  L.mask = (u64)(A.cap - 1);
+  L.count = A.count();
+  L.probeLimit = (int)std::min<int64_t>(A.cap, 1 << 16);
+  const size_t slots = hashSmemSlots(A, 64 * 1024);
+  L.smemSlots = (int)slots;
+  const size_t smem = slots * ((size_t)A.lay.rw * 8 + (A.plan.nkeys > 1 ? (size_t)A.plan.nkeys * 8 : 0));
+  launchScan(f, persistentGrid(f, smem, d.ntiles), smem, L);
+}
+
+// Occupied row indices of the result rows (ascending), on the device; returns the count.
+static int64_t aggCompactIdx(ws_aggregator& A, DBuf<int64_t>& idx) {
+  const int64_t nr = A.nrows();
+  OccSpec s{A.lay.rw, A.isDense ? 1 : 2, A.lay.woff[0], A.cap};
+  const int64_t nchunks = (nr + kOccChunk - 1) / kOccChunk;
+  DBuf<int64_t> counts(nchunks + 1);
+  WS_LAUNCH(kOccCount, (unsigned)nchunks, 256, 0, A.rows.p, nr, s, counts.p);
+  WS_LAUNCH(kScanExclusive, 1, 1024, 0, counts.p, nchunks);
+  int64_t g = 0;
+  d2hSync(&g, counts.p + nchunks, 8);
+  idx = DBuf<int64_t>(std::max<int64_t>(g, 1));
+  if (g) WS_LAUNCH(kOccWrite, (unsigned)nchunks, 256, 0, A.rows.p, nr, s, counts.p, idx.p);
+  return g;
+}
+
+static EmitSpec emitSpec(const ws_aggregator& A) {
+  EmitSpec s{};
+  s.nk = A.plan.nkeys;
+  s.na = A.plan.naggs;
+  s.rw = A.lay.rw;
+  s.mode = A.plan.nkeys == 0 ? 0 : A.isDense ? 1 : 2;
+  for (int a = 0; a < s.na; ++a) {
+    s.kind[a] = A.lay.kind[a];
+    s.woff[a] = (int16_t)A.lay.woff[a];
+    s.partner[a] = (int16_t)A.lay.partner[a];
+  }
+  for (int k = 0; k < s.nk; ++k) {
+    s.keyInt[k] = A.plan.keyInt[k];
+    s.kmin[k] = A.dense.kmin[k];
+    s.range[k] = A.isDense ? A.dense.range[k] : 1;
+    s.stride[k] = A.isDense ? A.dense.stride[k] : 1;
+  }
+  s.tkeys = A.tkeys.p;
+  s.cap = A.cap;
+  return s;
+}
+
+static DblSpec dblSpec(const ws_aggregator& A) {
+  DblSpec s{};
+  s.na = A.plan.naggs;
+  s.nokeys = A.plan.nkeys == 0;
+  for (int a = 0; a < s.na; ++a) {
+    s.kind[a] = A.lay.kind[a];
+    s.aggBits[a] = A.plan.aggBits[a];
+    s.aggPart[a] = A.plan.aggPart[a];
+  }
+  return s;
+}
+
+static void checkFlags(ws_aggregator& A, bool* overflow) {
+  int e[2] = {0, 0};
+  d2hSync(e, A.err(), 8);
+  if (e[0]) throw Error("dense GROUP BY key outside its declared range", WS_ERR_RANGE);
+  if (overflow) *overflow = e[1] != 0;
+}
+
+}  // namespace ws
+
+extern "C" {
+
+int ws_agg_create(const ws_agg_plan* plan, int64_t capacity, const ws_dense_spec* dense, ws_aggregator** out) {
+  return guardedCall([&] {
+    *out = nullptr;
+    std::unique_ptr<ws_aggregator> A(new ws_aggregator);
+    A->plan = *plan;
+    A->lay = layoutOf(*plan);
+    if (dense && dense->G > 0 && plan->nkeys) {
+      A->dense = *dense;
+      A->isDense = true;
+      A->cap = dense->G;
+    } else if (plan->nkeys) {
+      int64_t c = 1;
+      while (c < capacity) c <<= 1;
+      A->cap = std::max<int64_t>(c, 2);
+    } else {
+      A->cap = 1;
+    }
+    aggInitRows(*A);
+    *out = A.release();
+  });
+}
+
+void ws_agg_destroy(ws_aggregator* agg) { delete agg; }
+
+int ws_agg_add_batch(ws_aggregator* A, const ws_expr_env* env, int ncols, int64_t n, const uint32_t* del) {
+  return guardedCall([&] {
+    if (n <= 0) return;
+    if (ncols < 0 || ncols > WS_MAX_COLS) throw Error("bad column count", WS_ERR_ARG);
+    if (!A->bn.empty() && ncols != A->ncols) throw Error("batches must have the same column count", WS_ERR_ARG);
+    A->ncols = ncols;
+    A->bn.push_back(n);
+    A->bdel.push_back(del);
+    for (int i = 0; i < ncols; ++i) A->bcols.push_back(env->cols[i]);
+  });
+}
+
+int ws_agg_run(ws_aggregator* A, const ws_expr_env* env, const ws_jit_program* jit) {
+  return guardedCall([&] { aggRun(*A, *env, jit); });
+}
+
+int ws_agg_run_window(ws_aggregator* A, const ws_expr_env* env, const ws_jit_program* jit) {
+  return guardedCall([&] {
+    if (A->bn.empty()) return;
+    aggRun(*A, *env, jit);
+    ++A->windows;
+    for (int64_t n : A->bn) A->rowsDone += n;
+    A->batchesDone += (int)A->bn.size();
+    A->bn.clear();
+    A->bdel.clear();
+    A->bcols.clear();
+  });
+}
+
+int ws_agg_batches(const ws_aggregator* A) { return A->batchesDone + (int)A->bn.size(); }
+int ws_agg_windows(const ws_aggregator* A) { return A->windows; }
+int64_t ws_agg_rows_in(const ws_aggregator* A) {
+  int64_t r = A->rowsDone;
+  for (int64_t n : A->bn) r += n;
+  return r;
+}
+int ws_agg_is_dense(const ws_aggregator* A) { return A->isDense ? 1 : 0; }
+int64_t ws_agg_capacity(const ws_aggregator* A) { return A->cap; }
+
+int ws_agg_overflowed(ws_aggregator* A, int* out) {
+  return guardedCall([&] {
+    bool o = false;
+    checkFlags(*A, &o);
+    *out = A->plan.nkeys && !A->isDense && o ? 1 : 0;
+  });
+}
+
+int ws_agg_group_count(ws_aggregator* A, int64_t* out) {
+  return guardedCall([&] {
+    if (!A->plan.nkeys) {
+      *out = 1;
+      return;
+    }
+    if (A->isDense) {
+      DBuf<int64_t> idx;
+      *out = aggCompactIdx(*A, idx);
+      return;
+    }
+    u64 c = 0;
+    d2hSync(&c, A->count(), 8);
+    *out = (int64_t)c;
+  });
+}
+
+int ws_agg_fetch(ws_aggregator* A, int64_t max_groups, double* keys, double* accs, int64_t* exact, int64_t* ngroups) {
+  return guardedCall([&] {
+    checkFlags(*A, nullptr);
+    const int nk = A->plan.nkeys, na = A->plan.naggs;
+    DBuf<int64_t> idx;
+    const int64_t g = nk ? aggCompactIdx(*A, idx) : 1;
+    *ngroups = g;
+    if (g > max_groups) throw Error("output buffer too small for " + std::to_string(g) + " groups", WS_ERR_SIZE);
+    DBuf<double> dk(std::max<int64_t>(g * nk, 1));
+    DBuf<int64_t> dx(std::max<int64_t>(g * na * 2, 1));
+    if (g) WS_LAUNCH(kEmit, gridFor(g), 256, 0, A->rows.p, nk ? idx.p : nullptr, g, emitSpec(*A), dk.p, dx.p, 0);
+    std::vector<int64_t> ex((size_t)std::max<int64_t>(g * na * 2, 1));
+    if (nk && keys && g) {
+      WS_CK(cudaMemcpyAsync(keys, dk.p, sizeof(double) * g * nk, cudaMemcpyDeviceToHost, stream()));
+    }
+    if (g) WS_CK(cudaMemcpyAsync(ex.data(), dx.p, sizeof(int64_t) * g * na * 2, cudaMemcpyDeviceToHost, stream()));
+    sync();
+    if (exact && g) memcpy(exact, ex.data(), sizeof(int64_t) * g * na * 2);
+    const DblSpec s = dblSpec(*A);
+    A->hi.assign(na, 0);
+    if (accs)
+      for (int64_t j = 0; j < g; ++j)
+        for (int a = 0; a < na; ++a) {
+          const bool none = A->lay.kind[a] == SK_NONE;
+          const uint8_t sk = none ? A->lay.kind[A->lay.partner[a]] : A->lay.kind[a];
+          const long long w0 = ex[(j * na + a) * 2], w1 = ex[(j * na + a) * 2 + 1];
+          accs[j * na + a] = slotDouble(s, a, w0, w1, none, sk);
+        }
+    if (!nk)
+      for (int a = 0; a < na; ++a) {
+        const uint8_t k = A->lay.kind[a] == SK_NONE ? A->lay.kind[A->lay.partner[a]] : A->lay.kind[a];
+        A->hi[a] = k == SK_ISUM ? ex[a * 2 + 1] : 0;
+      }
+    A->fetched = true;
+  });
+}
+
+int ws_agg_sum_bits_slots(const ws_aggregator* A, uint8_t* out) {
+  for (int a = 0; a < A->plan.naggs; ++a) {
+    if (A->plan.nkeys) out[a] = A->plan.aggBits[a];
+    else
+      out[a] = (A->plan.ops[a] == WS_AGG_SUM || A->plan.ops[a] == WS_AGG_MIN || A->plan.ops[a] == WS_AGG_MAX) && A->plan.aggInt[a];
+  }
+  return WS_OK;
+}
+
+int ws_agg_sum_high(const ws_aggregator* A, int64_t* out) {
+  for (int a = 0; a < A->plan.naggs; ++a) out[a] = a < (int)A->hi.size() ? A->hi[a] : 0;
+  return WS_OK;
+}
+
+int ws_agg_compact(ws_aggregator* A, double** keys, double** accs, int64_t* ngroups) {
+  return guardedCall([&] {
+    checkFlags(*A, nullptr);
+    const int nk = A->plan.nkeys, na = A->plan.naggs;
+    DBuf<int64_t> idx;
+    const int64_t g = nk ? aggCompactIdx(*A, idx) : 1;
+    DBuf<double> dk(std::max<int64_t>(g * nk, 1)), da(std::max<int64_t>(g * na, 1));
+    DBuf<int64_t> dx(std::max<int64_t>(g * na * 2, 1));
+    DBuf<int16_t> pk(WS_MAX_AGGS);
+    if (g) {
+      WS_LAUNCH(kEmit, gridFor(g), 256, 0, A->rows.p, nk ? idx.p : nullptr, g, emitSpec(*A), dk.p, dx.p, 1);
+      int16_t* st = (int16_t*)pinnedStage(2 * WS_MAX_AGGS);
+      for (int a = 0; a < WS_MAX_AGGS; ++a) st[a] = a < na ? A->lay.kind[A->lay.partner[a]] : 0;
+      h2dAsync(pk.p, st, 2 * WS_MAX_AGGS);
+      stageCopied();
+      WS_LAUNCH(kExactToDouble, gridFor(g), 256, 0, dx.p, g, dblSpec(*A), pk.p, da.p);
+    }
+    *keys = dk.release();
+    *accs = da.release();
+    *ngroups = g;
+  });
+}
+
+}  // extern "C"

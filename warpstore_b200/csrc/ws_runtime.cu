@@ -1,0 +1,296 @@
+// Device runtime of libwarpstore_b200: initialisation, per-thread streams, the stream-ordered memory
+// pool, pinned staging, error reporting and the launch helpers (reference: src/gpu.cu:23-240).
+#include <cstdio>
+#include <cstring>
+
+#include "ws_internal.h"
+
+namespace ws {
+
+namespace {
+thread_local int tErrCode = 0;
+thread_local std::string tErrMsg;
+thread_local cudaStream_t tStream = nullptr;
+thread_local bool tStreamSet = false;
+std::once_flag gInitOnce;
+int gSms = 148, gArch = 100;
+std::atomic<int64_t> gLaunches{0};
+}  // namespace
+
+void setLastError(int code, const std::string& msg) {
+  tErrCode = code;
+  tErrMsg = msg;
+}
+
+void ck(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return;
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    throw Error("GPU out of memory", WS_ERR_OOM);
+  }
+  throw Error(std::string("CUDA error: ") + cudaGetErrorString(e) + " at " + what, WS_ERR_INTERNAL);
+}
+
+void ckDrv(CUresult r, const char* what) {
+  if (r == CUDA_SUCCESS) return;
+  const char* msg = nullptr;
+  if (drv().getErrorString) drv().getErrorString(r, &msg);
+  if (r == CUDA_ERROR_OUT_OF_MEMORY) throw Error("GPU out of memory", WS_ERR_OOM);
+  throw Error(std::string("CUDA driver error: ") + (msg ? msg : "?") + " at " + what, WS_ERR_INTERNAL);
+}
+
+void ensureInit() {
+  std::call_once(gInitOnce, [] {
+    int dev = 0;
+    WS_CK(cudaGetDevice(&dev));
+    cudaDeviceProp prop;
+    WS_CK(cudaGetDeviceProperties(&prop, dev));
+    gSms = prop.multiProcessorCount;
+    gArch = prop.major * 10 + prop.minor;
+    // Query temporaries come from the stream-ordered pool, which keeps freed memory for the next
+    // queries instead of returning it at every synchronization.
+    cudaMemPool_t pool;
+    WS_CK(cudaDeviceGetDefaultMemPool(&pool, dev));
+    uint64_t thresh = UINT64_MAX;
+    WS_CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thresh));
+    (void)drv();
+  });
+}
+
+const DriverApi& drv() {
+  static DriverApi api = [] {
+    DriverApi a{};
+    auto get = [](const char* name, void** fn) {
+      cudaDriverEntryPointQueryResult q;
+      if (cudaGetDriverEntryPoint(name, fn, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess) {
+        cudaGetLastError();
+        throw Error(std::string("CUDA driver entry point unavailable: ") + name, WS_ERR_INTERNAL);
+      }
+    };
+    get("cuModuleLoadData", (void**)&a.moduleLoadData);
+    get("cuModuleGetFunction", (void**)&a.moduleGetFunction);
+    get("cuLaunchKernel", (void**)&a.launchKernel);
+    get("cuFuncSetAttribute", (void**)&a.funcSetAttribute);
+    get("cuOccupancyMaxActiveBlocksPerMultiprocessor", (void**)&a.occupancy);
+    get("cuGetErrorString", (void**)&a.getErrorString);
+    return a;
+  }();
+  return api;
+}
+
+int smCount() {
+  ensureInit();
+  return gSms;
+}
+int arch() {
+  ensureInit();
+  return gArch;
+}
+
+cudaStream_t stream() { return tStreamSet ? tStream : cudaStreamPerThread; }
+void setStream(cudaStream_t s) {
+  tStream = s;
+  tStreamSet = s != nullptr;
+}
+
+static void trimPool() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) return;
+  cudaDeviceSynchronize();
+  cudaMemPoolTrimTo(pool, 0);
+  cudaGetLastError();
+}
+
+void* tmpAlloc(size_t bytes) {
+  if (!bytes) return nullptr;
+  ensureInit();
+  void* p = nullptr;
+  if (cudaMallocAsync(&p, bytes, stream()) != cudaSuccess) {  // once more with the pool's spare memory released
+    cudaGetLastError();
+    trimPool();
+    WS_CK(cudaMallocAsync(&p, bytes, stream()));
+  }
+  return p;
+}
+void tmpFree(void* p) {
+  if (p) cudaFreeAsync(p, stream());
+}
+void h2dAsync(void* d, const void* h, size_t b) {
+  if (b) WS_CK(cudaMemcpyAsync(d, h, b, cudaMemcpyHostToDevice, stream()));
+}
+void d2hSync(void* h, const void* d, size_t b) {
+  if (!b) return;
+  WS_CK(cudaMemcpyAsync(h, d, b, cudaMemcpyDeviceToHost, stream()));
+  WS_CK(cudaStreamSynchronize(stream()));
+}
+void sync() { WS_CK(cudaStreamSynchronize(stream())); }
+void countLaunch(int n) { gLaunches += n; }
+
+// Per-thread pinned staging buffer; an event marks the last copy out of it so reuse waits only then.
+namespace {
+thread_local uint8_t* tStage = nullptr;
+thread_local size_t tStageCap = 0;
+thread_local cudaEvent_t tStageEv = nullptr;
+}  // namespace
+uint8_t* pinnedStage(size_t bytes) {
+  if (tStageEv) WS_CK(cudaEventSynchronize(tStageEv));
+  else WS_CK(cudaEventCreateWithFlags(&tStageEv, cudaEventDisableTiming));
+  if (bytes > tStageCap) {
+    if (tStage) cudaFreeHost(tStage);
+    tStageCap = std::max<size_t>(bytes, 64 << 10);
+    WS_CK(cudaHostAlloc((void**)&tStage, tStageCap, cudaHostAllocDefault));
+  }
+  return tStage;
+}
+void stageCopied() { WS_CK(cudaEventRecord(tStageEv, stream())); }
+
+void launchScan(CUfunction f, unsigned grid, size_t smem, const Launch& L) {
+  if (smem > 48 * 1024) WS_CKD(drv().funcSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)smem));
+  void* args[] = {(void*)&L};
+  WS_CKD(drv().launchKernel(f, grid, 1, 1, kThreads, 1, 1, (unsigned)smem, (CUstream)stream(), args, nullptr));
+  countLaunch();
+}
+
+unsigned persistentGrid(CUfunction f, size_t smem, int64_t ntiles) {
+  if (smem > 48 * 1024) WS_CKD(drv().funcSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)smem));
+  int per = 0;
+  WS_CKD(drv().occupancy(&per, f, kThreads, smem));
+  if (per < 1) throw Error("scan kernel does not fit on an SM (shared memory " + std::to_string(smem) + " B)", WS_ERR_INTERNAL);
+  int64_t g = (int64_t)per * smCount();
+  if (g > ntiles) g = ntiles;
+  return (unsigned)(g < 1 ? 1 : g);
+}
+
+}  // namespace ws
+
+using namespace ws;
+
+// Runs f, translating exceptions into the thread's last error.
+template <class F>
+static int guarded(F&& f) {
+  try {
+    f();
+    return WS_OK;
+  } catch (const Error& e) {
+    setLastError(e.code, e.what());
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    setLastError(WS_ERR_OOM, "host out of memory");
+    return WS_ERR_OOM;
+  } catch (const std::exception& e) {
+    setLastError(WS_ERR_INTERNAL, e.what());
+    return WS_ERR_INTERNAL;
+  }
+}
+
+extern "C" {
+
+const char* ws_last_error(void) { return tErrMsg.c_str(); }
+int ws_last_error_code(void) { return tErrCode; }
+
+int ws_gpu_init(void) { return guarded([] { ensureInit(); }); }
+int ws_gpu_sm_count(void) {
+  int r = 0;
+  guarded([&] { r = smCount(); });
+  return r;
+}
+int ws_gpu_arch(void) {
+  int r = 0;
+  guarded([&] { r = arch(); });
+  return r;
+}
+int ws_gpu_describe(char* buf, size_t size) {
+  return guarded([&] {
+    ensureInit();
+    int dev = 0;
+    WS_CK(cudaGetDevice(&dev));
+    cudaDeviceProp prop;
+    WS_CK(cudaGetDeviceProperties(&prop, dev));
+    size_t fr = 0, tot = 0;
+    WS_CK(cudaMemGetInfo(&fr, &tot));
+    snprintf(buf, size, "%s (sm_%d%d, %d SMs, %.1f GiB free / %.1f GiB)", prop.name, prop.major, prop.minor,
+             prop.multiProcessorCount, fr / 1073741824.0, tot / 1073741824.0);
+  });
+}
+int ws_set_stream(void* s) {
+  setStream((cudaStream_t)s);
+  return WS_OK;
+}
+void* ws_get_stream(void) { return (void*)stream(); }
+int ws_dev_alloc(size_t bytes, void** out) {
+  return guarded([&] {
+    ensureInit();
+    *out = nullptr;
+    if (bytes) WS_CK(cudaMalloc(out, bytes));
+  });
+}
+int ws_dev_free(void* p) {
+  return guarded([&] {
+    if (p) WS_CK(cudaFree(p));
+  });
+}
+int ws_tmp_alloc(size_t bytes, void** out) { return guarded([&] { *out = tmpAlloc(bytes); }); }
+int ws_tmp_free(void* p) { return guarded([&] { tmpFree(p); }); }
+int ws_h2d(void* dst, const void* src, size_t bytes) {
+  return guarded([&] {
+    if (bytes) {
+      WS_CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream()));
+      WS_CK(cudaStreamSynchronize(stream()));
+    }
+  });
+}
+int ws_d2h(void* dst, const void* src, size_t bytes) { return guarded([&] { d2hSync(dst, src, bytes); }); }
+int ws_d2d(void* dst, const void* src, size_t bytes) {
+  return guarded([&] {
+    if (bytes) WS_CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, stream()));
+  });
+}
+int ws_gpu_sync(void) { return guarded([] { sync(); }); }
+int ws_gpu_trim_pool(void) { return guarded([] { trimPool(); }); }
+
+int ws_abi_layout(int64_t* out, int n) {
+  const int64_t v[] = {(int64_t)sizeof(ws_instr),
+                       (int64_t)sizeof(ws_col_view),
+                       (int64_t)offsetof(ws_col_view, off),
+                       (int64_t)sizeof(ws_expr_env),
+                       (int64_t)offsetof(ws_expr_env, consts),
+                       (int64_t)offsetof(ws_expr_env, sets),
+                       (int64_t)offsetof(ws_expr_env, setSize),
+                       (int64_t)offsetof(ws_expr_env, maps),
+                       (int64_t)offsetof(ws_expr_env, mapSize),
+                       (int64_t)offsetof(ws_expr_env, cols),
+                       (int64_t)offsetof(ws_expr_env, ovf),
+                       (int64_t)sizeof(ws_agg_plan),
+                       (int64_t)offsetof(ws_agg_plan, where),
+                       (int64_t)offsetof(ws_agg_plan, nkeys),
+                       (int64_t)offsetof(ws_agg_plan, keys),
+                       (int64_t)offsetof(ws_agg_plan, naggs),
+                       (int64_t)offsetof(ws_agg_plan, aggs),
+                       (int64_t)offsetof(ws_agg_plan, ops),
+                       (int64_t)offsetof(ws_agg_plan, aggInt),
+                       (int64_t)offsetof(ws_agg_plan, aggBits),
+                       (int64_t)offsetof(ws_agg_plan, aggPart),
+                       (int64_t)offsetof(ws_agg_plan, aggNull),
+                       (int64_t)offsetof(ws_agg_plan, densePriv),
+                       (int64_t)offsetof(ws_agg_plan, keyInt),
+                       (int64_t)offsetof(ws_agg_plan, genv),
+                       (int64_t)sizeof(ws_dense_spec),
+                       (int64_t)offsetof(ws_dense_spec, kmin),
+                       (int64_t)offsetof(ws_dense_spec, range),
+                       (int64_t)offsetof(ws_dense_spec, stride),
+                       (int64_t)offsetof(ws_dense_spec, slotOff),
+                       (int64_t)offsetof(ws_dense_spec, kind)};
+  const int m = (int)(sizeof v / sizeof v[0]);
+  for (int i = 0; i < n && i < m; ++i) out[i] = v[i];
+  return m;
+}
+
+int64_t ws_kernel_launches(void) { return gLaunches.load(); }
+
+}  // extern "C"
+
+namespace ws {
+int guardedCall(const std::function<void()>& f) { return guarded(f); }
+}  // namespace ws

@@ -1,0 +1,262 @@
+"""Python mirror of the engine's GPU operator interface (src/gpu.h, src/jit.h) over the C ABI.
+
+Names follow the reference: GpuAggregator (add_batch / run / run_window / overflowed / fetch / compact /
+group_count), select / select_multi, gather_multi, hash_join / hash_join_parts, jit_get and the jit
+modes.  Errors raise WsError with the engine's SQL error code.  Every call goes to libwarpstore_b200;
+there is no host fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from ._lib import WsError, check, lib
+
+P = C.c_void_p
+
+
+class DeviceBuffer:
+    """A device allocation owned by Python (cudaMalloc through the library)."""
+
+    def __init__(self, nbytes: int):
+        self.nbytes = int(nbytes)
+        p = P()
+        check(lib().ws_dev_alloc(max(self.nbytes, 1), C.byref(p)))
+        self.ptr = p.value
+
+    @classmethod
+    def from_array(cls, a: np.ndarray) -> "DeviceBuffer":
+        a = np.ascontiguousarray(a)
+        b = cls(a.nbytes)
+        if a.nbytes:
+            check(lib().ws_h2d(b.ptr, a.ctypes.data, a.nbytes))
+        return b
+
+    def to_array(self, dtype, count: int | None = None) -> np.ndarray:
+        dt = np.dtype(dtype)
+        n = self.nbytes // dt.itemsize if count is None else count
+        out = np.empty(n, dtype=dt)
+        if n:
+            check(lib().ws_d2h(out.ctypes.data, self.ptr, n * dt.itemsize))
+        return out
+
+    def free(self):
+        if self.ptr:
+            lib().ws_dev_free(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def device_to_array(ptr: int, dtype, count: int) -> np.ndarray:
+    dt = np.dtype(dtype)
+    out = np.empty(count, dtype=dt)
+    if count:
+        check(lib().ws_d2h(out.ctypes.data, ptr, count * dt.itemsize))
+    return out
+
+
+def tmp_free(ptr: int):
+    if ptr:
+        check(lib().ws_tmp_free(ptr))
+
+
+def gpu_init():
+    check(lib().ws_gpu_init())
+
+
+def sync():
+    check(lib().ws_gpu_sync())
+
+
+def kernel_launches() -> int:
+    return int(lib().ws_kernel_launches())
+
+
+# ------------------------------------------------------------------ compiled plans
+def jit_set_mode(mode: int):
+    check(lib().ws_jit_set_mode(mode))
+
+
+def jit_set_default_mode(mode: int):
+    check(lib().ws_jit_set_default_mode(mode))
+
+
+def jit_set_cache_dir(path: str):
+    check(lib().ws_jit_set_cache_dir(path.encode()))
+
+
+def jit_get(env: abi.ExprEnv, ncols: int, plan: abi.AggPlan, fn: int, kind: str = "") -> int | None:
+    out = P()
+    check(lib().ws_jit_get(C.byref(env), ncols, C.byref(plan), fn, kind.encode(), C.byref(out)))
+    return out.value
+
+
+def jit_info(prog: int) -> abi.JitInfo:
+    info = abi.JitInfo()
+    check(lib().ws_jit_program_info(prog, C.byref(info)))
+    return info
+
+
+def codegen_source(env: abi.ExprEnv, ncols: int, plan: abi.AggPlan, fn: int) -> str:
+    need = C.c_size_t()
+    check(lib().ws_codegen_source(C.byref(env), ncols, C.byref(plan), fn, None, 0, C.byref(need)))
+    buf = C.create_string_buffer(need.value)
+    check(lib().ws_codegen_source(C.byref(env), ncols, C.byref(plan), fn, buf, need.value, C.byref(need)))
+    return buf.value.decode()
+
+
+def codegen_compile_check(env: abi.ExprEnv, ncols: int, plan: abi.AggPlan, fn: int, dense_groups: int = 0,
+                          arch_sm: int = 100) -> int:
+    n = C.c_size_t()
+    check(lib().ws_codegen_compile_check(C.byref(env), ncols, C.byref(plan), fn, dense_groups, arch_sm, C.byref(n)))
+    return n.value
+
+
+# ------------------------------------------------------------------ aggregation
+class GpuAggregator:
+    """GPU aggregation state of one query (src/gpu.h:84-130)."""
+
+    def __init__(self, plan: abi.AggPlan, capacity: int, dense: abi.DenseSpec | None = None):
+        self.plan = plan
+        h = P()
+        check(lib().ws_agg_create(C.byref(plan), int(capacity), C.byref(dense) if dense is not None else None,
+                                  C.byref(h)))
+        self.h = h.value
+
+    def close(self):
+        if self.h:
+            lib().ws_agg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_batch(self, env: abi.ExprEnv, ncols: int, n: int, deleted: int = 0):
+        check(lib().ws_agg_add_batch(self.h, C.byref(env), ncols, int(n), deleted or None))
+
+    def run(self, env: abi.ExprEnv, jit: int | None = None):
+        check(lib().ws_agg_run(self.h, C.byref(env), jit))
+
+    def run_window(self, env: abi.ExprEnv, jit: int | None = None):
+        check(lib().ws_agg_run_window(self.h, C.byref(env), jit))
+
+    def overflowed(self) -> bool:
+        o = C.c_int()
+        check(lib().ws_agg_overflowed(self.h, C.byref(o)))
+        return bool(o.value)
+
+    def group_count(self) -> int:
+        g = C.c_int64()
+        check(lib().ws_agg_group_count(self.h, C.byref(g)))
+        return g.value
+
+    def capacity(self) -> int:
+        return int(lib().ws_agg_capacity(self.h))
+
+    def batches(self) -> int:
+        return int(lib().ws_agg_batches(self.h))
+
+    def rows_in(self) -> int:
+        return int(lib().ws_agg_rows_in(self.h))
+
+    def is_dense(self) -> bool:
+        return bool(lib().ws_agg_is_dense(self.h))
+
+    def fetch(self, exact: bool = True):
+        """(keys [g, nk] float64, accs [g, na] float64, exact [g, na, 2] int64 or None)."""
+        nk, na = self.plan.nkeys, self.plan.naggs
+        g = C.c_int64()
+        rc = lib().ws_agg_fetch(self.h, 0, None, None, None, C.byref(g))
+        if rc not in (0, 1206):
+            check(rc)
+        n = g.value
+        keys = np.empty((n, nk), dtype=np.float64)
+        accs = np.empty((n, na), dtype=np.float64)
+        ex = np.empty((n, na, 2), dtype=np.int64) if exact else None
+        check(lib().ws_agg_fetch(self.h, n, keys.ctypes.data if nk else None, accs.ctypes.data,
+                                 ex.ctypes.data if exact else None, C.byref(g)))
+        return keys, accs, ex
+
+    def sum_bits_slots(self) -> np.ndarray:
+        out = np.zeros(self.plan.naggs, dtype=np.uint8)
+        check(lib().ws_agg_sum_bits_slots(self.h, out.ctypes.data))
+        return out
+
+    def sum_high(self) -> np.ndarray:
+        out = np.zeros(self.plan.naggs, dtype=np.int64)
+        check(lib().ws_agg_sum_high(self.h, out.ctypes.data))
+        return out
+
+    def compact(self):
+        """Groups left on the device, column-major: (keys_ptr, accs_ptr, g); free with tmp_free."""
+        k, a, g = P(), P(), C.c_int64()
+        check(lib().ws_agg_compact(self.h, C.byref(k), C.byref(a), C.byref(g)))
+        return k.value, a.value, g.value
+
+
+# ------------------------------------------------------------------ selection / gathers / joins
+def _views_array(views: list) -> C.Array:
+    arr = (abi.ColView * max(len(views), 1))()
+    for i, v in enumerate(views):
+        arr[i] = v
+    return arr
+
+
+def select_multi(env: abi.ExprEnv, where: abi.Prog | None, batches: list, ncols: int, jit: int | None = None):
+    """batches: [(n, deleted_ptr, [ColView per column])].  Returns (idx_ptr, count, per_batch counts);
+    idx_ptr holds ascending global indices into the concatenated batches (free with tmp_free)."""
+    nb = len(batches)
+    bn = (C.c_int64 * max(nb, 1))(*[b[0] for b in batches])
+    bdel = (P * max(nb, 1))(*[b[1] or None for b in batches])
+    cols = []
+    for b in batches:
+        cols.extend(b[2])
+    arr = _views_array(cols)
+    per = (C.c_int64 * max(nb, 1))()
+    out = P()
+    cnt = C.c_int64()
+    check(lib().ws_select_multi(C.byref(env), 1 if where is not None else 0, where or abi.Prog(0, 0), nb, bn, bdel,
+                                arr, ncols, C.byref(out), per, jit, C.byref(cnt)))
+    return out.value, cnt.value, list(per)[:nb]
+
+
+def gather_multi(views: list, boff: list, ptype: int, esize: int, idx_ptr: int, m: int, dst_ptr: int):
+    arr = _views_array(views)
+    bo = (C.c_int64 * max(len(boff), 1))(*boff)
+    check(lib().ws_gather_multi(arr, bo, len(views), ptype, esize, idx_ptr, int(m), dst_ptr))
+
+
+def gather(src_ptr: int, ptype: int, idx_ptr: int, m: int, dst_ptr: int):
+    check(lib().ws_gather(src_ptr, ptype, idx_ptr, int(m), dst_ptr))
+
+
+def hash_join_parts(build_key: abi.ColView, boff: list, probe_key: abi.ColView, poff: list):
+    """Returns (build_idx_ptr, probe_idx_ptr, m, out_off); free the pointers with tmp_free."""
+    bo = (C.c_int64 * len(boff))(*boff)
+    po = (C.c_int64 * len(poff))(*poff)
+    oo = (C.c_int64 * len(poff))()
+    ob, op_ = P(), P()
+    m = C.c_int64()
+    check(lib().ws_hash_join_parts(build_key, bo, len(boff) - 1, probe_key, po, len(poff) - 1, C.byref(ob),
+                                   C.byref(op_), oo, C.byref(m)))
+    return ob.value, op_.value, m.value, list(oo)
+
+
+def hash_join(build_key: abi.ColView, nb: int, probe_key: abi.ColView, np_: int):
+    return hash_join_parts(build_key, [0, nb], probe_key, [0, np_])[:3]
+
+
+__all__ = ["DeviceBuffer", "GpuAggregator", "WsError", "device_to_array", "gather", "gather_multi", "gpu_init",
+           "hash_join", "hash_join_parts", "jit_get", "jit_info", "jit_set_cache_dir", "jit_set_default_mode",
+           "jit_set_mode", "kernel_launches", "select_multi", "sync", "tmp_free", "codegen_source",
+           "codegen_compile_check"]
