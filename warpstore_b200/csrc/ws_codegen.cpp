@@ -203,7 +203,7 @@ std::string genEvaluator(const ws_expr_env& env, int ncols, const ws_agg_plan& p
     lay = layoutOf(plan);
     for (int k = 0; k < plan.nkeys; ++k) keys.push_back(g.prog(plan.keys[k]));
     for (int a = 0; a < plan.naggs; ++a) {
-      if (plan.ops[a] == WS_AGG_COUNT || lay.kind[a] == SK_NONE || a == 0) {
+      if (plan.ops[a] == WS_AGG_COUNT || lay.kind[a] == SK_NONE) {
         aggs.push_back({"0", true});
         continue;
       }
@@ -291,7 +291,7 @@ std::string genEvaluator(const ws_expr_env& env, int ncols, const ws_agg_plan& p
   o << " } return 0; }\n";
   o << "  __device__ __forceinline__ bool ival(int a, int i, ws::i64& v) const { switch (a) {";
   if (agg)
-    for (int a = 1; a < na; ++a) {
+    for (int a = 0; a < na; ++a) {
       if (plan.ops[a] == WS_AGG_COUNT || lay.kind[a] == SK_NONE) continue;
       if (!(lay.kind[a] == SK_ISUM || lay.kind[a] == SK_IMIN || lay.kind[a] == SK_IMAX)) continue;
       if (plan.aggNull[a])
@@ -303,7 +303,7 @@ std::string genEvaluator(const ws_expr_env& env, int ncols, const ws_agg_plan& p
   o << " } v = 0; return false; }\n";
   o << "  __device__ __forceinline__ double dval(int a, int i) const { switch (a) {";
   if (agg)
-    for (int a = 1; a < na; ++a) {
+    for (int a = 0; a < na; ++a) {
       if (!(lay.kind[a] == SK_DSUM || lay.kind[a] == SK_DMIN || lay.kind[a] == SK_DMAX)) continue;
       o << "\n    case " << a << ": return " << D(aggs[a]) << ";";
     }

@@ -269,7 +269,7 @@ WS_DI bool denseIndex(const Launch& L, const Ev& ev, int i, i64& g) {
     if ((u64)d >= (u64)L.range[k]) return false;
     g += d * L.stride[k];
   }
-  return true;
+  return g < L.G;
 }
 
 // Few groups: every thread keeps all G accumulator rows in registers (GR = G, compile-time), rows

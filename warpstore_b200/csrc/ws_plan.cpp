@@ -159,8 +159,9 @@ void buildTProgs(const ws_expr_env& env, int ncols, const ws_agg_plan& plan, boo
   };
   if (hasWhere) add(plan.where, out.where);
   for (int k = 0; k < plan.nkeys; ++k) add(plan.keys[k], out.keys[k]);
-  for (int a = 1; a < plan.naggs; ++a)
-    if (plan.ops[a] != WS_AGG_COUNT) add(plan.aggs[a], out.aggs[a]);
+  const SlotLayout lay = layoutOf(plan);
+  for (int a = 0; a < plan.naggs; ++a)
+    if (plan.ops[a] != WS_AGG_COUNT && lay.kind[a] != SK_NONE) add(plan.aggs[a], out.aggs[a]);
   if (code.size() > sizeof(out.code) / sizeof(out.code[0])) throw Error("plan too large for the interpreter", WS_ERR_PLAN);
   memcpy(out.code, code.data(), code.size() * sizeof(TInstr));
 }
