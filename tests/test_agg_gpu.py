@@ -191,13 +191,18 @@ def test_hash_overflow_then_retry_bigger():
     t.add("v", abi.T_I64, rng.integers(0, 100, n, dtype=np.int64))
     e = W.env_for(t)
     aq = q.AggQuery(e, None, [(q.col(0), True)], [q.Agg("SUM", q.col(1), "BIGINT", True)])
-    agg = gpu_aggregate(t, e, aq.plan, cap=1024)
-    assert agg.overflowed()
-    want = max(agg.capacity() * 4, agg.group_count() * 4)  # the engine's retry rule
-    agg.close()
+    cap, tries = 1024, 0
+    while True:  # the engine's loop (src/engine_select.cpp:1514-1522): detect, resize, rerun
+        agg = gpu_aggregate(t, e, aq.plan, cap=cap)
+        if not agg.overflowed():
+            break
+        want = max(agg.capacity() * 4, agg.group_count() * 4)
+        agg.close()
+        cap = 1 << (want - 1).bit_length()
+        tries += 1
+        assert tries < 8
+    assert tries >= 1 and cap >= 50_000
     ok, ow, _ = oracle_aggregate(t, e, aq.plan)
-    agg = gpu_aggregate(t, e, aq.plan, cap=want)
-    assert not agg.overflowed()
     keys, accs, ex = agg.fetch()
     compare_exact(aq.plan, keys, ex, ok, ow)
 

@@ -193,7 +193,7 @@ const char* valType(const ColUse& u) {
 }  // namespace
 
 // Generated evaluator for one plan (see the evaluator contract in ws_kern.cuh).
-std::string genEvaluator(const ws_expr_env& env, int ncols, const ws_agg_plan& plan, int fnKind) {
+std::string genEvaluator(const ws_expr_env& env, int ncols, const ws_agg_plan& plan, int fnKind, int* stageBytesOut) {
   Gen g{env, ncols, {}, {}, {}};
   const bool agg = fnKind == WS_JF_NOKEYS || fnKind == WS_JF_GROUPED || fnKind == WS_JF_DENSE;
   const Sym where = plan.hasWhere ? g.prog(plan.where) : Sym{"1", true};
@@ -220,7 +220,33 @@ std::string genEvaluator(const ws_expr_env& env, int ncols, const ws_agg_plan& p
   const int nk = agg ? plan.nkeys : 0, na = agg ? plan.naggs : 1;
   std::ostringstream o;
   o << "struct QEv {\n";
-  o << "  static constexpr int NK = " << std::max(nk, 1) << ", NA = " << na << ", RW = " << (agg ? lay.rw : 1) << ";\n";
+  // staged columns: every column whose row values are loaded; stage slot = the type's widest storage
+  std::vector<int> staged;
+  std::vector<int> soff;
+  int stageBytes = 0;
+  for (auto& [c, u] : g.cols) {
+    if (u.vec) continue;
+    staged.push_back(c);
+    soff.push_back(stageBytes);
+    stageBytes += ((u.t == 0 || u.t == 3) ? 4 : 8) * 1024;  // kTile rows
+  }
+  if (stageBytesOut) *stageBytesOut = stageBytes;
+  o << "  static constexpr int NK = " << std::max(nk, 1) << ", NA = " << na << ", RW = " << (agg ? lay.rw : 1)
+    << ", FRW = " << std::max(agg ? lay.frw : 1, 1) << ";\n";
+  o << "  static constexpr bool STAGED = " << (staged.empty() ? "false" : "true") << ";\n";
+  o << "  static constexpr int NSC = " << std::max<size_t>(staged.size(), 1) << ", STAGE_BYTES = " << stageBytes << ";\n";
+  o << "  struct Stage { const unsigned char* d[NSC]; int w[NSC]; unsigned bytes; int ok; };\n";
+  o << "  __device__ static void stageBind(const ws::Launch& l, int b, Stage& st) {\n";
+  o << "    const ws_col_view* cv = l.cols + (ws::i64)b * l.ncols;\n    st.bytes = 0; st.ok = 1;\n";
+  for (size_t j = 0; j < staged.size(); ++j)
+    o << "    { const ws::ColRef v = ws::resolveCol(cv[" << staged[j] << "]); st.d[" << j << "] = v.d; st.w[" << j
+      << "] = v.width; st.bytes += ws::kTile * v.width; st.ok &= (((unsigned long long)v.d & 15) == 0); }\n";
+  o << "  }\n";
+  o << "  __device__ static void stageIssue(const Stage& st, ws::i64 tr0, unsigned dst, unsigned bar) {\n";
+  for (size_t j = 0; j < staged.size(); ++j)
+    o << "    ws::bulkG2S(dst + " << soff[j] << ", st.d[" << j << "] + tr0 * st.w[" << j << "], ws::kTile * st.w[" << j
+      << "], bar);\n";
+  o << "  }\n";
   o << "  const ws::Launch& L;\n  int* ovf;\n  bool fastOk;\n  ws::i64 rb;\n";
   for (int k : g.iconsts) o << "  ws::i64 ik" << k << ";\n";
   for (int k : g.dconsts) o << "  double k" << k << ";\n";
@@ -242,6 +268,10 @@ std::string genEvaluator(const ws_expr_env& env, int ncols, const ws_agg_plan& p
   o << "  __device__ __forceinline__ int woff(int a) const { switch (a) {";
   if (agg)
     for (int a = 0; a < na; ++a) o << " case " << a << ": return " << lay.woff[a] << ";";
+  o << " } return 0; }\n";
+  o << "  __device__ __forceinline__ int fwoff(int a) const { switch (a) {";
+  if (agg)
+    for (int a = 0; a < na; ++a) o << " case " << a << ": return " << lay.fwoff[a] << ";";
   o << " } return 0; }\n";
   o << "  __device__ __forceinline__ bool keyInt(int k) const { switch (k) {";
   for (int k = 0; k < nk; ++k) o << " case " << k << ": return " << (plan.keyInt[k] ? "true" : "false") << ";";
@@ -278,6 +308,27 @@ std::string genEvaluator(const ws_expr_env& env, int ncols, const ws_agg_plan& p
         o << "    if (" << v << ".enc) ws::load4enc(" << a << "," << v << ".d + r0 * " << v << ".width," << v << ".enc," << v
           << ".base,(ws::i64)WS_NULL_I64,fast,nv); else ";
       o << "    ws::load4i64(" << a << ",(const ws::i64*)" << v << ".d + r0,fast,nv);\n";
+    }
+  }
+  o << "  }\n";
+  // the same rows from a shared-memory stage (whole tile; rt = the thread's first row in it)
+  o << "  __device__ __forceinline__ void loadStage(const unsigned char* st, int rt) {\n";
+  for (size_t j = 0; j < staged.size(); ++j) {
+    const int c = staged[j];
+    const ColUse& u = g.cols[c];
+    const std::string C = std::to_string(c), v = "v" + C, a = "c" + C;
+    const std::string src = "st + " + std::to_string(soff[j]) + " + rt * " + v + ".width";
+    if (u.t == 2) {
+      if (u.enc) o << "    if (" << v << ".enc) ws::stage4encD(" << a << "," << src << "," << v << ".dict," << v << ".enc," << v << ".base," << v << ".p10); else ";
+      o << "    ws::stage4f64(" << a << "," << src << ");\n";
+    } else if (u.t == 0 || u.t == 3) {
+      if (u.enc)
+        o << "    if (" << v << ".enc) ws::stage4enc(" << a << "," << src << "," << v << ".enc," << v
+          << ".base,(ws::i64)WS_NULL_I32); else { int t_[4]; ws::stage4i32(t_," << src << "); for (int j = 0; j < 4; ++j) " << a << "[j] = t_[j]; }\n";
+      else o << "    ws::stage4i32(" << a << "," << src << ");\n";
+    } else {
+      if (u.enc) o << "    if (" << v << ".enc) ws::stage4enc(" << a << "," << src << "," << v << ".enc," << v << ".base,(ws::i64)WS_NULL_I64); else ";
+      o << "    ws::stage4i64(" << a << "," << src << ");\n";
     }
   }
   o << "  }\n";
@@ -540,7 +591,8 @@ int ws_jit_get(const ws_expr_env* env, int ncols, const ws_agg_plan* plan, int f
     *out = nullptr;
     const int mode = jitMode();
     if (mode == WS_JIT_OFF) return;
-    const std::string ev = genEvaluator(*env, ncols, *plan, fn);
+    int stageBytes = 0;
+    const std::string ev = genEvaluator(*env, ncols, *plan, fn, &stageBytes);
     const std::string key = std::to_string(fn) + "\n" + ev;
     std::shared_ptr<ws_jit_program> p;
     bool fresh = false;
@@ -556,6 +608,7 @@ int ws_jit_get(const ws_expr_env* env, int ncols, const ws_agg_plan* plan, int f
         p->kind = kind ? kind : "";
         p->sql = tSql;
         p->source = ev;
+        p->stageBytes = stageBytes;
         gById.push_back(p);
         gCache.emplace(key, p);
         fresh = true;
@@ -591,7 +644,7 @@ int ws_jit_get(const ws_expr_env* env, int ncols, const ws_agg_plan* plan, int f
 int ws_codegen_source(const ws_expr_env* env, int ncols, const ws_agg_plan* plan, int fn, char* buf, size_t size,
                       size_t* needed) {
   return guardedCall([&] {
-    const std::string ev = genEvaluator(*env, ncols, *plan, fn);
+    const std::string ev = genEvaluator(*env, ncols, *plan, fn, nullptr);
     if (needed) *needed = ev.size() + 1;
     if (buf && size) {
       const size_t n = std::min(size - 1, ev.size());
@@ -604,7 +657,7 @@ int ws_codegen_source(const ws_expr_env* env, int ncols, const ws_agg_plan* plan
 int ws_codegen_compile_check(const ws_expr_env* env, int ncols, const ws_agg_plan* plan, int fn, int dense_groups,
                              int arch_sm, size_t* cubin_bytes) {
   return guardedCall([&] {
-    std::string body = genEvaluator(*env, ncols, *plan, fn) + kindKernels(fn);
+    std::string body = genEvaluator(*env, ncols, *plan, fn, nullptr) + kindKernels(fn);
     if (dense_groups > 0)
       body += "extern \"C\" __global__ void __launch_bounds__(ws::kThreads) wsq_dense_reg(const __grid_constant__ ws::Launch L) "
               "{ ws::aggDenseReg<QEv, " + std::to_string(dense_groups) + ">(L); }\n";

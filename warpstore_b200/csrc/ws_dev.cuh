@@ -69,6 +69,7 @@ WS_DI i64 isubc(i64 a, i64 b, int* f) {
   return r;
 }
 WS_DI i64 imulc(i64 a, i64 b, int* f) {
+  if (a == (i64)(int)a && b == (i64)(int)b) return (i64)(int)a * (i64)(int)b;  // 32 x 32 bits: exact
   const i64 r = (i64)((u64)a * (u64)b);
   if (__mul64hi(a, b) != (r >> 63) && f) *f = 1;
   return r;
@@ -375,6 +376,89 @@ WS_DI void load4encD(double (&o)[4], const unsigned char* d, const double* dict,
   for (int i = 0; i < 4; ++i) o[i] = t[i] == (i64)WS_NULL_I64 ? nanv() : (double)t[i] / p10;
 }
 
+// The same 4-row loads from a shared-memory stage (generic addressing; the stage holds whole tiles, so
+// every group is full and aligned).
+WS_DI void stage4i32(int (&o)[4], const unsigned char* p) {
+  const int4 v = *(const int4*)p;
+  o[0] = v.x, o[1] = v.y, o[2] = v.z, o[3] = v.w;
+}
+WS_DI void stage4i64(i64 (&o)[4], const unsigned char* p) {
+  const longlong2 a = *(const longlong2*)p, b = *(const longlong2*)(p + 16);
+  o[0] = a.x, o[1] = a.y, o[2] = b.x, o[3] = b.y;
+}
+WS_DI void stage4f64(double (&o)[4], const unsigned char* p) {
+  const double2 a = *(const double2*)p, b = *(const double2*)(p + 16);
+  o[0] = a.x, o[1] = a.y, o[2] = b.x, o[3] = b.y;
+}
+WS_DI void stage4enc(i64 (&o)[4], const unsigned char* p, int enc, i64 base, i64 nul) {
+  unsigned c[4], top;
+  if (enc == 1) {
+    const unsigned v = *(const unsigned*)p;
+    for (int i = 0; i < 4; ++i) c[i] = (v >> (8 * i)) & 0xffu;
+    top = 0xffu;
+  } else if (enc == 2) {
+    const uint2 v = *(const uint2*)p;
+    c[0] = v.x & 0xffffu, c[1] = v.x >> 16, c[2] = v.y & 0xffffu, c[3] = v.y >> 16;
+    top = 0xffffu;
+  } else {
+    const uint4 v = *(const uint4*)p;
+    c[0] = v.x, c[1] = v.y, c[2] = v.z, c[3] = v.w;
+    top = 0xffffffffu;
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) o[i] = c[i] == top ? nul : base + (i64)c[i];
+}
+WS_DI void stage4encD(double (&o)[4], const unsigned char* p, const double* dict, int enc, i64 base, double p10) {
+  if (enc == 4) {
+    const unsigned v = *(const unsigned*)p;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) o[i] = __ldg(dict + ((v >> (8 * i)) & 0xffu));
+    return;
+  }
+  i64 t[4];
+  stage4enc(t, p, enc == 5 ? 2 : 3, base, (i64)WS_NULL_I64);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) o[i] = t[i] == (i64)WS_NULL_I64 ? nanv() : (double)t[i] / p10;
+}
+
+// ---- bulk asynchronous copies (TMA engine, non-tensor form) into shared memory, completed on an
+// mbarrier.  No cluster multicast: every copy reads this GPU's own memory into this CTA.
+WS_DI unsigned smemAddr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+WS_DI void mbarInit(unsigned bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+WS_DI void fenceMbarInit() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+WS_DI void fenceProxyAsync() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+WS_DI void mbarArriveTx(unsigned bar, unsigned tx) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(tx) : "memory");
+}
+WS_DI void mbarArrive(unsigned bar) { asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory"); }
+WS_DI bool mbarTest(unsigned bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Waits for the phase with the given parity; gives up after about 2^32 SM cycles (~2 s) and returns false.
+WS_DI bool mbarWait(unsigned bar, unsigned parity) {
+  if (mbarTest(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (!mbarTest(bar, parity)) {
+    if (clock64() - t0 > (1ll << 32)) return false;
+    __nanosleep(32);
+  }
+  return true;
+}
+// global -> shared bulk copy of `bytes` (multiple of 16; both addresses 16-byte aligned)
+WS_DI void bulkG2S(unsigned dst, const void* src, unsigned bytes, unsigned bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
 // Resolved view of one column of the current batch: where row 0's data starts and how it is encoded.
 struct ColRef {
   const unsigned char* d;  // data of row 0 (raw: the view pointer; encoded: header skipped + off applied)
@@ -461,12 +545,16 @@ struct Launch {
   const int* woff;            // interpreter only: word offset per slot
   const uint8_t* aggNull;     // interpreter only
   const uint8_t* keyInt;      // interpreter only
+  const int* fwoff;           // interpreter only: word offset per slot in register rows
   int nkeys, naggs, rowWords; // interpreter only (JIT: compile-time)
+  int fastWords;              // interpreter only: words of a register row
+  int stages;                 // shared-memory stages of staged scans (0: loads straight from global memory)
   // aggregation outputs
   u64* part;                  // per-CTA partial rows
   u64* rows;                  // result rows
   unsigned* ticket;           // last-CTA-done counter (zeroed before launch)
-  int* err;                   // error flags: [0] dense key out of range, [1] hash table overflow
+  int* err;                   // error flags: [0] dense key out of range, [1] hash table overflow,
+                              // [2] a staged tile did not arrive in time
   // dense GROUP BY
   i64 G;
   i64 kmin[WS_MAX_KEYS], range[WS_MAX_KEYS], stride[WS_MAX_KEYS];

@@ -117,6 +117,8 @@ struct SlotLayout {
   uint8_t kind[WS_MAX_AGGS] = {};
   int woff[WS_MAX_AGGS] = {};
   int partner[WS_MAX_AGGS] = {};  // SK_NONE slots: the slot whose value they repeat
+  int fwoff[WS_MAX_AGGS] = {};    // word of the slot in per-thread register rows
+  int frw = 0;                    // words of a register row
 };
 SlotLayout layoutOf(const ws_agg_plan& plan);
 // Typed interpreter code for the plan's programs (where, keys, aggregates).
@@ -148,6 +150,7 @@ struct ws_jit_program {
   double compileMs = 0;
   std::atomic<int> state{0};  // 0 compiling, 1 ready, 2 failed
   bool fromDisk = false;
+  int stageBytes = 0;  // shared memory per staged tile (0: the plan reads global memory directly)
   ws::KernelSet kernels;
   CUmodule module = nullptr;
   std::mutex mu;

@@ -58,6 +58,193 @@ WS_DI void forEachRow(const Launch& L, Ev& ev, F&& f) {
   }
 }
 
+// Same visit, with each tile's column chunks brought into shared memory by bulk asynchronous copies
+// (TMA engine) S-1 tiles ahead of use: a ring of S stages of Ev::STAGE_BYTES, one mbarrier per stage.
+// Thread 0 issues the copies; every thread waits on the stage's barrier, reads its 4 rows from shared
+// memory, and the CTA synchronizes before the stage is refilled.  Tiles that cannot be copied in bulk
+// (a batch's ragged last tile, a column not 16-byte aligned) are marked "direct" and read from global
+// memory as in forEachRow; their stage barrier still completes its phase (plain arrive), so the
+// parity of every stage advances once per use.  A wait that exceeds its limit sets err[2] and ends the
+// CTA's loop (all threads agree through __syncthreads_or).
+template <class Ev, class F>
+WS_DI void forEachRowStaged(const Launch& L, Ev& ev, unsigned char* stages, int S, F&& f) {
+  __shared__ __align__(8) u64 bars[8];
+  __shared__ int smode[8];
+  __shared__ typename Ev::Stage pst;  // the producer's view of its current batch
+  __shared__ int pbatch;
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    for (int s = 0; s < S; ++s) mbarInit(smemAddr(&bars[s]), 1);
+    fenceMbarInit();
+    fenceProxyAsync();
+    pbatch = -1;
+  }
+  __syncthreads();
+  const i64 K = L.ntiles > (i64)blockIdx.x ? (L.ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+  int pb = 0;  // producer batch cursor (thread 0)
+  auto issue = [&](i64 k) {
+    const i64 t = blockIdx.x + k * (i64)gridDim.x;
+    const int s = (int)(k % S);
+    while (t >= __ldg(L.tileStart + pb + 1)) ++pb;
+    if (pb != pbatch) {
+      Ev::stageBind(L, pb, pst);
+      pbatch = pb;
+    }
+    const i64 tr0 = (t - __ldg(L.tileStart + pb)) * kTile;
+    const bool bulk = pst.ok && tr0 + kTile <= __ldg(L.n + pb);
+    smode[s] = bulk;
+    const unsigned bar = smemAddr(&bars[s]);
+    if (bulk) {
+      mbarArriveTx(bar, pst.bytes);
+      Ev::stageIssue(pst, tr0, smemAddr(stages + (size_t)s * Ev::STAGE_BYTES), bar);
+    } else {
+      mbarArrive(bar);
+    }
+  };
+  if (tid == 0) {
+    fenceProxyAsync();
+    for (i64 k = 0; k < S - 1 && k < K; ++k) issue(k);
+  }
+  int b = 0, bound = -1;
+  for (i64 k = 0; k < K; ++k) {
+    const i64 t = blockIdx.x + k * (i64)gridDim.x;
+    const int s = (int)(k % S);
+    if (tid == 0 && k + S - 1 < K) {
+      fenceProxyAsync();  // the stage being refilled was last read through the generic proxy
+      issue(k + S - 1);
+    }
+    const bool ok = mbarWait(smemAddr(&bars[s]), (unsigned)((k / S) & 1));
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        L.err[2] = 1;
+        // give the copies already issued for later stages their chance to land (bounded) before exit
+        for (i64 j = k + 1; j < K && j < k + S; ++j) mbarWait(smemAddr(&bars[j % S]), (unsigned)((j / S) & 1));
+      }
+      __syncthreads();
+      break;
+    }
+    while (t >= __ldg(L.tileStart + b + 1)) ++b;
+    if (b != bound) {
+      ev.bind(L, b);
+      bound = b;
+    }
+    const i64 n = __ldg(L.n + b);
+    const i64 r0 = (t - __ldg(L.tileStart + b)) * kTile + tid * 4;
+    const i64 left = n - r0;
+    if (left > 0) {
+      const int nv = left >= 4 ? 4 : (int)left;
+      if (smode[s]) ev.loadStage(stages + (size_t)s * Ev::STAGE_BYTES, tid * 4);
+      else ev.load(r0, ev.fastOk && nv == 4, nv);
+      unsigned live = (1u << nv) - 1;
+      const uint32_t* del = L.del[b];
+      if (del) live &= ~(__ldg(del + (r0 >> 5)) >> (r0 & 31)) & 0xfu;
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        if (((live >> i) & 1u) && ev.where(i)) f(i, b, r0 + i);
+    }
+    __syncthreads();  // stage s consumed: it may be refilled
+  }
+}
+
+// Visits rows, staged through shared memory when the evaluator supports it and stages were given.
+template <class Ev, class F>
+WS_DI void scanRows(const Launch& L, Ev& ev, F&& f) {
+  if constexpr (Ev::STAGED) {
+    if (L.stages >= 2) {
+      extern __shared__ __align__(16) u64 wsSmem[];
+      forEachRowStaged(L, ev, (unsigned char*)wsSmem, L.stages, f);
+      return;
+    }
+  }
+  forEachRow(L, ev, f);
+}
+
+// ------------------------------------------------------------------ register rows
+// Per-thread accumulators of the no-key and dense kernels: one word per slot (fwoff).  An integer SUM
+// keeps an int64 sum of the values in [-2^31, 2^31) (no overflow below 2^32 rows per thread); a larger
+// value goes exactly into the CTA's shared int128 spill counter of its (group, slot).
+template <class Ev>
+WS_DI void fastIdentity(const Ev& ev, u64* w) {
+#pragma unroll
+  for (int a = 0; a < Ev::NA; ++a) {
+    if (a >= ev.na()) break;
+    const int o = ev.fwoff(a);
+    switch (ev.kind(a)) {
+      case SK_COUNT: case SK_ISUM: case SK_DSUM: w[o] = 0; break;
+      case SK_IMIN: w[o] = (u64)0x7fffffffffffffffll; break;
+      case SK_IMAX: w[o] = (u64)0x8000000000000000ll; break;
+      case SK_DMIN: w[o] = (u64)dord(__longlong_as_double(0x7ff0000000000000ll)); break;
+      case SK_DMAX: w[o] = (u64)dord(__longlong_as_double((i64)0xfff0000000000000ull)); break;
+      default: break;
+    }
+  }
+}
+// The register-row contribution of row i (spilling large integer values into spill[slot][2]).
+template <class Ev>
+WS_DI void fastOfInput(const Ev& ev, int i, u64* x, u64* spill) {
+  fastIdentity(ev, x);
+#pragma unroll
+  for (int a = 0; a < Ev::NA; ++a) {
+    if (a >= ev.na()) break;
+    const int o = ev.fwoff(a);
+    switch (ev.kind(a)) {
+      case SK_COUNT: x[o] = 1; break;
+      case SK_ISUM: {
+        i64 v;
+        if (ev.ival(a, i, v)) {
+          if ((u64)(v + 0x80000000ll) < 0x100000000ull) x[o] = (u64)v;
+          else atomicAdd128(spill + 2 * a, (i64*)(spill + 2 * a + 1), (u64)v, v >> 63);
+        }
+        break;
+      }
+      case SK_IMIN: case SK_IMAX: {
+        i64 v;
+        if (ev.ival(a, i, v)) x[o] = (u64)v;
+        break;
+      }
+      case SK_DSUM: {
+        const double v = ev.dval(a, i);
+        if (v == v) x[o] = (u64)__double_as_longlong(v);
+        break;
+      }
+      case SK_DMIN: case SK_DMAX: {
+        const double v = ev.dval(a, i);
+        if (v == v) x[o] = (u64)dord(v);
+        break;
+      }
+      default: break;
+    }
+  }
+}
+template <class Ev>
+WS_DI void fastCombine(const Ev& ev, u64* w, const u64* x) {
+#pragma unroll
+  for (int a = 0; a < Ev::NA; ++a) {
+    if (a >= ev.na()) break;
+    const int o = ev.fwoff(a);
+    switch (ev.kind(a)) {
+      case SK_COUNT: case SK_ISUM: w[o] += x[o]; break;
+      case SK_IMIN: case SK_DMIN: if ((i64)x[o] < (i64)w[o]) w[o] = x[o]; break;
+      case SK_IMAX: case SK_DMAX: if ((i64)x[o] > (i64)w[o]) w[o] = x[o]; break;
+      case SK_DSUM:
+        w[o] = (u64)__double_as_longlong(__longlong_as_double((i64)w[o]) + __longlong_as_double((i64)x[o]));
+        break;
+      default: break;
+    }
+  }
+}
+// register row -> accumulator row (integer sums widened to int128)
+template <class Ev>
+WS_DI void fastExpand(const Ev& ev, const u64* f, u64* w) {
+#pragma unroll
+  for (int a = 0; a < Ev::NA; ++a) {
+    if (a >= ev.na()) break;
+    const int o = ev.woff(a), fo = ev.fwoff(a);
+    if (ev.kind(a) == SK_ISUM) w[o] = f[fo], w[o + 1] = (u64)((i64)f[fo] >> 63);
+    else if (ev.kind(a) != SK_NONE) w[o] = f[fo];
+  }
+}
+
 // ------------------------------------------------------------------ row words
 // A group's accumulator row: word 0 = key word, then each slot's words at woff(a) (slot kinds in
 // SlotKind).  DMIN / DMAX words hold dord(value) so that integer min / max orders them.
@@ -245,16 +432,30 @@ WS_DI void lastCtaReduce(const Launch& L, const Ev& ev, int nrows, u64* sred) {
 // ------------------------------------------------------------------ no GROUP BY
 template <class Ev>
 __device__ void aggNoKeys(const Launch& L) {
-  constexpr int RW = Ev::RW;
+  constexpr int RW = Ev::RW, FW = Ev::FRW;
   __shared__ u64 sred[(kThreads / 32) * RW];
+  __shared__ u64 spill[2 * Ev::NA];
   Ev ev(L);
+  for (int j = threadIdx.x; j < 2 * Ev::NA; j += blockDim.x) spill[j] = 0;
+  __syncthreads();
+  u64 f[FW];
+  fastIdentity(ev, f);
+  scanRows(L, ev, [&](int i, int, i64) {
+    u64 x[FW];
+    fastOfInput(ev, i, x, spill);
+    fastCombine(ev, f, x);
+  });
   u64 w[RW];
   rowIdentity(ev, w);
-  forEachRow(L, ev, [&](int i, int, i64) { rowAccumulate(ev, i, w); });
+  fastExpand(ev, f, w);
+  __syncthreads();
   blockReduceRow(ev, w, sred);
   const int rw = ev.rowWords();
-  if (threadIdx.x == 0)
+  if (threadIdx.x == 0) {
+    for (int a = 0; a < ev.na(); ++a)
+      if (ev.kind(a) == SK_ISUM) add128w(w[ev.woff(a)], *(i64*)&w[ev.woff(a) + 1], spill[2 * a], (i64)spill[2 * a + 1]);
     for (int j = 1; j < rw; ++j) L.part[(size_t)blockIdx.x * rw + j] = w[j];
+  }
   lastCtaReduce<Ev, RW>(L, ev, 1, sred);
 }
 
@@ -272,34 +473,45 @@ WS_DI bool denseIndex(const Launch& L, const Ev& ev, int i, i64& g) {
   return g < L.G;
 }
 
-// Few groups: every thread keeps all G accumulator rows in registers (GR = G, compile-time), rows
-// of one 4-row group are added with predication, no atomics.  Partials per CTA, last CTA reduces.
+// Few groups: every thread keeps all G register rows (GR = G, compile-time); a row is added to its
+// group's row with predication, no atomics.  Partials per CTA, the last CTA reduces them.
 template <class Ev, int GR>
 __device__ void aggDenseReg(const Launch& L) {
-  constexpr int RW = Ev::RW;
+  constexpr int RW = Ev::RW, FW = Ev::FRW;
   __shared__ u64 sred[(kThreads / 32) * RW];
+  __shared__ u64 spill[GR * 2 * Ev::NA];
   Ev ev(L);
-  u64 w[GR][RW];
+  for (int j = threadIdx.x; j < GR * 2 * Ev::NA; j += blockDim.x) spill[j] = 0;
+  __syncthreads();
+  u64 f[GR][FW];
 #pragma unroll
-  for (int g = 0; g < GR; ++g) rowIdentity(ev, w[g]);
-  forEachRow(L, ev, [&](int i, int, i64) {
+  for (int g = 0; g < GR; ++g) fastIdentity(ev, f[g]);
+  scanRows(L, ev, [&](int i, int, i64) {
     i64 gi;
     if (!denseIndex(L, ev, i, gi)) {
       L.err[0] = 1;
       return;
     }
-    u64 x[RW];
-    rowOfInput(ev, i, x);
+    u64 x[FW];
+    fastOfInput(ev, i, x, spill + gi * 2 * Ev::NA);
 #pragma unroll
     for (int g = 0; g < GR; ++g)
-      if (gi == g) rowCombine(ev, w[g], x);
+      if (gi == g) fastCombine(ev, f[g], x);
   });
+  __syncthreads();
   const int rw = ev.rowWords();
 #pragma unroll
   for (int g = 0; g < GR; ++g) {
-    blockReduceRow(ev, w[g], sred);
-    if (threadIdx.x == 0)
-      for (int j = 1; j < rw; ++j) L.part[((size_t)blockIdx.x * GR + g) * rw + j] = w[g][j];
+    u64 w[RW];
+    rowIdentity(ev, w);
+    fastExpand(ev, f[g], w);
+    blockReduceRow(ev, w, sred);
+    if (threadIdx.x == 0) {
+      const u64* sp = spill + g * 2 * Ev::NA;
+      for (int a = 0; a < ev.na(); ++a)
+        if (ev.kind(a) == SK_ISUM) add128w(w[ev.woff(a)], *(i64*)&w[ev.woff(a) + 1], sp[2 * a], (i64)sp[2 * a + 1]);
+      for (int j = 1; j < rw; ++j) L.part[((size_t)blockIdx.x * GR + g) * rw + j] = w[j];
+    }
   }
   lastCtaReduce<Ev, RW>(L, ev, GR, sred);
 }

@@ -249,6 +249,7 @@ struct BatchDesc {
   const TProgs* progs = nullptr;
   const uint8_t* kinds = nullptr;
   const int* woff = nullptr;
+  const int* fwoff = nullptr;
   const uint8_t* aggNull = nullptr;
   const uint8_t* keyInt = nullptr;
 };
@@ -265,11 +266,12 @@ static BatchDesc uploadBatches(int nb, int ncols, const int64_t* bn, const uint3
   };
   const size_t oCols = take(colBytes), oN = take(8 * nb), oDel = take(8 * nb), oTile = take(8 * (nb + 1)),
                oRow = take(8 * (nb + 1));
-  size_t oProg = 0, oKinds = 0, oWoff = 0, oNull = 0, oKeyInt = 0;
+  size_t oProg = 0, oKinds = 0, oWoff = 0, oFwoff = 0, oNull = 0, oKeyInt = 0;
   if (progs) {
     oProg = take(sizeof(TProgs));
     oKinds = take(WS_MAX_AGGS);
     oWoff = take(4 * WS_MAX_AGGS);
+    oFwoff = take(4 * WS_MAX_AGGS);
     oNull = take(WS_MAX_AGGS);
     oKeyInt = take(WS_MAX_KEYS);
   }
@@ -293,6 +295,7 @@ static BatchDesc uploadBatches(int nb, int ncols, const int64_t* bn, const uint3
     memcpy(st + oProg, progs, sizeof(TProgs));
     memcpy(st + oKinds, lay->kind, WS_MAX_AGGS);
     memcpy(st + oWoff, lay->woff, 4 * WS_MAX_AGGS);
+    memcpy(st + oFwoff, lay->fwoff, 4 * WS_MAX_AGGS);
     memcpy(st + oNull, plan->aggNull, WS_MAX_AGGS);
     memcpy(st + oKeyInt, plan->keyInt, WS_MAX_KEYS);
   }
@@ -309,6 +312,7 @@ static BatchDesc uploadBatches(int nb, int ncols, const int64_t* bn, const uint3
     d.progs = (const TProgs*)(p + oProg);
     d.kinds = p + oKinds;
     d.woff = (const int*)(p + oWoff);
+    d.fwoff = (const int*)(p + oFwoff);
     d.aggNull = p + oNull;
     d.keyInt = p + oKeyInt;
   }
@@ -330,13 +334,17 @@ static void fillLaunch(Launch& L, const BatchDesc& d, int nb, int ncols, const w
   L.progs = d.progs;
   L.kinds = d.kinds;
   L.woff = d.woff;
+  L.fwoff = d.fwoff;
   L.aggNull = d.aggNull;
   L.keyInt = d.keyInt;
   if (plan) {
     L.nkeys = plan->nkeys;
     L.naggs = plan->naggs;
   }
-  if (lay) L.rowWords = lay->rw;
+  if (lay) {
+    L.rowWords = lay->rw;
+    L.fastWords = lay->frw;
+  }
 }
 
 // A compiled plan can only run batches whose columns it was generated for: one generated for raw
@@ -367,14 +375,14 @@ struct ws_aggregator {
   int batchesDone = 0, windows = 0;
   DBuf<u64> rows;
   DBuf<double> tkeys;
-  DBuf<uint8_t> ctl;  // [count u64][err int x2][ticket]
+  DBuf<uint8_t> ctl;  // [count u64][err int x3][pad][ticket u32]
   bool fetched = false;
   std::vector<int64_t> hi;
   int64_t lastGroups = -1;
 
   u64* count() { return (u64*)ctl.p; }
   int* err() { return (int*)(ctl.p + 8); }
-  unsigned* ticket() { return (unsigned*)(ctl.p + 16); }
+  unsigned* ticket() { return (unsigned*)(ctl.p + 24); }
   int64_t nrows() const { return isDense ? dense.G : plan.nkeys ? cap + 1 : 1; }
 };
 
@@ -447,14 +455,19 @@ static void aggRun(ws_aggregator& A, const ws_expr_env& env, const ws_jit_progra
   L.err = A.err();
   L.ticket = A.ticket();
   const KernelSet& ks = useJit ? jit->kernels : interpKernels();
+  // Staged scans: a ring of 2..4 tile stages in shared memory (compiled plans only).
+  const int stageBytes = useJit ? jit->stageBytes : 0;
+  const int S = stageBytes > 0 ? (int)std::min<int64_t>(4, (200 * 1024) / stageBytes) : 0;
+  const size_t stageSmem = S >= 2 ? (size_t)S * stageBytes : 0;
   if (A.plan.nkeys == 0) {
     CUfunction f = ks.fn[K_NOKEYS];
     if (!f) throw Error("compiled plan has no aggregation kernel", WS_ERR_INTERNAL);
-    const unsigned grid = persistentGrid(f, 0, d.ntiles);
+    L.stages = S >= 2 ? S : 0;
+    const unsigned grid = persistentGrid(f, stageSmem, d.ntiles);
     DBuf<u64> part((int64_t)grid * A.lay.rw);
     L.part = part.p;
     WS_CK(cudaMemsetAsync(A.ticket(), 0, 4, stream()));
-    launchScan(f, grid, 0, L);
+    launchScan(f, grid, stageSmem, L);
     return;
   }
   if (A.isDense) {
@@ -468,11 +481,12 @@ static void aggRun(ws_aggregator& A, const ws_expr_env& env, const ws_jit_progra
     if (useJit && G <= 32 && G <= denseRegMaxGroups(A.plan)) {
       CUfunction f = denseRegKernel(const_cast<ws_jit_program*>(jit), (int)G);
       if (f) {
-        const unsigned grid = persistentGrid(f, 0, d.ntiles);
+        L.stages = S >= 2 ? S : 0;
+        const unsigned grid = persistentGrid(f, stageSmem, d.ntiles);
         DBuf<u64> part((int64_t)grid * G * A.lay.rw);
         L.part = part.p;
         WS_CK(cudaMemsetAsync(A.ticket(), 0, 4, stream()));
-        launchScan(f, grid, 0, L);
+        launchScan(f, grid, stageSmem, L);
         return;
       }
     }
@@ -550,9 +564,10 @@ static DblSpec dblSpec(const ws_aggregator& A) {
 }
 
 static void checkFlags(ws_aggregator& A, bool* overflow) {
-  int e[2] = {0, 0};
-  d2hSync(e, A.err(), 8);
+  int e[3] = {0, 0, 0};
+  d2hSync(e, A.err(), 12);
   if (e[0]) throw Error("dense GROUP BY key outside its declared range", WS_ERR_RANGE);
+  if (e[2]) throw Error("a staged tile copy did not complete in time", WS_ERR_INTERNAL);
   if (overflow) *overflow = e[1] != 0;
 }
 

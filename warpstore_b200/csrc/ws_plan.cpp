@@ -128,7 +128,9 @@ SlotLayout layoutOf(const ws_agg_plan& plan) {
     else throw Error("plan: unknown aggregate op", WS_ERR_INTERNAL);
     L.kind[a] = k;
     L.woff[a] = w;
+    L.fwoff[a] = L.frw;
     w += k == SK_NONE ? 0 : k == SK_ISUM ? 2 : 1;
+    L.frw += k == SK_NONE ? 0 : 1;
   }
   L.rw = w;
   return L;
