@@ -269,6 +269,7 @@ std::string genEvaluator(const ws_expr_env& env, int ncols, const ws_agg_plan& p
   if (agg)
     for (int a = 0; a < na; ++a) o << " case " << a << ": return " << lay.woff[a] << ";";
   o << " } return 0; }\n";
+  o << "  __device__ __forceinline__ int fastBits() const { return L.fastBits; }\n";
   o << "  __device__ __forceinline__ int fwoff(int a) const { switch (a) {";
   if (agg)
     for (int a = 0; a < na; ++a) o << " case " << a << ": return " << lay.fwoff[a] << ";";

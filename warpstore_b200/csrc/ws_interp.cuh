@@ -180,6 +180,7 @@ struct InterpEv {
   WS_DI int kind(int a) const { return __ldg(L.kinds + a); }
   WS_DI int woff(int a) const { return __ldg(L.woff + a); }
   WS_DI int fwoff(int a) const { return __ldg(L.fwoff + a); }
+  WS_DI int fastBits() const { return L.fastBits; }
   WS_DI bool keyInt(int k) const { return __ldg(L.keyInt + k) != 0; }
   WS_DI Word run(const int (&p)[2], int i) const { return vmRun(L.progs->code, p[0], p[1], cv, r0 + i, L.env); }
   WS_DI bool resInt(const int (&p)[2]) const { return L.progs->code[p[0] + p[1] - 1].rInt != 0; }

@@ -161,8 +161,9 @@ WS_DI void scanRows(const Launch& L, Ev& ev, F&& f) {
 
 // ------------------------------------------------------------------ register rows
 // Per-thread accumulators of the no-key and dense kernels: one word per slot (fwoff).  An integer SUM
-// keeps an int64 sum of the values in [-2^31, 2^31) (no overflow below 2^32 rows per thread); a larger
-// value goes exactly into the CTA's shared int128 spill counter of its (group, slot).
+// keeps an int64 sum of the values in [-2^fastBits, 2^fastBits), where fastBits is set per launch so
+// that a thread's rows (at most 4 per tile it owns) can never overflow it; a larger value goes exactly
+// into the CTA's shared int128 spill counter of its (group, slot).
 template <class Ev>
 WS_DI void fastIdentity(const Ev& ev, u64* w) {
 #pragma unroll
@@ -192,7 +193,8 @@ WS_DI void fastOfInput(const Ev& ev, int i, u64* x, u64* spill) {
       case SK_ISUM: {
         i64 v;
         if (ev.ival(a, i, v)) {
-          if ((u64)(v + 0x80000000ll) < 0x100000000ull) x[o] = (u64)v;
+          const u64 lim = 1ull << ev.fastBits();
+          if ((u64)v + lim < 2 * lim) x[o] = (u64)v;
           else atomicAdd128(spill + 2 * a, (i64*)(spill + 2 * a + 1), (u64)v, v >> 63);
         }
         break;

@@ -319,6 +319,14 @@ static BatchDesc uploadBatches(int nb, int ncols, const int64_t* bn, const uint3
   return d;
 }
 
+// fastBits for a grid: each thread adds at most 4 rows per tile it owns (see fastOfInput).
+static int fastBitsFor(int64_t ntiles, unsigned grid) {
+  const int64_t rows = 4 * ((ntiles + grid - 1) / grid);
+  int lg = 0;
+  while ((1ll << lg) < rows) ++lg;
+  return std::max(0, std::min(62, 62 - lg));
+}
+
 static void fillLaunch(Launch& L, const BatchDesc& d, int nb, int ncols, const ws_expr_env& env, const ws_agg_plan* plan,
                        const SlotLayout* lay) {
   memset(&L, 0, sizeof L);
@@ -457,13 +465,18 @@ static void aggRun(ws_aggregator& A, const ws_expr_env& env, const ws_jit_progra
   const KernelSet& ks = useJit ? jit->kernels : interpKernels();
   // Staged scans: a ring of 2..4 tile stages in shared memory (compiled plans only).
   const int stageBytes = useJit ? jit->stageBytes : 0;
-  const int S = stageBytes > 0 ? (int)std::min<int64_t>(4, (200 * 1024) / stageBytes) : 0;
+  static const int maxStages = [] {  // WARPSTORE_B200_STAGES: 0 reads tiles straight from global memory
+    const char* e = getenv("WARPSTORE_B200_STAGES");
+    return e ? std::max(0, std::min(8, atoi(e))) : 4;
+  }();
+  const int S = stageBytes > 0 ? (int)std::min<int64_t>(maxStages, (200 * 1024) / stageBytes) : 0;
   const size_t stageSmem = S >= 2 ? (size_t)S * stageBytes : 0;
   if (A.plan.nkeys == 0) {
     CUfunction f = ks.fn[K_NOKEYS];
     if (!f) throw Error("compiled plan has no aggregation kernel", WS_ERR_INTERNAL);
     L.stages = S >= 2 ? S : 0;
     const unsigned grid = persistentGrid(f, stageSmem, d.ntiles);
+    L.fastBits = fastBitsFor(d.ntiles, grid);
     DBuf<u64> part((int64_t)grid * A.lay.rw);
     L.part = part.p;
     WS_CK(cudaMemsetAsync(A.ticket(), 0, 4, stream()));
@@ -483,6 +496,7 @@ static void aggRun(ws_aggregator& A, const ws_expr_env& env, const ws_jit_progra
       if (f) {
         L.stages = S >= 2 ? S : 0;
         const unsigned grid = persistentGrid(f, stageSmem, d.ntiles);
+        L.fastBits = fastBitsFor(d.ntiles, grid);
         DBuf<u64> part((int64_t)grid * G * A.lay.rw);
         L.part = part.p;
         WS_CK(cudaMemsetAsync(A.ticket(), 0, 4, stream()));
