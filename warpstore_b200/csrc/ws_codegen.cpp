@@ -270,6 +270,7 @@ std::string genEvaluator(const ws_expr_env& env, int ncols, const ws_agg_plan& p
     for (int a = 0; a < na; ++a) o << " case " << a << ": return " << lay.woff[a] << ";";
   o << " } return 0; }\n";
   o << "  __device__ __forceinline__ int fastBits() const { return L.fastBits; }\n";
+  o << "  __device__ __forceinline__ int fastWords() const { return " << std::max(agg ? lay.frw : 1, 1) << "; }\n";
   o << "  __device__ __forceinline__ int fwoff(int a) const { switch (a) {";
   if (agg)
     for (int a = 0; a < na; ++a) o << " case " << a << ": return " << lay.fwoff[a] << ";";
@@ -371,7 +372,7 @@ const char* kindKernels(int fnKind) {
   switch (fnKind) {
     case WS_JF_NOKEYS: return "WS_K_NOKEYS(QEv, wsq)\n";
     case WS_JF_GROUPED: return "WS_K_HASH(QEv, wsq)\n";
-    case WS_JF_DENSE: return "WS_K_DENSE_SHARED(QEv, wsq)\nWS_K_DENSE_GLOBAL(QEv, wsq)\n";
+    case WS_JF_DENSE: return "WS_K_DENSE_PRIV(QEv, wsq)\nWS_K_DENSE_SHARED(QEv, wsq)\nWS_K_DENSE_GLOBAL(QEv, wsq)\n";
     default: return "WS_K_SELECT_COUNT(QEv, wsq)\nWS_K_SELECT_WRITE(QEv, wsq)\n";
   }
 }
@@ -500,8 +501,8 @@ void compileProgram(ws_jit_program& p) {
   bool disk = false;
   p.module = compileModule(body, &disk);
   p.fromDisk = disk;
-  static const char* names[K_COUNT_] = {"wsq_nokeys", "wsq_dense_shared", "wsq_dense_global",
-                                        "wsq_hash", "wsq_select_count", "wsq_select_write"};
+  static const char* names[K_COUNT_] = {"wsq_nokeys", "wsq_dense_shared", "wsq_dense_global", "wsq_hash",
+                                        "wsq_select_count", "wsq_select_write", "wsq_dense_priv"};
   for (int k = 0; k < K_COUNT_; ++k) {
     CUfunction f = nullptr;
     if (drv().moduleGetFunction(&f, p.module, names[k]) == CUDA_SUCCESS) p.kernels.fn[k] = f;

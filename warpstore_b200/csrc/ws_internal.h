@@ -127,7 +127,7 @@ EnvK envK(const ws_expr_env& env);
 
 // ---------------------------------------------------------------- kernels
 // The scan kernels of one evaluator: the interpreter's (built into the library) or a compiled plan's.
-enum KernelId { K_NOKEYS = 0, K_DENSE_SHARED, K_DENSE_GLOBAL, K_HASH, K_SELECT_COUNT, K_SELECT_WRITE, K_COUNT_ };
+enum KernelId { K_NOKEYS = 0, K_DENSE_SHARED, K_DENSE_GLOBAL, K_HASH, K_SELECT_COUNT, K_SELECT_WRITE, K_DENSE_PRIV, K_COUNT_ };
 struct KernelSet {
   CUfunction fn[K_COUNT_] = {};
   bool interp = true;

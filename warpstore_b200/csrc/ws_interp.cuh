@@ -167,6 +167,7 @@ static __device__ __noinline__ Word vmRun(const TInstr* code, int start, int len
 struct InterpEv {
   static constexpr int NK = WS_INTERP_KEYS, NA = WS_INTERP_AGGS, RW = 1 + 2 * WS_INTERP_AGGS, FRW = WS_INTERP_AGGS;
   static constexpr bool STAGED = false;
+  static constexpr int STAGE_BYTES = 0;
   const Launch& L;
   const ws_col_view* cv = nullptr;
   i64 r0 = 0;
@@ -181,6 +182,7 @@ struct InterpEv {
   WS_DI int woff(int a) const { return __ldg(L.woff + a); }
   WS_DI int fwoff(int a) const { return __ldg(L.fwoff + a); }
   WS_DI int fastBits() const { return L.fastBits; }
+  WS_DI int fastWords() const { return L.fastWords; }
   WS_DI bool keyInt(int k) const { return __ldg(L.keyInt + k) != 0; }
   WS_DI Word run(const int (&p)[2], int i) const { return vmRun(L.progs->code, p[0], p[1], cv, r0 + i, L.env); }
   WS_DI bool resInt(const int (&p)[2]) const { return L.progs->code[p[0] + p[1] - 1].rInt != 0; }

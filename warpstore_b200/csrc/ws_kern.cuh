@@ -518,6 +518,74 @@ __device__ void aggDenseReg(const Launch& L) {
   lastCtaReduce<Ev, RW>(L, ev, GR, sred);
 }
 
+// Few groups, register rows in shared memory: every thread owns G private rows laid out
+// [group][word][thread] (a warp's accesses are consecutive words: no bank conflicts), so adding a row
+// is one read-modify-write per word at a computed address: no atomics, no per-group predication.
+// Dynamic shared memory: [stages (staged scans)][private rows G * FRW * blockDim][spill G * NA * 2].
+// Each (group, word) is then reduced over the CTA's threads in a fixed order; partial rows per CTA,
+// the last CTA reduces them.
+template <class Ev>
+__device__ void aggDensePriv(const Launch& L) {
+  constexpr int RW = Ev::RW, FW = Ev::FRW;
+  extern __shared__ __align__(16) u64 wsSmem[];
+  __shared__ u64 sred[(kThreads / 32) * RW];
+  Ev ev(L);
+  const int G = (int)L.G, T = blockDim.x, tid = threadIdx.x;
+  const int fw = ev.fastWords();
+  u64* priv = wsSmem + (size_t)(L.stages > 1 ? L.stages : 0) * (Ev::STAGE_BYTES / 8);
+  u64* spill = priv + (size_t)G * fw * T;
+  {
+    u64 id[FW];
+    fastIdentity(ev, id);
+    for (int g = 0; g < G; ++g)
+      for (int j = 0; j < fw; ++j) priv[((size_t)g * fw + j) * T + tid] = id[j];
+    for (int j = tid; j < G * 2 * Ev::NA; j += T) spill[j] = 0;
+  }
+  __syncthreads();
+  scanRows(L, ev, [&](int i, int, i64) {
+    i64 gi;
+    if (!denseIndex(L, ev, i, gi)) {
+      L.err[0] = 1;
+      return;
+    }
+    u64 x[FW];
+    fastOfInput(ev, i, x, spill + gi * 2 * Ev::NA);
+    u64* p = priv + (size_t)gi * fw * T + tid;
+#pragma unroll
+    for (int a = 0; a < Ev::NA; ++a) {
+      if (a >= ev.na()) break;
+      const int o = ev.fwoff(a);
+      u64* q = p + (size_t)o * T;
+      switch (ev.kind(a)) {
+        case SK_COUNT: case SK_ISUM: *q += x[o]; break;
+        case SK_IMIN: case SK_DMIN: if ((i64)x[o] < (i64)*q) *q = x[o]; break;
+        case SK_IMAX: case SK_DMAX: if ((i64)x[o] > (i64)*q) *q = x[o]; break;
+        case SK_DSUM: *q = (u64)__double_as_longlong(__longlong_as_double((i64)*q) + __longlong_as_double((i64)x[o])); break;
+        default: break;
+      }
+    }
+  });
+  __syncthreads();
+  const int rw = ev.rowWords();
+  for (int g = 0; g < G; ++g) {
+    u64 f[FW];
+#pragma unroll
+    for (int j = 0; j < FW; ++j)
+      if (j < fw) f[j] = priv[((size_t)g * fw + j) * T + tid];
+    u64 w[RW];
+    rowIdentity(ev, w);
+    fastExpand(ev, f, w);
+    blockReduceRow(ev, w, sred);
+    if (tid == 0) {
+      const u64* sp = spill + (size_t)g * 2 * Ev::NA;
+      for (int a = 0; a < ev.na(); ++a)
+        if (ev.kind(a) == SK_ISUM) add128w(w[ev.woff(a)], *(i64*)&w[ev.woff(a) + 1], sp[2 * a], (i64)sp[2 * a + 1]);
+      for (int j = 1; j < rw; ++j) L.part[((size_t)blockIdx.x * G + g) * rw + j] = w[j];
+    }
+  }
+  lastCtaReduce<Ev, RW>(L, ev, G, sred);
+}
+
 // Medium G: the CTA's rows [G][rw] live in shared memory (rows' key words unused) and take shared
 // atomics; at the end each non-empty group is merged into the global rows with global atomics.
 template <class Ev>
@@ -776,6 +844,7 @@ __device__ void selectWrite(const Launch& L) {
 #define WS_K_NOKEYS(EV, PREFIX) WS_K_ENTRY(PREFIX, nokeys, ws::aggNoKeys<EV>)
 #define WS_K_DENSE_SHARED(EV, PREFIX) WS_K_ENTRY(PREFIX, dense_shared, ws::aggDenseShared<EV>)
 #define WS_K_DENSE_GLOBAL(EV, PREFIX) WS_K_ENTRY(PREFIX, dense_global, ws::aggDenseGlobal<EV>)
+#define WS_K_DENSE_PRIV(EV, PREFIX) WS_K_ENTRY(PREFIX, dense_priv, ws::aggDensePriv<EV>)
 #define WS_K_HASH(EV, PREFIX) WS_K_ENTRY(PREFIX, hash, ws::aggHash<EV>)
 #define WS_K_SELECT_COUNT(EV, PREFIX) WS_K_ENTRY(PREFIX, select_count, ws::selectCount<EV>)
 #define WS_K_SELECT_WRITE(EV, PREFIX) WS_K_ENTRY(PREFIX, select_write, ws::selectWrite<EV>)
@@ -783,6 +852,7 @@ __device__ void selectWrite(const Launch& L) {
   WS_K_NOKEYS(EV, PREFIX)                  \
   WS_K_DENSE_SHARED(EV, PREFIX)            \
   WS_K_DENSE_GLOBAL(EV, PREFIX)            \
+  WS_K_DENSE_PRIV(EV, PREFIX)              \
   WS_K_HASH(EV, PREFIX)                    \
   WS_K_SELECT_COUNT(EV, PREFIX)            \
   WS_K_SELECT_WRITE(EV, PREFIX)

@@ -15,7 +15,8 @@ const KernelSet& interpKernels() {
   static KernelSet ks = [] {
     KernelSet k;
     const void* syms[K_COUNT_] = {(const void*)wsi_nokeys, (const void*)wsi_dense_shared, (const void*)wsi_dense_global,
-                                  (const void*)wsi_hash, (const void*)wsi_select_count, (const void*)wsi_select_write};
+                                  (const void*)wsi_hash, (const void*)wsi_select_count, (const void*)wsi_select_write,
+                                  (const void*)wsi_dense_priv};
     for (int i = 0; i < K_COUNT_; ++i) {
       cudaFunction_t f;
       WS_CK(cudaGetFuncBySymbol(&f, syms[i]));
@@ -491,18 +492,22 @@ static void aggRun(ws_aggregator& A, const ws_expr_env& env, const ws_jit_progra
     }
     L.G = A.dense.G;
     const int64_t G = A.dense.G;
-    if (useJit && G <= 32 && G <= denseRegMaxGroups(A.plan)) {
-      CUfunction f = denseRegKernel(const_cast<ws_jit_program*>(jit), (int)G);
-      if (f) {
-        L.stages = S >= 2 ? S : 0;
-        const unsigned grid = persistentGrid(f, stageSmem, d.ntiles);
-        L.fastBits = fastBitsFor(d.ntiles, grid);
-        DBuf<u64> part((int64_t)grid * G * A.lay.rw);
-        L.part = part.p;
-        WS_CK(cudaMemsetAsync(A.ticket(), 0, 4, stream()));
-        launchScan(f, grid, stageSmem, L);
-        return;
-      }
+    // few groups: private register rows per thread in shared memory (+ staged tiles when they fit)
+    const size_t privBytes = (size_t)G * A.lay.frw * kThreads * 8 + (size_t)G * WS_MAX_AGGS * 16;
+    if (G * A.lay.frw <= 48 && ks.fn[K_DENSE_PRIV]) {
+      CUfunction f = ks.fn[K_DENSE_PRIV];
+      const size_t budget = 220 * 1024;
+      int S2 = stageBytes > 0 ? (int)std::min<int64_t>(maxStages, (int64_t)(budget - privBytes) / stageBytes) : 0;
+      if (S2 < 2) S2 = 0;
+      L.stages = S2;
+      const size_t smem = (size_t)S2 * stageBytes + privBytes;
+      const unsigned grid = persistentGrid(f, smem, d.ntiles);
+      L.fastBits = fastBitsFor(d.ntiles, grid);
+      DBuf<u64> part((int64_t)grid * G * A.lay.rw);
+      L.part = part.p;
+      WS_CK(cudaMemsetAsync(A.ticket(), 0, 4, stream()));
+      launchScan(f, grid, smem, L);
+      return;
     }
     const size_t smem = (size_t)G * A.lay.rw * 8;
     if (smem <= 96 * 1024 && ks.fn[K_DENSE_SHARED]) {
