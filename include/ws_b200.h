@@ -140,10 +140,9 @@ int ws_jit_end_query(double query_ms, ws_jit_query_info* info);
 int ws_codegen_source(const ws_expr_env* env, int ncols, const ws_agg_plan* plan, int fn, char* buf, size_t size,
                       size_t* needed);
 /* Compiles a plan's module with NVRTC for sm_<arch_sm> without loading it (host only, no device):
- * a build check of the generated code.  dense_groups > 0 also compiles the register-accumulator
- * dense kernel for that many groups. */
-int ws_codegen_compile_check(const ws_expr_env* env, int ncols, const ws_agg_plan* plan, int fn, int dense_groups,
-                             int arch_sm, size_t* cubin_bytes);
+ * a build check of the generated code. */
+int ws_codegen_compile_check(const ws_expr_env* env, int ncols, const ws_agg_plan* plan, int fn, int arch_sm,
+                             size_t* cubin_bytes);
 
 /* ---- introspection */
 /* Layout check: out[0..] = sizeof / offsetof values of the ABI structs as this library sees them. */

@@ -76,7 +76,7 @@ SIGNATURES = {
     "ws_codegen_source": (C.c_int, [C.POINTER(abi.ExprEnv), C.c_int, C.POINTER(abi.AggPlan), C.c_int, C.c_char_p,
                                     C.c_size_t, C.POINTER(C.c_size_t)]),
     "ws_codegen_compile_check": (C.c_int, [C.POINTER(abi.ExprEnv), C.c_int, C.POINTER(abi.AggPlan), C.c_int, C.c_int,
-                                           C.c_int, C.POINTER(C.c_size_t)]),
+                                           C.POINTER(C.c_size_t)]),
     "ws_abi_layout": (C.c_int, [I64P, C.c_int]),
     "ws_kernel_launches": (C.c_int64, []),
 }

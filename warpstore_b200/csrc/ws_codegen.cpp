@@ -56,6 +56,20 @@ struct Gen {
   int ncols;
   std::map<int, ColUse> cols;
   std::set<int> iconsts, dconsts;
+  // common subexpressions of keys and aggregates: computed once per row into temporaries (prep)
+  bool cse = false;
+  std::map<std::string, std::string> tempOf;
+  std::vector<std::pair<std::string, bool>> temps;  // (expression, is int) in dependency order
+
+  Sym memo(const Sym& r) {
+    if (!cse) return r;
+    auto it = tempOf.find(r.e);
+    if (it != tempOf.end()) return {it->second, r.isInt};
+    const std::string name = "t" + std::to_string(temps.size());
+    tempOf.emplace(r.e, name);
+    temps.emplace_back(r.e, r.isInt);
+    return {name, r.isInt};
+  }
 
   void useCol(int c, bool vecOnly) {
     auto it = cols.find(c);
@@ -72,6 +86,12 @@ struct Gen {
   std::string cv(int c) { return "c" + std::to_string(c) + "[i]"; }
 
   Sym node(const TypedProg& t, int ni) {
+    const TNode& n = t.nodes[ni];
+    const Sym r = node0(t, ni);
+    if (n.op == WS_OP_COL || n.op == WS_OP_COLRAW || n.op == WS_OP_CONST) return r;
+    return memo(r);
+  }
+  Sym node0(const TypedProg& t, int ni) {
     const TNode& n = t.nodes[ni];
     auto kid = [&](int k) { return node(t, n.kid[k]); };
     const std::string arg = std::to_string(n.arg);
@@ -201,6 +221,7 @@ std::string genEvaluator(const ws_expr_env& env, int ncols, const ws_agg_plan& p
   SlotLayout lay;
   if (agg) {
     lay = layoutOf(plan);
+    g.cse = true;
     for (int k = 0; k < plan.nkeys; ++k) keys.push_back(g.prog(plan.keys[k]));
     for (int a = 0; a < plan.naggs; ++a) {
       if (plan.ops[a] == WS_AGG_COUNT || lay.kind[a] == SK_NONE) {
@@ -216,6 +237,7 @@ std::string genEvaluator(const ws_expr_env& env, int ncols, const ws_agg_plan& p
       }
       aggs.push_back(g.prog(plan.aggs[a]));
     }
+    g.cse = false;
   }
   const int nk = agg ? plan.nkeys : 0, na = agg ? plan.naggs : 1;
   std::ostringstream o;
@@ -250,6 +272,7 @@ std::string genEvaluator(const ws_expr_env& env, int ncols, const ws_agg_plan& p
   o << "  const ws::Launch& L;\n  int* ovf;\n  bool fastOk;\n  ws::i64 rb;\n";
   for (int k : g.iconsts) o << "  ws::i64 ik" << k << ";\n";
   for (int k : g.dconsts) o << "  double k" << k << ";\n";
+  for (size_t j = 0; j < g.temps.size(); ++j) o << "  " << (g.temps[j].second ? "ws::i64" : "double") << " t" << j << ";\n";
   for (auto& [c, u] : g.cols) {
     o << "  ws::ColRef v" << c << ";\n";
     if (!u.vec) o << "  " << valType(u) << " c" << c << "[4];\n";
@@ -269,7 +292,6 @@ std::string genEvaluator(const ws_expr_env& env, int ncols, const ws_agg_plan& p
   if (agg)
     for (int a = 0; a < na; ++a) o << " case " << a << ": return " << lay.woff[a] << ";";
   o << " } return 0; }\n";
-  o << "  __device__ __forceinline__ int fastBits() const { return L.fastBits; }\n";
   o << "  __device__ __forceinline__ int fastWords() const { return " << std::max(agg ? lay.frw : 1, 1) << "; }\n";
   o << "  __device__ __forceinline__ int fwoff(int a) const { switch (a) {";
   if (agg)
@@ -333,6 +355,9 @@ std::string genEvaluator(const ws_expr_env& env, int ncols, const ws_agg_plan& p
       o << "    ws::stage4i64(" << a << "," << src << ");\n";
     }
   }
+  o << "  }\n";
+  o << "  __device__ __forceinline__ void prep(int i) {\n";
+  for (size_t j = 0; j < g.temps.size(); ++j) o << "    t" << j << " = " << g.temps[j].first << ";\n";
   o << "  }\n";
   o << "  __device__ __forceinline__ bool where(int i) const { return "
     << (where.isInt ? "(" + where.e + ") != 0" : "ws::truthy(" + where.e + ")") << "; }\n";
@@ -525,33 +550,6 @@ void compileAndPublish(const std::shared_ptr<ws_jit_program>& p) {
 
 }  // namespace
 
-// Register accumulators per thread: G rows of rw words must stay well inside the register file.
-int denseRegMaxGroups(const ws_agg_plan& plan) {
-  const SlotLayout lay = layoutOf(plan);
-  const int words = lay.rw - 1;
-  return words <= 0 ? 0 : std::max(0, 72 / words);
-}
-
-CUfunction denseRegKernel(ws_jit_program* p, int G) {
-  std::lock_guard<std::mutex> g(p->mu);
-  auto it = p->denseReg.find(G);
-  if (it != p->denseReg.end()) return it->second;
-  CUfunction f = nullptr;
-  try {
-    const std::string body = p->source +
-                             "extern \"C\" __global__ void __launch_bounds__(ws::kThreads) wsq_dense_reg(const __grid_constant__ ws::Launch L) "
-                             "{ ws::aggDenseReg<QEv, " + std::to_string(G) + ">(L); }\n";
-    CUmodule m = compileModule(body, nullptr);
-    p->variantModules.push_back(m);
-    WS_CKD(drv().moduleGetFunction(&f, m, "wsq_dense_reg"));
-  } catch (const std::exception& e) {
-    fprintf(stderr, "[warpstore_b200] dense variant failed to compile: %s\n", e.what());
-    f = nullptr;
-  }
-  p->denseReg[G] = f;
-  return f;
-}
-
 }  // namespace ws
 
 using namespace ws;
@@ -656,13 +654,10 @@ int ws_codegen_source(const ws_expr_env* env, int ncols, const ws_agg_plan* plan
   });
 }
 
-int ws_codegen_compile_check(const ws_expr_env* env, int ncols, const ws_agg_plan* plan, int fn, int dense_groups,
-                             int arch_sm, size_t* cubin_bytes) {
+int ws_codegen_compile_check(const ws_expr_env* env, int ncols, const ws_agg_plan* plan, int fn, int arch_sm,
+                             size_t* cubin_bytes) {
   return guardedCall([&] {
-    std::string body = genEvaluator(*env, ncols, *plan, fn, nullptr) + kindKernels(fn);
-    if (dense_groups > 0)
-      body += "extern \"C\" __global__ void __launch_bounds__(ws::kThreads) wsq_dense_reg(const __grid_constant__ ws::Launch L) "
-              "{ ws::aggDenseReg<QEv, " + std::to_string(dense_groups) + ">(L); }\n";
+    const std::string body = genEvaluator(*env, ncols, *plan, fn, nullptr) + kindKernels(fn);
     const std::string image = nvrtcCubin("#include \"ws_kern.cuh\"\n" + body, archOpts(arch_sm));
     if (cubin_bytes) *cubin_bytes = image.size();
   });

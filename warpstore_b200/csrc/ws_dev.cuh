@@ -549,8 +549,6 @@ struct Launch {
   int nkeys, naggs, rowWords; // interpreter only (JIT: compile-time)
   int fastWords;              // interpreter only: words of a register row
   int stages;                 // shared-memory stages of staged scans (0: loads straight from global memory)
-  int fastBits;               // register-row integer sums take values in [-2^fastBits, 2^fastBits) as int64:
-                              // with at most 2^(62 - fastBits) rows per thread they cannot overflow
   // aggregation outputs
   u64* part;                  // per-CTA partial rows
   u64* rows;                  // result rows

@@ -141,8 +141,7 @@ unsigned persistentGrid(CUfunction f, size_t smem, int64_t ntiles);
 }  // namespace ws
 
 // A compiled plan (the engine's JitProgram, src/jit.h:16-31): generated evaluator source, its module
-// and kernels, state and statistics.  Variants (a dense GROUP BY specialised for a group count) are
-// compiled on first use and cached with the plan.
+// and kernels, state and statistics.
 struct ws_jit_program {
   int id = 0;
   int fnKind = 0;
@@ -154,15 +153,7 @@ struct ws_jit_program {
   ws::KernelSet kernels;
   CUmodule module = nullptr;
   std::mutex mu;
-  std::map<int, CUfunction> denseReg;  // group count -> register-accumulator dense kernel
-  std::vector<CUmodule> variantModules;
   int64_t execs = 0;
   double totalMs = 0, lastMs = 0;
 };
 
-namespace ws {
-// The register-accumulator dense kernel of a compiled plan for G groups (compiled on first use);
-// nullptr when G is too large for registers or compilation failed.
-CUfunction denseRegKernel(ws_jit_program* p, int G);
-int denseRegMaxGroups(const ws_agg_plan& plan);
-}  // namespace ws

@@ -175,13 +175,13 @@ struct InterpEv {
   __device__ InterpEv(const Launch& l) : L(l) {}
   WS_DI void bind(const Launch&, int b) { cv = L.cols + (i64)b * L.ncols; }
   WS_DI void load(i64 r, bool, int) { r0 = r; }
+  WS_DI void prep(int) {}
   WS_DI int nk() const { return L.nkeys; }
   WS_DI int na() const { return L.naggs; }
   WS_DI int rowWords() const { return L.rowWords; }
   WS_DI int kind(int a) const { return __ldg(L.kinds + a); }
   WS_DI int woff(int a) const { return __ldg(L.woff + a); }
   WS_DI int fwoff(int a) const { return __ldg(L.fwoff + a); }
-  WS_DI int fastBits() const { return L.fastBits; }
   WS_DI int fastWords() const { return L.fastWords; }
   WS_DI bool keyInt(int k) const { return __ldg(L.keyInt + k) != 0; }
   WS_DI Word run(const int (&p)[2], int i) const { return vmRun(L.progs->code, p[0], p[1], cv, r0 + i, L.env); }

@@ -54,7 +54,10 @@ WS_DI void forEachRow(const Launch& L, Ev& ev, F&& f) {
     if (del) live &= ~(__ldg(del + (r0 >> 5)) >> (r0 & 31)) & 0xfu;
 #pragma unroll
     for (int i = 0; i < 4; ++i)
-      if (((live >> i) & 1u) && ev.where(i)) f(i, b, r0 + i);
+      if (((live >> i) & 1u) && ev.where(i)) {
+        ev.prep(i);
+        f(i, b, r0 + i);
+      }
   }
 }
 
@@ -140,7 +143,10 @@ WS_DI void forEachRowStaged(const Launch& L, Ev& ev, unsigned char* stages, int 
       if (del) live &= ~(__ldg(del + (r0 >> 5)) >> (r0 & 31)) & 0xfu;
 #pragma unroll
       for (int i = 0; i < 4; ++i)
-        if (((live >> i) & 1u) && ev.where(i)) f(i, b, r0 + i);
+        if (((live >> i) & 1u) && ev.where(i)) {
+          ev.prep(i);
+          f(i, b, r0 + i);
+        }
     }
     __syncthreads();  // stage s consumed: it may be refilled
   }
@@ -161,9 +167,9 @@ WS_DI void scanRows(const Launch& L, Ev& ev, F&& f) {
 
 // ------------------------------------------------------------------ register rows
 // Per-thread accumulators of the no-key and dense kernels: one word per slot (fwoff).  An integer SUM
-// keeps an int64 sum of the values in [-2^fastBits, 2^fastBits), where fastBits is set per launch so
-// that a thread's rows (at most 4 per tile it owns) can never overflow it; a larger value goes exactly
-// into the CTA's shared int128 spill counter of its (group, slot).
+// adds into an int64 word; when an addition overflows it (signed), the word keeps the wrapped value
+// and +-1 goes to the high word of the CTA's shared int128 spill counter of its (group, slot), so the
+// exact sum is word + 2^64 * spill at the end.
 template <class Ev>
 WS_DI void fastIdentity(const Ev& ev, u64* w) {
 #pragma unroll
@@ -180,9 +186,9 @@ WS_DI void fastIdentity(const Ev& ev, u64* w) {
     }
   }
 }
-// The register-row contribution of row i (spilling large integer values into spill[slot][2]).
+// The register-row contribution of row i (NULL arguments: the slot's identity).
 template <class Ev>
-WS_DI void fastOfInput(const Ev& ev, int i, u64* x, u64* spill) {
+WS_DI void fastOfInput(const Ev& ev, int i, u64* x) {
   fastIdentity(ev, x);
 #pragma unroll
   for (int a = 0; a < Ev::NA; ++a) {
@@ -190,16 +196,7 @@ WS_DI void fastOfInput(const Ev& ev, int i, u64* x, u64* spill) {
     const int o = ev.fwoff(a);
     switch (ev.kind(a)) {
       case SK_COUNT: x[o] = 1; break;
-      case SK_ISUM: {
-        i64 v;
-        if (ev.ival(a, i, v)) {
-          const u64 lim = 1ull << ev.fastBits();
-          if ((u64)v + lim < 2 * lim) x[o] = (u64)v;
-          else atomicAdd128(spill + 2 * a, (i64*)(spill + 2 * a + 1), (u64)v, v >> 63);
-        }
-        break;
-      }
-      case SK_IMIN: case SK_IMAX: {
+      case SK_ISUM: case SK_IMIN: case SK_IMAX: {
         i64 v;
         if (ev.ival(a, i, v)) x[o] = (u64)v;
         break;
@@ -218,14 +215,22 @@ WS_DI void fastOfInput(const Ev& ev, int i, u64* x, u64* spill) {
     }
   }
 }
+// *w += x for an int64 SUM word, carrying a signed overflow into the spill's high word.
+WS_DI void addCarry(u64* w, u64 x, u64* spillHi) {
+  const u64 old = *w, r = old + x;
+  if ((i64)((old ^ r) & (x ^ r)) < 0) atomicAdd(spillHi, (i64)x < 0 ? ~0ull : 1ull);
+  *w = r;
+}
+// w += x (register rows); spill = this group's [slot][2] int128 counters
 template <class Ev>
-WS_DI void fastCombine(const Ev& ev, u64* w, const u64* x) {
+WS_DI void fastCombine(const Ev& ev, u64* w, const u64* x, u64* spill) {
 #pragma unroll
   for (int a = 0; a < Ev::NA; ++a) {
     if (a >= ev.na()) break;
     const int o = ev.fwoff(a);
     switch (ev.kind(a)) {
-      case SK_COUNT: case SK_ISUM: w[o] += x[o]; break;
+      case SK_COUNT: w[o] += x[o]; break;
+      case SK_ISUM: addCarry(&w[o], x[o], spill + 2 * a + 1); break;
       case SK_IMIN: case SK_DMIN: if ((i64)x[o] < (i64)w[o]) w[o] = x[o]; break;
       case SK_IMAX: case SK_DMAX: if ((i64)x[o] > (i64)w[o]) w[o] = x[o]; break;
       case SK_DSUM:
@@ -444,8 +449,8 @@ __device__ void aggNoKeys(const Launch& L) {
   fastIdentity(ev, f);
   scanRows(L, ev, [&](int i, int, i64) {
     u64 x[FW];
-    fastOfInput(ev, i, x, spill);
-    fastCombine(ev, f, x);
+    fastOfInput(ev, i, x);
+    fastCombine(ev, f, x, spill);
   });
   u64 w[RW];
   rowIdentity(ev, w);
@@ -464,58 +469,17 @@ __device__ void aggNoKeys(const Launch& L) {
 // ------------------------------------------------------------------ dense GROUP BY
 template <class Ev>
 WS_DI bool denseIndex(const Launch& L, const Ev& ev, int i, i64& g) {
-  g = 0;
+  // ranges and G are below 2^26 (the dense limit), so the index arithmetic fits 32 bits
+  unsigned gg = 0;
 #pragma unroll
   for (int k = 0; k < Ev::NK; ++k) {
     if (k >= ev.nk()) break;
     const i64 d = ev.ikey(k, i) - L.kmin[k];
     if ((u64)d >= (u64)L.range[k]) return false;
-    g += d * L.stride[k];
+    gg += (unsigned)d * (unsigned)L.stride[k];
   }
-  return g < L.G;
-}
-
-// Few groups: every thread keeps all G register rows (GR = G, compile-time); a row is added to its
-// group's row with predication, no atomics.  Partials per CTA, the last CTA reduces them.
-template <class Ev, int GR>
-__device__ void aggDenseReg(const Launch& L) {
-  constexpr int RW = Ev::RW, FW = Ev::FRW;
-  __shared__ u64 sred[(kThreads / 32) * RW];
-  __shared__ u64 spill[GR * 2 * Ev::NA];
-  Ev ev(L);
-  for (int j = threadIdx.x; j < GR * 2 * Ev::NA; j += blockDim.x) spill[j] = 0;
-  __syncthreads();
-  u64 f[GR][FW];
-#pragma unroll
-  for (int g = 0; g < GR; ++g) fastIdentity(ev, f[g]);
-  scanRows(L, ev, [&](int i, int, i64) {
-    i64 gi;
-    if (!denseIndex(L, ev, i, gi)) {
-      L.err[0] = 1;
-      return;
-    }
-    u64 x[FW];
-    fastOfInput(ev, i, x, spill + gi * 2 * Ev::NA);
-#pragma unroll
-    for (int g = 0; g < GR; ++g)
-      if (gi == g) fastCombine(ev, f[g], x);
-  });
-  __syncthreads();
-  const int rw = ev.rowWords();
-#pragma unroll
-  for (int g = 0; g < GR; ++g) {
-    u64 w[RW];
-    rowIdentity(ev, w);
-    fastExpand(ev, f[g], w);
-    blockReduceRow(ev, w, sred);
-    if (threadIdx.x == 0) {
-      const u64* sp = spill + g * 2 * Ev::NA;
-      for (int a = 0; a < ev.na(); ++a)
-        if (ev.kind(a) == SK_ISUM) add128w(w[ev.woff(a)], *(i64*)&w[ev.woff(a) + 1], sp[2 * a], (i64)sp[2 * a + 1]);
-      for (int j = 1; j < rw; ++j) L.part[((size_t)blockIdx.x * GR + g) * rw + j] = w[j];
-    }
-  }
-  lastCtaReduce<Ev, RW>(L, ev, GR, sred);
+  g = gg;
+  return gg < (unsigned)L.G;
 }
 
 // Few groups, register rows in shared memory: every thread owns G private rows laid out
@@ -549,7 +513,8 @@ __device__ void aggDensePriv(const Launch& L) {
       return;
     }
     u64 x[FW];
-    fastOfInput(ev, i, x, spill + gi * 2 * Ev::NA);
+    fastOfInput(ev, i, x);
+    u64* sp = spill + gi * 2 * Ev::NA;
     u64* p = priv + (size_t)gi * fw * T + tid;
 #pragma unroll
     for (int a = 0; a < Ev::NA; ++a) {
@@ -557,7 +522,8 @@ __device__ void aggDensePriv(const Launch& L) {
       const int o = ev.fwoff(a);
       u64* q = p + (size_t)o * T;
       switch (ev.kind(a)) {
-        case SK_COUNT: case SK_ISUM: *q += x[o]; break;
+        case SK_COUNT: *q += x[o]; break;
+        case SK_ISUM: addCarry(q, x[o], sp + 2 * a + 1); break;
         case SK_IMIN: case SK_DMIN: if ((i64)x[o] < (i64)*q) *q = x[o]; break;
         case SK_IMAX: case SK_DMAX: if ((i64)x[o] > (i64)*q) *q = x[o]; break;
         case SK_DSUM: *q = (u64)__double_as_longlong(__longlong_as_double((i64)*q) + __longlong_as_double((i64)x[o])); break;

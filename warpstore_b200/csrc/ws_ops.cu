@@ -320,14 +320,6 @@ static BatchDesc uploadBatches(int nb, int ncols, const int64_t* bn, const uint3
   return d;
 }
 
-// fastBits for a grid: each thread adds at most 4 rows per tile it owns (see fastOfInput).
-static int fastBitsFor(int64_t ntiles, unsigned grid) {
-  const int64_t rows = 4 * ((ntiles + grid - 1) / grid);
-  int lg = 0;
-  while ((1ll << lg) < rows) ++lg;
-  return std::max(0, std::min(62, 62 - lg));
-}
-
 static void fillLaunch(Launch& L, const BatchDesc& d, int nb, int ncols, const ws_expr_env& env, const ws_agg_plan* plan,
                        const SlotLayout* lay) {
   memset(&L, 0, sizeof L);
@@ -477,7 +469,6 @@ static void aggRun(ws_aggregator& A, const ws_expr_env& env, const ws_jit_progra
     if (!f) throw Error("compiled plan has no aggregation kernel", WS_ERR_INTERNAL);
     L.stages = S >= 2 ? S : 0;
     const unsigned grid = persistentGrid(f, stageSmem, d.ntiles);
-    L.fastBits = fastBitsFor(d.ntiles, grid);
     DBuf<u64> part((int64_t)grid * A.lay.rw);
     L.part = part.p;
     WS_CK(cudaMemsetAsync(A.ticket(), 0, 4, stream()));
@@ -502,8 +493,7 @@ static void aggRun(ws_aggregator& A, const ws_expr_env& env, const ws_jit_progra
       L.stages = S2;
       const size_t smem = (size_t)S2 * stageBytes + privBytes;
       const unsigned grid = persistentGrid(f, smem, d.ntiles);
-      L.fastBits = fastBitsFor(d.ntiles, grid);
-      DBuf<u64> part((int64_t)grid * G * A.lay.rw);
+        DBuf<u64> part((int64_t)grid * G * A.lay.rw);
       L.part = part.p;
       WS_CK(cudaMemsetAsync(A.ticket(), 0, 4, stream()));
       launchScan(f, grid, smem, L);

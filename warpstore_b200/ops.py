@@ -112,10 +112,9 @@ def codegen_source(env: abi.ExprEnv, ncols: int, plan: abi.AggPlan, fn: int) -> 
     return buf.value.decode()
 
 
-def codegen_compile_check(env: abi.ExprEnv, ncols: int, plan: abi.AggPlan, fn: int, dense_groups: int = 0,
-                          arch_sm: int = 100) -> int:
+def codegen_compile_check(env: abi.ExprEnv, ncols: int, plan: abi.AggPlan, fn: int, arch_sm: int = 100) -> int:
     n = C.c_size_t()
-    check(lib().ws_codegen_compile_check(C.byref(env), ncols, C.byref(plan), fn, dense_groups, arch_sm, C.byref(n)))
+    check(lib().ws_codegen_compile_check(C.byref(env), ncols, C.byref(plan), fn, arch_sm, C.byref(n)))
     return n.value
 
 
