@@ -134,9 +134,9 @@ struct KernelSet {
 };
 const KernelSet& interpKernels();
 // Launches `f` with the Launch descriptor as its only parameter.
-void launchScan(CUfunction f, unsigned grid, size_t smem, const Launch& L);
+void launchScan(CUfunction f, unsigned grid, size_t smem, const Launch& L, int threads = kThreads);
 // Persistent grid: resident CTAs per SM x SMs, capped by the tile count.
-unsigned persistentGrid(CUfunction f, size_t smem, int64_t ntiles);
+unsigned persistentGrid(CUfunction f, size_t smem, int64_t ntiles, int threads = kThreads);
 
 }  // namespace ws
 

@@ -62,68 +62,71 @@ WS_DI void forEachRow(const Launch& L, Ev& ev, F&& f) {
 }
 
 // Same visit, with each tile's column chunks brought into shared memory by bulk asynchronous copies
-// (TMA engine) S-1 tiles ahead of use: a ring of S stages of Ev::STAGE_BYTES, one mbarrier per stage.
-// Thread 0 issues the copies; every thread waits on the stage's barrier, reads its 4 rows from shared
-// memory, and the CTA synchronizes before the stage is refilled.  Tiles that cannot be copied in bulk
-// (a batch's ragged last tile, a column not 16-byte aligned) are marked "direct" and read from global
-// memory as in forEachRow; their stage barrier still completes its phase (plain arrive), so the
-// parity of every stage advances once per use.  A wait that exceeds its limit sets err[2] and ends the
-// CTA's loop (all threads agree through __syncthreads_or).
+// (TMA engine), warp-specialized: the CTA has kThreads consumer threads plus one producer warp (the
+// last).  A ring of S stages of Ev::STAGE_BYTES has two mbarriers per stage: `full` (the producer's
+// arrive.expect_tx; the copies complete its transaction count) and `empty` (one arrival per consumer
+// warp once it has read the stage).  The producer refills a stage as soon as every consumer warp has
+// released it, so consumers never wait on a CTA-wide barrier.  Tiles that cannot be copied in bulk (a
+// batch's ragged last tile, a column not 16-byte aligned) are marked "direct": their full barrier gets
+// a plain arrive and the consumers read global memory as forEachRow does.  Every wait is bounded; one
+// that runs out sets err[2] and ends that thread's loop.
+constexpr int kStagedThreads = kThreads + 32;
+
 template <class Ev, class F>
 WS_DI void forEachRowStaged(const Launch& L, Ev& ev, unsigned char* stages, int S, F&& f) {
-  __shared__ __align__(8) u64 bars[8];
+  __shared__ __align__(8) u64 full[8], empty[8];
   __shared__ int smode[8];
   __shared__ typename Ev::Stage pst;  // the producer's view of its current batch
-  __shared__ int pbatch;
-  const int tid = threadIdx.x;
+  constexpr int kConsumerWarps = kThreads / 32;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0) {
-    for (int s = 0; s < S; ++s) mbarInit(smemAddr(&bars[s]), 1);
+    for (int s = 0; s < S; ++s) {
+      mbarInit(smemAddr(&full[s]), 1);
+      mbarInit(smemAddr(&empty[s]), kConsumerWarps);
+    }
     fenceMbarInit();
     fenceProxyAsync();
-    pbatch = -1;
   }
   __syncthreads();
   const i64 K = L.ntiles > (i64)blockIdx.x ? (L.ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
-  int pb = 0;  // producer batch cursor (thread 0)
-  auto issue = [&](i64 k) {
-    const i64 t = blockIdx.x + k * (i64)gridDim.x;
-    const int s = (int)(k % S);
-    while (t >= __ldg(L.tileStart + pb + 1)) ++pb;
-    if (pb != pbatch) {
-      Ev::stageBind(L, pb, pst);
-      pbatch = pb;
+  if (warp == kConsumerWarps) {  // ---- producer warp (one elected lane)
+    if (lane == 0) {
+      int pb = 0, pbatch = -1;
+      for (i64 k = 0; k < K; ++k) {
+        const int s = (int)(k % S);
+        if (k >= S && !mbarWait(smemAddr(&empty[s]), (unsigned)(((k / S) - 1) & 1))) {
+          L.err[2] = 1;
+          break;
+        }
+        const i64 t = blockIdx.x + k * (i64)gridDim.x;
+        while (t >= __ldg(L.tileStart + pb + 1)) ++pb;
+        if (pb != pbatch) {
+          Ev::stageBind(L, pb, pst);
+          pbatch = pb;
+        }
+        const i64 tr0 = (t - __ldg(L.tileStart + pb)) * kTile;
+        const bool bulk = pst.ok && tr0 + kTile <= __ldg(L.n + pb);
+        smode[s] = bulk;
+        const unsigned bar = smemAddr(&full[s]);
+        if (bulk) {
+          fenceProxyAsync();  // the stage was last read through the generic proxy
+          mbarArriveTx(bar, pst.bytes);
+          Ev::stageIssue(pst, tr0, smemAddr(stages + (size_t)s * Ev::STAGE_BYTES), bar);
+        } else {
+          mbarArrive(bar);
+        }
+      }
     }
-    const i64 tr0 = (t - __ldg(L.tileStart + pb)) * kTile;
-    const bool bulk = pst.ok && tr0 + kTile <= __ldg(L.n + pb);
-    smode[s] = bulk;
-    const unsigned bar = smemAddr(&bars[s]);
-    if (bulk) {
-      mbarArriveTx(bar, pst.bytes);
-      Ev::stageIssue(pst, tr0, smemAddr(stages + (size_t)s * Ev::STAGE_BYTES), bar);
-    } else {
-      mbarArrive(bar);
-    }
-  };
-  if (tid == 0) {
-    fenceProxyAsync();
-    for (i64 k = 0; k < S - 1 && k < K; ++k) issue(k);
+    __syncwarp();
+    return;
   }
+  // ---- consumer warps
   int b = 0, bound = -1;
   for (i64 k = 0; k < K; ++k) {
     const i64 t = blockIdx.x + k * (i64)gridDim.x;
     const int s = (int)(k % S);
-    if (tid == 0 && k + S - 1 < K) {
-      fenceProxyAsync();  // the stage being refilled was last read through the generic proxy
-      issue(k + S - 1);
-    }
-    const bool ok = mbarWait(smemAddr(&bars[s]), (unsigned)((k / S) & 1));
-    if (__syncthreads_or(!ok)) {
-      if (tid == 0) {
-        L.err[2] = 1;
-        // give the copies already issued for later stages their chance to land (bounded) before exit
-        for (i64 j = k + 1; j < K && j < k + S; ++j) mbarWait(smemAddr(&bars[j % S]), (unsigned)((j / S) & 1));
-      }
-      __syncthreads();
+    if (!mbarWait(smemAddr(&full[s]), (unsigned)((k / S) & 1))) {
+      L.err[2] = 1;
       break;
     }
     while (t >= __ldg(L.tileStart + b + 1)) ++b;
@@ -148,7 +151,8 @@ WS_DI void forEachRowStaged(const Launch& L, Ev& ev, unsigned char* stages, int 
           f(i, b, r0 + i);
         }
     }
-    __syncthreads();  // stage s consumed: it may be refilled
+    __syncwarp();
+    if (lane == 0) mbarArrive(smemAddr(&empty[s]));  // this warp is done with the stage
   }
 }
 
@@ -156,7 +160,7 @@ WS_DI void forEachRowStaged(const Launch& L, Ev& ev, unsigned char* stages, int 
 template <class Ev, class F>
 WS_DI void scanRows(const Launch& L, Ev& ev, F&& f) {
   if constexpr (Ev::STAGED) {
-    if (L.stages >= 2) {
+    if (L.stages >= 2 && blockDim.x == kStagedThreads) {
       extern __shared__ __align__(16) u64 wsSmem[];
       forEachRowStaged(L, ev, (unsigned char*)wsSmem, L.stages, f);
       return;
@@ -218,7 +222,8 @@ WS_DI void fastOfInput(const Ev& ev, int i, u64* x) {
 // *w += x for an int64 SUM word, carrying a signed overflow into the spill's high word.
 WS_DI void addCarry(u64* w, u64 x, u64* spillHi) {
   const u64 old = *w, r = old + x;
-  if ((i64)((old ^ r) & (x ^ r)) < 0) atomicAdd(spillHi, (i64)x < 0 ? ~0ull : 1ull);
+  const unsigned ho = (unsigned)(old >> 32), hx = (unsigned)(x >> 32), hr = (unsigned)(r >> 32);
+  if ((int)((ho ^ hr) & (hx ^ hr)) < 0) atomicAdd(spillHi, (int)hx < 0 ? ~0ull : 1ull);  // signed overflow
   *w = r;
 }
 // w += x (register rows); spill = this group's [slot][2] int128 counters
@@ -365,7 +370,7 @@ WS_DI void rowOfInput(const Ev& ev, int i, u64* w) {
 
 // Warp + block reduction of one accumulator row per thread into `out` (thread 0's view).
 template <class Ev, int RW>
-WS_DI void blockReduceRow(const Ev& ev, u64 (&w)[RW], u64* sred /* [kThreads/32][RW] */) {
+WS_DI void blockReduceRow(const Ev& ev, u64 (&w)[RW], u64* sred /* [kStagedThreads/32][RW] */) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int rw = ev.rowWords();
 #pragma unroll
@@ -381,7 +386,7 @@ WS_DI void blockReduceRow(const Ev& ev, u64 (&w)[RW], u64* sred /* [kThreads/32]
       if (j < rw) sred[warp * RW + j] = w[j];
   __syncthreads();
   if (warp == 0) {
-    if (lane < kThreads / 32) {
+    if (lane < (int)(blockDim.x >> 5)) {
 #pragma unroll
       for (int j = 0; j < RW; ++j)
         if (j < rw) w[j] = sred[lane * RW + j];
@@ -440,7 +445,7 @@ WS_DI void lastCtaReduce(const Launch& L, const Ev& ev, int nrows, u64* sred) {
 template <class Ev>
 __device__ void aggNoKeys(const Launch& L) {
   constexpr int RW = Ev::RW, FW = Ev::FRW;
-  __shared__ u64 sred[(kThreads / 32) * RW];
+  __shared__ u64 sred[(kStagedThreads / 32) * RW];
   __shared__ u64 spill[2 * Ev::NA];
   Ev ev(L);
   for (int j = threadIdx.x; j < 2 * Ev::NA; j += blockDim.x) spill[j] = 0;
@@ -490,20 +495,22 @@ WS_DI bool denseIndex(const Launch& L, const Ev& ev, int i, i64& g) {
 // the last CTA reduces them.
 template <class Ev>
 __device__ void aggDensePriv(const Launch& L) {
-  constexpr int RW = Ev::RW, FW = Ev::FRW;
+  constexpr int RW = Ev::RW, FW = Ev::FRW, T = kThreads;
   extern __shared__ __align__(16) u64 wsSmem[];
-  __shared__ u64 sred[(kThreads / 32) * RW];
+  __shared__ u64 sred[(kStagedThreads / 32) * RW];
   Ev ev(L);
-  const int G = (int)L.G, T = blockDim.x, tid = threadIdx.x;
+  const int G = (int)L.G, tid = threadIdx.x;
+  const bool owner = tid < T;  // the producer warp of a staged launch owns no rows
   const int fw = ev.fastWords();
   u64* priv = wsSmem + (size_t)(L.stages > 1 ? L.stages : 0) * (Ev::STAGE_BYTES / 8);
   u64* spill = priv + (size_t)G * fw * T;
   {
     u64 id[FW];
     fastIdentity(ev, id);
-    for (int g = 0; g < G; ++g)
-      for (int j = 0; j < fw; ++j) priv[((size_t)g * fw + j) * T + tid] = id[j];
-    for (int j = tid; j < G * 2 * Ev::NA; j += T) spill[j] = 0;
+    if (owner)
+      for (int g = 0; g < G; ++g)
+        for (int j = 0; j < fw; ++j) priv[((size_t)g * fw + j) * T + tid] = id[j];
+    for (int j = tid; j < G * 2 * Ev::NA; j += blockDim.x) spill[j] = 0;
   }
   __syncthreads();
   scanRows(L, ev, [&](int i, int, i64) {
@@ -535,9 +542,11 @@ __device__ void aggDensePriv(const Launch& L) {
   const int rw = ev.rowWords();
   for (int g = 0; g < G; ++g) {
     u64 f[FW];
+    fastIdentity(ev, f);
+    if (owner)
 #pragma unroll
-    for (int j = 0; j < FW; ++j)
-      if (j < fw) f[j] = priv[((size_t)g * fw + j) * T + tid];
+      for (int j = 0; j < FW; ++j)
+        if (j < fw) f[j] = priv[((size_t)g * fw + j) * T + tid];
     u64 w[RW];
     rowIdentity(ev, w);
     fastExpand(ev, f, w);
@@ -804,7 +813,7 @@ __device__ void selectWrite(const Launch& L) {
 // descriptor is a __grid_constant__ parameter: the evaluator keeps a reference to it without forcing a
 // per-thread copy.
 #define WS_K_ENTRY(PREFIX, NAME, BODY)                                                                    \
-  extern "C" __global__ void __launch_bounds__(ws::kThreads) PREFIX##_##NAME(const __grid_constant__ ws::Launch L) { \
+  extern "C" __global__ void __launch_bounds__(ws::kStagedThreads) PREFIX##_##NAME(const __grid_constant__ ws::Launch L) { \
     BODY(L);                                                                                               \
   }
 #define WS_K_NOKEYS(EV, PREFIX) WS_K_ENTRY(PREFIX, nokeys, ws::aggNoKeys<EV>)

@@ -468,11 +468,12 @@ static void aggRun(ws_aggregator& A, const ws_expr_env& env, const ws_jit_progra
     CUfunction f = ks.fn[K_NOKEYS];
     if (!f) throw Error("compiled plan has no aggregation kernel", WS_ERR_INTERNAL);
     L.stages = S >= 2 ? S : 0;
-    const unsigned grid = persistentGrid(f, stageSmem, d.ntiles);
+    const int threads = L.stages ? kStagedThreads : kThreads;
+    const unsigned grid = persistentGrid(f, stageSmem, d.ntiles, threads);
     DBuf<u64> part((int64_t)grid * A.lay.rw);
     L.part = part.p;
     WS_CK(cudaMemsetAsync(A.ticket(), 0, 4, stream()));
-    launchScan(f, grid, stageSmem, L);
+    launchScan(f, grid, stageSmem, L, threads);
     return;
   }
   if (A.isDense) {
@@ -491,12 +492,13 @@ static void aggRun(ws_aggregator& A, const ws_expr_env& env, const ws_jit_progra
       int S2 = stageBytes > 0 ? (int)std::min<int64_t>(maxStages, (int64_t)(budget - privBytes) / stageBytes) : 0;
       if (S2 < 2) S2 = 0;
       L.stages = S2;
+      const int threads = S2 ? kStagedThreads : kThreads;
       const size_t smem = (size_t)S2 * stageBytes + privBytes;
-      const unsigned grid = persistentGrid(f, smem, d.ntiles);
-        DBuf<u64> part((int64_t)grid * G * A.lay.rw);
+      const unsigned grid = persistentGrid(f, smem, d.ntiles, threads);
+      DBuf<u64> part((int64_t)grid * G * A.lay.rw);
       L.part = part.p;
       WS_CK(cudaMemsetAsync(A.ticket(), 0, 4, stream()));
-      launchScan(f, grid, smem, L);
+      launchScan(f, grid, smem, L, threads);
       return;
     }
     const size_t smem = (size_t)G * A.lay.rw * 8;

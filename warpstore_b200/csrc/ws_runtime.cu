@@ -146,17 +146,17 @@ uint8_t* pinnedStage(size_t bytes) {
 }
 void stageCopied() { WS_CK(cudaEventRecord(tStageEv, stream())); }
 
-void launchScan(CUfunction f, unsigned grid, size_t smem, const Launch& L) {
+void launchScan(CUfunction f, unsigned grid, size_t smem, const Launch& L, int threads) {
   if (smem > 0) WS_CKD(drv().funcSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)smem));
   void* args[] = {(void*)&L};
-  WS_CKD(drv().launchKernel(f, grid, 1, 1, kThreads, 1, 1, (unsigned)smem, (CUstream)stream(), args, nullptr));
+  WS_CKD(drv().launchKernel(f, grid, 1, 1, (unsigned)threads, 1, 1, (unsigned)smem, (CUstream)stream(), args, nullptr));
   countLaunch();
 }
 
-unsigned persistentGrid(CUfunction f, size_t smem, int64_t ntiles) {
+unsigned persistentGrid(CUfunction f, size_t smem, int64_t ntiles, int threads) {
   if (smem > 0) WS_CKD(drv().funcSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)smem));
   int per = 0;
-  WS_CKD(drv().occupancy(&per, f, kThreads, smem));
+  WS_CKD(drv().occupancy(&per, f, threads, smem));
   if (per < 1) throw Error("scan kernel does not fit on an SM (shared memory " + std::to_string(smem) + " B)", WS_ERR_INTERNAL);
   int64_t g = (int64_t)per * smCount();
   if (g > ntiles) g = ntiles;
