@@ -65,7 +65,7 @@ struct Gen {
     if (!cse) return r;
     auto it = tempOf.find(r.e);
     if (it != tempOf.end()) return {it->second, r.isInt};
-    const std::string name = "t" + std::to_string(temps.size());
+    const std::string name = "t" + std::to_string(temps.size()) + "[i]";
     tempOf.emplace(r.e, name);
     temps.emplace_back(r.e, r.isInt);
     return {name, r.isInt};
@@ -272,7 +272,7 @@ std::string genEvaluator(const ws_expr_env& env, int ncols, const ws_agg_plan& p
   o << "  const ws::Launch& L;\n  int* ovf;\n  bool fastOk;\n  ws::i64 rb;\n";
   for (int k : g.iconsts) o << "  ws::i64 ik" << k << ";\n";
   for (int k : g.dconsts) o << "  double k" << k << ";\n";
-  for (size_t j = 0; j < g.temps.size(); ++j) o << "  " << (g.temps[j].second ? "ws::i64" : "double") << " t" << j << ";\n";
+  for (size_t j = 0; j < g.temps.size(); ++j) o << "  " << (g.temps[j].second ? "ws::i64" : "double") << " t" << j << "[4];\n";
   for (auto& [c, u] : g.cols) {
     o << "  ws::ColRef v" << c << ";\n";
     if (!u.vec) o << "  " << valType(u) << " c" << c << "[4];\n";
@@ -356,8 +356,11 @@ std::string genEvaluator(const ws_expr_env& env, int ncols, const ws_agg_plan& p
     }
   }
   o << "  }\n";
-  o << "  __device__ __forceinline__ void prep(int i) {\n";
-  for (size_t j = 0; j < g.temps.size(); ++j) o << "    t" << j << " = " << g.temps[j].first << ";\n";
+  // per-row common subexpressions, computed for all 4 rows without branches (rows that did not pass
+  // the filter compute unused values and raise no overflow flag)
+  o << "  __device__ __forceinline__ void prep(int i, bool live) {\n";
+  if (!g.temps.empty()) o << "    int* ovf = live ? this->ovf : nullptr;\n";
+  for (size_t j = 0; j < g.temps.size(); ++j) o << "    t" << j << "[i] = " << g.temps[j].first << ";\n";
   o << "  }\n";
   o << "  __device__ __forceinline__ bool where(int i) const { return "
     << (where.isInt ? "(" + where.e + ") != 0" : "ws::truthy(" + where.e + ")") << "; }\n";

@@ -175,7 +175,7 @@ struct InterpEv {
   __device__ InterpEv(const Launch& l) : L(l) {}
   WS_DI void bind(const Launch&, int b) { cv = L.cols + (i64)b * L.ncols; }
   WS_DI void load(i64 r, bool, int) { r0 = r; }
-  WS_DI void prep(int) {}
+  WS_DI void prep(int, bool) {}
   WS_DI int nk() const { return L.nkeys; }
   WS_DI int na() const { return L.naggs; }
   WS_DI int rowWords() const { return L.rowWords; }

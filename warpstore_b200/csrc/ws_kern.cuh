@@ -32,6 +32,20 @@ WS_DI u64 mix64(u64 x) {  // splitmix64 finalizer (Steele, Lea, Flood 2014)
   return x;
 }
 
+// The 4 loaded rows of a thread: filter each live row, evaluate the common subexpressions of all 4
+// rows together (independent chains the scheduler can interleave), then hand the passing rows to f.
+template <class Ev, class F>
+WS_DI void rowGroup(Ev& ev, unsigned live, int b, i64 r0, F&& f) {
+  bool ok[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) ok[i] = ((live >> i) & 1u) && ev.where(i);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) ev.prep(i, ok[i]);
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+    if (ok[i]) f(i, b, r0 + i);
+}
+
 // Visits every live row (not deleted, passing the filter) of the tiles this CTA owns.
 // f(i, batch, row) is called with i = the row's position (0..3) in the evaluator's 4-row group.
 template <class Ev, class F>
@@ -52,12 +66,7 @@ WS_DI void forEachRow(const Launch& L, Ev& ev, F&& f) {
     unsigned live = (1u << nv) - 1;
     const uint32_t* del = L.del[b];
     if (del) live &= ~(__ldg(del + (r0 >> 5)) >> (r0 & 31)) & 0xfu;
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-      if (((live >> i) & 1u) && ev.where(i)) {
-        ev.prep(i);
-        f(i, b, r0 + i);
-      }
+    rowGroup(ev, live, b, r0, f);
   }
 }
 
@@ -144,12 +153,7 @@ WS_DI void forEachRowStaged(const Launch& L, Ev& ev, unsigned char* stages, int 
       unsigned live = (1u << nv) - 1;
       const uint32_t* del = L.del[b];
       if (del) live &= ~(__ldg(del + (r0 >> 5)) >> (r0 & 31)) & 0xfu;
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-        if (((live >> i) & 1u) && ev.where(i)) {
-          ev.prep(i);
-          f(i, b, r0 + i);
-        }
+      rowGroup(ev, live, b, r0, f);
     }
     __syncwarp();
     if (lane == 0) mbarArrive(smemAddr(&empty[s]));  // this warp is done with the stage
