@@ -1,0 +1,236 @@
+// Header-only C++ shim: the Warpstore engine's GPU operator interface (src/gpu.h, src/jit.h) over the
+// C ABI of libwarpstore_b200 (ws_b200.h).  An engine build that includes this header instead of
+// compiling src/gpu.cu and src/jit.cu calls the same C++ signatures; every call forwards to the C ABI
+// and C-ABI errors are rethrown as the engine's SqlError (define WS_GPU_THROW before including this
+// header; by default a std::runtime_error carrying the code is thrown).
+//
+// The engine's own devtypes.h defines ColView / ExprEnv / AggPlan / DenseSpec / Prog with the same
+// layout as ws_types.h (checked below); define WS_GPU_ENGINE_TYPES when it is included first.
+#pragma once
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "ws_b200.h"
+
+#ifndef WS_GPU_THROW
+namespace gdb {
+struct WsGpuError : std::runtime_error {
+  int code;
+  WsGpuError(const std::string& m, int c) : std::runtime_error(m), code(c) {}
+};
+}  // namespace gdb
+#define WS_GPU_THROW(msg, code) throw ::gdb::WsGpuError((msg), (code))
+#endif
+
+namespace gdb {
+
+#ifndef WS_GPU_ENGINE_TYPES
+using ColView = ws_col_view;
+using ExprEnv = ws_expr_env;
+using AggPlan = ws_agg_plan;
+using DenseSpec = ws_dense_spec;
+using Prog = ws_prog;
+#endif
+static_assert(sizeof(ColView) == sizeof(ws_col_view) && sizeof(ExprEnv) == sizeof(ws_expr_env) &&
+                  sizeof(AggPlan) == sizeof(ws_agg_plan) && sizeof(DenseSpec) == sizeof(ws_dense_spec),
+              "engine ABI structs and ws_types.h differ");
+
+inline void wsCheck(int rc) {
+  if (rc != WS_OK) WS_GPU_THROW(std::string(ws_last_error()), rc);
+}
+
+// ---- device runtime (src/gpu.h:12-56)
+inline void gpuInit() { wsCheck(ws_gpu_init()); }
+inline int gpuSmCount() { return ws_gpu_sm_count(); }
+inline int gpuArch() { return ws_gpu_arch(); }
+inline std::string gpuDescribe() {
+  char buf[256] = {};
+  wsCheck(ws_gpu_describe(buf, sizeof buf));
+  return buf;
+}
+inline void* devAlloc(size_t bytes) {
+  void* p = nullptr;
+  wsCheck(ws_dev_alloc(bytes, &p));
+  return p;
+}
+inline void devFree(void* p) { ws_dev_free(p); }
+inline void* tmpAlloc(size_t bytes) {
+  void* p = nullptr;
+  wsCheck(ws_tmp_alloc(bytes, &p));
+  return p;
+}
+inline void tmpFree(void* p) { ws_tmp_free(p); }
+inline void gpuTrimPool() { ws_gpu_trim_pool(); }
+inline void h2d(void* dst, const void* src, size_t b) { wsCheck(ws_h2d(dst, src, b)); }
+inline void d2h(void* dst, const void* src, size_t b) { wsCheck(ws_d2h(dst, src, b)); }
+inline void d2d(void* dst, const void* src, size_t b) { wsCheck(ws_d2d(dst, src, b)); }
+inline void gpuSync() { wsCheck(ws_gpu_sync()); }
+
+// RAII temp device array (src/gpu.h:59-79)
+template <class T>
+struct DevVec {
+  T* p = nullptr;
+  int64_t n = 0;
+  DevVec() = default;
+  explicit DevVec(int64_t count) : n(count) { p = count ? (T*)tmpAlloc(sizeof(T) * count) : nullptr; }
+  DevVec(T* q, int64_t count) : p(q), n(count) {}  // takes over a buffer returned by the C ABI
+  DevVec(const DevVec&) = delete;
+  DevVec& operator=(const DevVec&) = delete;
+  DevVec(DevVec&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr, o.n = 0; }
+  DevVec& operator=(DevVec&& o) noexcept {
+    if (this != &o) {
+      reset();
+      p = o.p, n = o.n;
+      o.p = nullptr, o.n = 0;
+    }
+    return *this;
+  }
+  ~DevVec() { reset(); }
+  void reset() {
+    if (p) tmpFree(p);
+    p = nullptr, n = 0;
+  }
+  std::vector<T> download(int64_t count = -1) const {
+    std::vector<T> v(count < 0 ? n : count);
+    if (!v.empty()) d2h(v.data(), p, sizeof(T) * v.size());
+    return v;
+  }
+};
+
+// ---- compiled plans (src/jit.h)
+using JitProgram = ws_jit_program;
+enum JitFn { JF_NOKEYS = WS_JF_NOKEYS, JF_GROUPED = WS_JF_GROUPED, JF_DENSE = WS_JF_DENSE, JF_FLAG = WS_JF_FLAG, JF_FLAGM = WS_JF_FLAGM };
+enum JitMode { JIT_OFF = WS_JIT_OFF, JIT_ON = WS_JIT_ON, JIT_SYNC = WS_JIT_SYNC };
+inline JitMode jitMode() { return (JitMode)ws_jit_mode(); }
+inline bool jitEnabled() { return jitMode() != JIT_OFF; }
+inline void jitSetMode(JitMode m) { ws_jit_set_mode(m); }
+inline void jitSetDefaultMode(JitMode m) { ws_jit_set_default_mode(m); }
+inline void jitSetCacheDir(const std::string& dir) { wsCheck(ws_jit_set_cache_dir(dir.c_str())); }
+inline const JitProgram* jitGet(const ExprEnv& env, int ncols, const AggPlan& plan, JitFn fn, const std::string& kind) {
+  const ws_jit_program* p = nullptr;
+  wsCheck(ws_jit_get((const ws_expr_env*)&env, ncols, (const ws_agg_plan*)&plan, fn, kind.c_str(), &p));
+  return p;
+}
+inline bool progIsInt(const ExprEnv& env, Prog p) { return ws_prog_is_int((const ws_expr_env*)&env, *(const ws_prog*)&p) != 0; }
+inline void jitBeginQuery(const std::string& sql) { ws_jit_begin_query(sql.c_str()); }
+inline ws_jit_query_info jitEndQuery(double queryMs) {
+  ws_jit_query_info i{};
+  ws_jit_end_query(queryMs, &i);
+  return i;
+}
+inline void jitClearCache() { ws_jit_clear_cache(); }
+
+// ---- aggregation (src/gpu.h:84-130)
+class GpuAggregator {
+ public:
+  GpuAggregator(const AggPlan& plan, int64_t capacity, const DenseSpec* dense = nullptr) : naggs_(plan.naggs), nkeys_(plan.nkeys) {
+    wsCheck(ws_agg_create((const ws_agg_plan*)&plan, capacity, (const ws_dense_spec*)dense, &h_));
+  }
+  ~GpuAggregator() { ws_agg_destroy(h_); }
+  GpuAggregator(const GpuAggregator&) = delete;
+  GpuAggregator& operator=(const GpuAggregator&) = delete;
+  void addBatch(const ExprEnv& env, int ncols, int64_t n, const uint32_t* del) {
+    wsCheck(ws_agg_add_batch(h_, (const ws_expr_env*)&env, ncols, n, del));
+  }
+  void run(const ExprEnv& env, const JitProgram* jit) { wsCheck(ws_agg_run(h_, (const ws_expr_env*)&env, jit)); }
+  void runWindow(const ExprEnv& env, const JitProgram* jit) { wsCheck(ws_agg_run_window(h_, (const ws_expr_env*)&env, jit)); }
+  int batches() const { return ws_agg_batches(h_); }
+  int windows() const { return ws_agg_windows(h_); }
+  int64_t rowsIn() const { return ws_agg_rows_in(h_); }
+  bool dense() const { return ws_agg_is_dense(h_) != 0; }
+  bool overflowed() {
+    int o = 0;
+    wsCheck(ws_agg_overflowed(h_, &o));
+    return o != 0;
+  }
+  int64_t fetch(std::vector<double>& keys, std::vector<double>& accs) {
+    int64_t g = 0;
+    int rc = ws_agg_fetch(h_, 0, nullptr, nullptr, nullptr, &g);
+    if (rc != WS_OK && rc != WS_ERR_SIZE) wsCheck(rc);
+    keys.resize((size_t)g * nkeys_);
+    accs.resize((size_t)g * naggs_);
+    wsCheck(ws_agg_fetch(h_, g, keys.data(), accs.data(), nullptr, &g));
+    hi_.assign(naggs_, 0);
+    ws_agg_sum_high(h_, hi_.data());
+    return g;
+  }
+  std::vector<uint8_t> sumBitsSlots() const {
+    std::vector<uint8_t> f(naggs_);
+    ws_agg_sum_bits_slots(h_, f.data());
+    return f;
+  }
+  const std::vector<int64_t>& sumHigh() const { return hi_; }
+  int64_t compact(DevVec<double>& keys, DevVec<double>& accs) {
+    double *k = nullptr, *a = nullptr;
+    int64_t g = 0;
+    wsCheck(ws_agg_compact(h_, &k, &a, &g));
+    keys = DevVec<double>(k, g * nkeys_);
+    accs = DevVec<double>(a, g * naggs_);
+    return g;
+  }
+  int64_t capacity() const { return ws_agg_capacity(h_); }
+  int64_t groupCount() {
+    int64_t g = 0;
+    wsCheck(ws_agg_group_count(h_, &g));
+    return g;
+  }
+
+ private:
+  ws_aggregator* h_ = nullptr;
+  int naggs_, nkeys_;
+  std::vector<int64_t> hi_;
+};
+
+// ---- selection / gathers (src/gpu.h:132-143, :170-172)
+inline int64_t gpuSelect(const ExprEnv& env, bool hasWhere, Prog where, int64_t n, const uint32_t* del, int32_t* outIdx,
+                         const JitProgram* jit = nullptr) {
+  int64_t c = 0;
+  wsCheck(ws_select((const ws_expr_env*)&env, hasWhere, *(const ws_prog*)&where, n, del, outIdx, jit, &c));
+  return c;
+}
+inline int64_t gpuSelectMulti(const ExprEnv& env, bool hasWhere, Prog where, const std::vector<int64_t>& bn,
+                              const std::vector<const uint32_t*>& bdel, const std::vector<ColView>& bcols, int ncols,
+                              DevVec<int32_t>& outIdx, std::vector<int64_t>& perBatch, const JitProgram* jit = nullptr) {
+  perBatch.assign(bn.size(), 0);
+  int32_t* idx = nullptr;
+  int64_t c = 0;
+  wsCheck(ws_select_multi((const ws_expr_env*)&env, hasWhere, *(const ws_prog*)&where, (int)bn.size(),
+                          (const int64_t*)bn.data(), bdel.data(), (const ws_col_view*)bcols.data(), ncols, &idx,
+                          (int64_t*)perBatch.data(), jit, &c));
+  outIdx = DevVec<int32_t>(idx, c);
+  return c;
+}
+template <class PType>
+inline void gpuGatherMulti(const std::vector<ColView>& src, const std::vector<int64_t>& boff, PType t, int esize,
+                           const int32_t* idx, int64_t m, void* dst) {
+  wsCheck(ws_gather_multi((const ws_col_view*)src.data(), (const int64_t*)boff.data(), (int)src.size(), (int)t, esize, idx, m, dst));
+}
+template <class PType>
+inline void gpuGather(const void* src, PType t, const int32_t* idx, int64_t m, void* dst) {
+  wsCheck(ws_gather(src, (int)t, idx, m, dst));
+}
+
+// ---- joins (src/gpu.h:178-186)
+inline int64_t gpuHashJoinParts(ColView buildKey, const std::vector<int64_t>& bOff, ColView probeKey,
+                                const std::vector<int64_t>& pOff, DevVec<int32_t>& outBuild, DevVec<int32_t>& outProbe,
+                                std::vector<int64_t>* outOff) {
+  int32_t *ob = nullptr, *op = nullptr;
+  int64_t m = 0;
+  std::vector<int64_t> off(pOff.size(), 0);
+  wsCheck(ws_hash_join_parts(*(const ws_col_view*)&buildKey, (const int64_t*)bOff.data(), (int)bOff.size() - 1,
+                             *(const ws_col_view*)&probeKey, (const int64_t*)pOff.data(), (int)pOff.size() - 1, &ob, &op,
+                             (int64_t*)off.data(), &m));
+  outBuild = DevVec<int32_t>(ob, m);
+  outProbe = DevVec<int32_t>(op, m);
+  if (outOff) *outOff = off;
+  return m;
+}
+inline int64_t gpuHashJoin(ColView buildKey, int64_t nb, ColView probeKey, int64_t np, DevVec<int32_t>& outBuild,
+                           DevVec<int32_t>& outProbe) {
+  return gpuHashJoinParts(buildKey, {0, nb}, probeKey, {0, np}, outBuild, outProbe, nullptr);
+}
+
+}  // namespace gdb

@@ -68,3 +68,32 @@ def test_jit_modes_are_per_thread(built):
     assert l.ws_jit_mode() == abi.JIT_SYNC
     assert seen[0] == abi.JIT_ON  # the default
     l.ws_jit_set_mode(-1)
+
+
+def test_cpp_shim_compiles_and_links(built, tmp_path):
+    """include/ws_gpu.hpp (the engine-side C++ interface over the C ABI) compiles and links."""
+    import subprocess
+    src = tmp_path / "shim.cpp"
+    src.write_text('''
+#include "ws_gpu.hpp"
+#include <cstdio>
+int main() {
+  gdb::AggPlan plan{};
+  plan.naggs = 1;
+  plan.ops[0] = WS_AGG_COUNT;
+  try {
+    gdb::gpuInit();
+    gdb::GpuAggregator agg(plan, 1024);
+    std::vector<double> k, a;
+    agg.fetch(k, a);
+  } catch (const gdb::WsGpuError& e) {
+    std::printf("error %d\\n", e.code);
+  }
+  return 0;
+}
+''')
+    exe = tmp_path / "shim"
+    r = subprocess.run(["g++", "-std=c++17", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe),
+                        "-L", os.path.join(ROOT, "warpstore_b200"), "-lwarpstore_b200",
+                        "-Wl,-rpath," + os.path.join(ROOT, "warpstore_b200")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr

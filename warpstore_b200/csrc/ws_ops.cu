@@ -458,9 +458,10 @@ static void aggRun(ws_aggregator& A, const ws_expr_env& env, const ws_jit_progra
   const KernelSet& ks = useJit ? jit->kernels : interpKernels();
   // Staged scans: a ring of 2..4 tile stages in shared memory (compiled plans only).
   const int stageBytes = useJit ? jit->stageBytes : 0;
-  static const int maxStages = [] {  // WARPSTORE_B200_STAGES: 0 reads tiles straight from global memory
+  static const int maxStages = [] {  // WARPSTORE_B200_STAGES: shared-memory tile stages (0: direct loads,
+                                      // measured faster for the dense scan, which then fits 2 CTAs per SM)
     const char* e = getenv("WARPSTORE_B200_STAGES");
-    return e ? std::max(0, std::min(8, atoi(e))) : 4;
+    return e ? std::max(0, std::min(8, atoi(e))) : 0;
   }();
   const int S = stageBytes > 0 ? (int)std::min<int64_t>(maxStages, (200 * 1024) / stageBytes) : 0;
   const size_t stageSmem = S >= 2 ? (size_t)S * stageBytes : 0;
