@@ -87,6 +87,23 @@ int ws_agg_sum_high(const ws_aggregator* agg, int64_t* out);
 /* Groups left in device memory, column-major (GpuAggregator::compact): keys[k * g + i], accs[a * g + i]. */
 int ws_agg_compact(ws_aggregator* agg, double** keys, double** accs, int64_t* ngroups);
 
+/* ---- aggregation without any allocation.  No counterpart in the reference: an addition for callers
+ * that may not allocate device memory (code running where the allocator is off limits, or under a
+ * memory budget owned by someone else).  Filter + aggregates without GROUP BY over the batches, like
+ * ws_agg_create / add_batch / run / fetch with nkeys = 0, but all scratch (batch descriptor, per-CTA
+ * partial rows, result row, control words) lives in one fixed array of WS_NOALLOC_SCRATCH_BYTES inside
+ * this library, held on every GPU that loads it until the process exits.  The caller passes the plan,
+ * the column views and `exact`, a host array of plan->naggs * 2 words that receives the result in the
+ * format of ws_agg_fetch's `exact`.  jit: a compiled WS_JF_NOKEYS plan, or null for the interpreter.
+ * Limits: the batch descriptor (about nb * (ncols * 16 + 32) bytes, plus 9 KiB interpreted) must fit
+ * 1 MiB, else WS_ERR_SIZE.  Every call shares the array and reinitialises it; calls that overlap on
+ * the GPU race, so serialise them.  The first call on each device looks up the array's address (do
+ * it before any stream capture). */
+#define WS_NOALLOC_SCRATCH_BYTES (4u << 20)
+int ws_agg_nokeys_noalloc(const ws_expr_env* env, int ncols, const ws_agg_plan* plan, const ws_jit_program* jit,
+                          int nb, const int64_t* bn, const uint32_t* const* bdel, const ws_col_view* bcols,
+                          int64_t* exact);
+
 /* ---- selection and gathers (src/gpu.h:132-143, :170-172) */
 int ws_select(const ws_expr_env* env, int has_where, ws_prog where, int64_t n, const uint32_t* del, int32_t* out_idx,
               const ws_jit_program* jit, int64_t* count);

@@ -51,6 +51,8 @@ SIGNATURES = {
     "ws_agg_sum_bits_slots": (C.c_int, [P, P]),
     "ws_agg_sum_high": (C.c_int, [P, P]),
     "ws_agg_compact": (C.c_int, [P, C.POINTER(P), C.POINTER(P), I64P]),
+    "ws_agg_nokeys_noalloc": (C.c_int, [C.POINTER(abi.ExprEnv), C.c_int, C.POINTER(abi.AggPlan), P, C.c_int, P, P,
+                                        P, P]),
     "ws_select": (C.c_int, [C.POINTER(abi.ExprEnv), C.c_int, abi.Prog, C.c_int64, P, P, P, I64P]),
     "ws_select_multi": (C.c_int, [C.POINTER(abi.ExprEnv), C.c_int, abi.Prog, C.c_int, P, P, P, C.c_int,
                                   C.POINTER(P), P, P, I64P]),

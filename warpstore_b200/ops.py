@@ -203,6 +203,20 @@ class GpuAggregator:
         return k.value, a.value, g.value
 
 
+def agg_nokeys_noalloc(env: abi.ExprEnv, ncols: int, plan: abi.AggPlan, batches: list, jit: int | None = None):
+    """Filter + aggregate without GROUP BY through ws_agg_nokeys_noalloc (no memory is allocated: the
+    library's fixed scratch array is used).  batches: [(n, deleted_ptr, [ColView])].  Returns the exact
+    words [naggs, 2] (the layout of GpuAggregator.fetch's exact output)."""
+    nb = len(batches)
+    bn = (C.c_int64 * max(nb, 1))(*[b[0] for b in batches])
+    bdel = (P * max(nb, 1))(*[b[1] or None for b in batches])
+    cols = [v for b in batches for v in b[2]]
+    arr = _views_array(cols)
+    out = np.zeros((plan.naggs, 2), dtype=np.int64)
+    check(lib().ws_agg_nokeys_noalloc(C.byref(env), ncols, C.byref(plan), jit, nb, bn, bdel, arr, out.ctypes.data))
+    return out
+
+
 # ------------------------------------------------------------------ selection / gathers / joins
 def _views_array(views: list) -> C.Array:
     arr = (abi.ColView * max(len(views), 1))()
@@ -255,7 +269,7 @@ def hash_join(build_key: abi.ColView, nb: int, probe_key: abi.ColView, np_: int)
     return hash_join_parts(build_key, [0, nb], probe_key, [0, np_])[:3]
 
 
-__all__ = ["DeviceBuffer", "GpuAggregator", "WsError", "device_to_array", "gather", "gather_multi", "gpu_init",
+__all__ = ["DeviceBuffer", "GpuAggregator", "WsError", "agg_nokeys_noalloc", "device_to_array", "gather", "gather_multi", "gpu_init",
            "hash_join", "hash_join_parts", "jit_get", "jit_info", "jit_set_cache_dir", "jit_set_default_mode",
            "jit_set_mode", "kernel_launches", "select_multi", "sync", "tmp_free", "codegen_source",
            "codegen_compile_check"]
