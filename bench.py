@@ -184,10 +184,7 @@ def run_ours(args, ws, rank, local):
 
     def step(i=None):
         agg = ops.GpuAggregator(aq.plan, cap, ds)
-        for n, _, views in batches:
-            for c, v in enumerate(views):
-                env.env.cols[c] = v
-            agg.add_batch(env.env, env.ncols, n)
+        agg.add_batches(env.ncols, batches)
         with torch.cuda.stream(stream):
             if i is not None:
                 ev[i][0].record(stream)
@@ -253,10 +250,7 @@ def run_ours(args, ws, rank, local):
             for h, d in zip(hosts, devs):
                 d.copy_(h, non_blocking=True)
         agg = ops.GpuAggregator(aq.plan, cap, ds)
-        for n, _, views in e2e_batches:
-            for c, v in enumerate(views):
-                env.env.cols[c] = v
-            agg.add_batch(env.env, env.ncols, n)
+        agg.add_batches(env.ncols, e2e_batches)
         agg.run(env.env, prog)
         keys, accs, exact = agg.fetch()
         d2h = keys.nbytes + exact.nbytes

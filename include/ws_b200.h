@@ -65,6 +65,10 @@ typedef struct ws_jit_program ws_jit_program;
 int ws_agg_create(const ws_agg_plan* plan, int64_t capacity, const ws_dense_spec* dense, ws_aggregator** out);
 void ws_agg_destroy(ws_aggregator* agg);
 int ws_agg_add_batch(ws_aggregator* agg, const ws_expr_env* env, int ncols, int64_t n, const uint32_t* del);
+/* Many batches in one call (batch b: bn[b] rows, deleted bitmap bdel[b], views bcols[b * ncols ..]); the
+ * same as ws_agg_add_batch per batch with env.cols set to that batch's views. */
+int ws_agg_add_batches(ws_aggregator* agg, int ncols, int nb, const int64_t* bn, const uint32_t* const* bdel,
+                       const ws_col_view* bcols);
 int ws_agg_run(ws_aggregator* agg, const ws_expr_env* env, const ws_jit_program* jit);
 int ws_agg_run_window(ws_aggregator* agg, const ws_expr_env* env, const ws_jit_program* jit);
 int ws_agg_batches(const ws_aggregator* agg);

@@ -30,6 +30,12 @@ def lib() -> C.CDLL:
                                       C.POINTER(C.c_int64), P, P, C.POINTER(C.c_float)]
         l.wsref_select_multi.argtypes = [C.POINTER(abi.ExprEnv), C.c_int, abi.Prog, C.c_int, P, P, P, C.c_int,
                                          C.c_int64, C.POINTER(C.c_int64), P, P]
+        l.wsref_gather.argtypes = [P, C.c_int, P, C.c_int64, P, C.POINTER(C.c_float)]
+        l.wsref_hash_join_dev.argtypes = [abi.ColView, C.c_int64, abi.ColView, C.c_int64, C.POINTER(C.c_int64),
+                                          C.POINTER(P), C.POINTER(P), C.POINTER(C.c_float)]
+        l.wsref_free.argtypes = [P]
+        l.wsref_select_multi_dev.argtypes = [C.POINTER(abi.ExprEnv), C.c_int, abi.Prog, C.c_int, P, P, P, C.c_int,
+                                             C.POINTER(C.c_int64), C.POINTER(P), C.POINTER(C.c_float)]
         if l.wsref_init():
             raise RuntimeError(l.wsref_error().decode())
         _lib = l
@@ -94,3 +100,37 @@ def select_multi(env: abi.ExprEnv, where: abi.Prog | None, batches: list, ncols:
     _check(l.wsref_select_multi(C.byref(env), hw, w, nb, bn, bdel, arr, ncols, m.value, C.byref(m), idx.ctypes.data,
                                 per.ctypes.data))
     return idx[:m.value], per[:nb]
+
+
+def gather(src: int, ptype: int, idx: int, m: int, dst: int) -> float:
+    ms = C.c_float()
+    _check(lib().wsref_gather(src, ptype, idx, m, dst, C.byref(ms)))
+    return ms.value
+
+
+def hash_join_dev(bk: abi.ColView, nb: int, pk: abi.ColView, np_: int):
+    """(build idx ptr, probe idx ptr, m, ms); free the pointers with free()."""
+    m = C.c_int64()
+    ob, op = P(), P()
+    ms = C.c_float()
+    _check(lib().wsref_hash_join_dev(bk, nb, pk, np_, C.byref(m), C.byref(ob), C.byref(op), C.byref(ms)))
+    return ob.value, op.value, m.value, ms.value
+
+
+def select_multi_dev(env: abi.ExprEnv, where, batches: list, ncols: int):
+    nb = len(batches)
+    bn = (C.c_int64 * max(nb, 1))(*[b[0] for b in batches])
+    bdel = (P * max(nb, 1))(*[b[1] or None for b in batches])
+    cols = [v for b in batches for v in b[2]]
+    arr = (abi.ColView * max(len(cols), 1))(*cols)
+    m = C.c_int64()
+    idx = P()
+    ms = C.c_float()
+    _check(lib().wsref_select_multi_dev(C.byref(env), 1 if where is not None else 0, where or abi.Prog(0, 0), nb, bn,
+                                        bdel, arr, ncols, C.byref(m), C.byref(idx), C.byref(ms)))
+    return idx.value, m.value, ms.value
+
+
+def free(p: int):
+    if p:
+        lib().wsref_free(p)

@@ -123,4 +123,73 @@ int wsref_select_multi(const ExprEnv* envIn, int hasWhere, Prog where, int nb, c
   });
 }
 
+// dst[j] = src[idx[j]] (gpuGather), all device pointers; *ms: CUDA-event time.
+int wsref_gather(const void* src, int ptype, const int32_t* idx, int64_t m, void* dst, float* ms) {
+  return guard([&] {
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, cudaStreamPerThread);
+    gpuGather(src, (PType)ptype, idx, m, dst);
+    cudaEventRecord(e1, cudaStreamPerThread);
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  });
+}
+
+// Inner hash join leaving the pairs on the device (the engine's use): *ob / *op are cudaMallocAsync'd
+// on the per-thread stream (free with wsref_free).
+int wsref_hash_join_dev(ColView bk, int64_t nb, ColView pk, int64_t np, int64_t* m, int32_t** ob, int32_t** op, float* ms) {
+  return guard([&] {
+    DevVec<int32_t> b, p;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, cudaStreamPerThread);
+    *m = gpuHashJoin(bk, nb, pk, np, b, p);
+    cudaEventRecord(e1, cudaStreamPerThread);
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ob = b.p;
+    *op = p.p;
+    b.p = nullptr;
+    p.p = nullptr;
+  });
+}
+
+int wsref_free(void* p) {
+  return guard([&] { tmpFree(p); });
+}
+
+// Row selection leaving the indices on the device.
+int wsref_select_multi_dev(const ExprEnv* envIn, int hasWhere, Prog where, int nb, const int64_t* bn,
+                           const uint32_t* const* bdel, const ColView* bcols, int ncols, int64_t* m, int32_t** idx,
+                           float* ms) {
+  return guard([&] {
+    std::vector<int64_t> n(bn, bn + nb);
+    std::vector<const uint32_t*> d(nb, nullptr);
+    if (bdel)
+      for (int b = 0; b < nb; ++b) d[b] = bdel[b];
+    std::vector<ColView> cols(bcols, bcols + (size_t)nb * ncols);
+    DevVec<int32_t> out;
+    std::vector<int64_t> per;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, cudaStreamPerThread);
+    *m = gpuSelectMulti(*envIn, hasWhere != 0, where, n, d, cols, ncols, out, per, nullptr);
+    cudaEventRecord(e1, cudaStreamPerThread);
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *idx = out.p;
+    out.p = nullptr;
+  });
+}
+
 }  // extern "C"

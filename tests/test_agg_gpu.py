@@ -263,3 +263,17 @@ def test_expressions_and_functions():
             q.Agg("SUM", q.call2("ROUND2", q.col(1), q.ilit(2)), "DOUBLE")]
     aq = q.AggQuery(e, q.and_(q.col(1).ne(q.lit(0.25)), q.not_(q.isnull(q.col(2)))), [(yr, True), (case, True)], aggs)
     check(t, e, aq, cap=256)
+
+
+def test_add_batches_equals_add_batch():
+    t = W.pricing_summary(2_200_000, seed=9)
+    e, aq, ds = W.pricing_summary_query(t)
+    t.to_device()
+    one = gpu_aggregate(t, e, aq.plan, ds)
+    k1, a1, x1 = one.fetch()
+    agg = ops.GpuAggregator(aq.plan, 1024, ds)
+    agg.add_batches(e.ncols, t.batches(True))
+    agg.run(e.env, None)
+    k2, a2, x2 = agg.fetch()
+    o1, o2 = np.lexsort(k1.view(np.int64).T[::-1]), np.lexsort(k2.view(np.int64).T[::-1])
+    assert np.array_equal(x1[o1], x2[o2]) and np.array_equal(k1[o1].view(np.int64), k2[o2].view(np.int64))

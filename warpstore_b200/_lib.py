@@ -38,6 +38,7 @@ SIGNATURES = {
     "ws_agg_create": (C.c_int, [C.POINTER(abi.AggPlan), C.c_int64, C.POINTER(abi.DenseSpec), C.POINTER(P)]),
     "ws_agg_destroy": (None, [P]),
     "ws_agg_add_batch": (C.c_int, [P, C.POINTER(abi.ExprEnv), C.c_int, C.c_int64, P]),
+    "ws_agg_add_batches": (C.c_int, [P, C.c_int, C.c_int, P, P, P]),
     "ws_agg_run": (C.c_int, [P, C.POINTER(abi.ExprEnv), P]),
     "ws_agg_run_window": (C.c_int, [P, C.POINTER(abi.ExprEnv), P]),
     "ws_agg_batches": (C.c_int, [P]),

@@ -380,6 +380,10 @@ struct ws_aggregator {
   bool fetched = false;
   std::vector<int64_t> hi;
   int64_t lastGroups = -1;
+  // groups downloaded by the last fetch (reused until the next run)
+  int64_t cachedGroups = -1;
+  std::vector<double> cachedKeys;
+  std::vector<int64_t> cachedExact;
 
   u64* count() { return (u64*)ctl.p; }
   int* err() { return (int*)(ctl.p + 8); }
@@ -440,6 +444,7 @@ static void aggRun(ws_aggregator& A, const ws_expr_env& env, const ws_jit_progra
   if (nb == 0) return;
   A.fetched = false;
   A.lastGroups = -1;
+  A.cachedGroups = -1;
   const bool useJit = jit && jit->state.load() == 1 && planCovers(env, nb, A.ncols, A.bcols.data());
   if (!useJit && (A.plan.naggs > WS_INTERP_AGGS || A.plan.nkeys > WS_INTERP_KEYS))
     throw Error("this aggregation needs a compiled plan (more than 16 aggregates or 4 GROUP BY keys); codegen failed or is off", WS_ERR_PLAN);
@@ -623,6 +628,21 @@ int ws_agg_add_batch(ws_aggregator* A, const ws_expr_env* env, int ncols, int64_
   });
 }
 
+int ws_agg_add_batches(ws_aggregator* A, int ncols, int nb, const int64_t* bn, const uint32_t* const* bdel,
+                       const ws_col_view* bcols) {
+  return guardedCall([&] {
+    if (ncols < 0 || ncols > WS_MAX_COLS || nb < 0) throw Error("bad column or batch count", WS_ERR_ARG);
+    for (int b = 0; b < nb; ++b) {
+      if (bn[b] <= 0) continue;
+      if (!A->bn.empty() && ncols != A->ncols) throw Error("batches must have the same column count", WS_ERR_ARG);
+      A->ncols = ncols;
+      A->bn.push_back(bn[b]);
+      A->bdel.push_back(bdel ? bdel[b] : nullptr);
+      A->bcols.insert(A->bcols.end(), bcols + (int64_t)b * ncols, bcols + (int64_t)(b + 1) * ncols);
+    }
+  });
+}
+
 int ws_agg_run(ws_aggregator* A, const ws_expr_env* env, const ws_jit_program* jit) {
   return guardedCall([&] { aggRun(*A, *env, jit); });
 }
@@ -677,21 +697,26 @@ int ws_agg_group_count(ws_aggregator* A, int64_t* out) {
 
 int ws_agg_fetch(ws_aggregator* A, int64_t max_groups, double* keys, double* accs, int64_t* exact, int64_t* ngroups) {
   return guardedCall([&] {
-    checkFlags(*A, nullptr);
     const int nk = A->plan.nkeys, na = A->plan.naggs;
-    DBuf<int64_t> idx;
-    const int64_t g = nk ? aggCompactIdx(*A, idx) : 1;
+    if (A->cachedGroups < 0) {  // compact, emit and download once; a second call (the copy after a size query) reuses it
+      checkFlags(*A, nullptr);
+      DBuf<int64_t> idx;
+      const int64_t g = nk ? aggCompactIdx(*A, idx) : 1;
+      DBuf<double> dk(std::max<int64_t>(g * nk, 1));
+      DBuf<int64_t> dx(std::max<int64_t>(g * na * 2, 1));
+      if (g) WS_LAUNCH(kEmit, gridFor(g), 256, 0, A->rows.p, nk ? idx.p : nullptr, g, emitSpec(*A), dk.p, dx.p, 0);
+      A->cachedKeys.assign((size_t)(g * nk), 0.0);
+      A->cachedExact.assign((size_t)std::max<int64_t>(g * na * 2, 1), 0);
+      if (nk && g) WS_CK(cudaMemcpyAsync(A->cachedKeys.data(), dk.p, sizeof(double) * g * nk, cudaMemcpyDeviceToHost, stream()));
+      if (g) WS_CK(cudaMemcpyAsync(A->cachedExact.data(), dx.p, sizeof(int64_t) * g * na * 2, cudaMemcpyDeviceToHost, stream()));
+      sync();
+      A->cachedGroups = g;
+    }
+    const int64_t g = A->cachedGroups;
     *ngroups = g;
     if (g > max_groups) throw Error("output buffer too small for " + std::to_string(g) + " groups", WS_ERR_SIZE);
-    DBuf<double> dk(std::max<int64_t>(g * nk, 1));
-    DBuf<int64_t> dx(std::max<int64_t>(g * na * 2, 1));
-    if (g) WS_LAUNCH(kEmit, gridFor(g), 256, 0, A->rows.p, nk ? idx.p : nullptr, g, emitSpec(*A), dk.p, dx.p, 0);
-    std::vector<int64_t> ex((size_t)std::max<int64_t>(g * na * 2, 1));
-    if (nk && keys && g) {
-      WS_CK(cudaMemcpyAsync(keys, dk.p, sizeof(double) * g * nk, cudaMemcpyDeviceToHost, stream()));
-    }
-    if (g) WS_CK(cudaMemcpyAsync(ex.data(), dx.p, sizeof(int64_t) * g * na * 2, cudaMemcpyDeviceToHost, stream()));
-    sync();
+    const std::vector<int64_t>& ex = A->cachedExact;
+    if (nk && keys && g) memcpy(keys, A->cachedKeys.data(), sizeof(double) * g * nk);
     if (exact && g) memcpy(exact, ex.data(), sizeof(int64_t) * g * na * 2);
     const DblSpec s = dblSpec(*A);
     A->hi.assign(na, 0);

@@ -143,6 +143,14 @@ class GpuAggregator:
     def add_batch(self, env: abi.ExprEnv, ncols: int, n: int, deleted: int = 0):
         check(lib().ws_agg_add_batch(self.h, C.byref(env), ncols, int(n), deleted or None))
 
+    def add_batches(self, ncols: int, batches: list):
+        """All batches at once: [(n, deleted_ptr, [ColView per column])]."""
+        nb = len(batches)
+        bn = (C.c_int64 * max(nb, 1))(*[b[0] for b in batches])
+        bdel = (P * max(nb, 1))(*[b[1] or None for b in batches])
+        arr = _views_array([v for b in batches for v in b[2]])
+        check(lib().ws_agg_add_batches(self.h, ncols, nb, bn, bdel, arr))
+
     def run(self, env: abi.ExprEnv, jit: int | None = None):
         check(lib().ws_agg_run(self.h, C.byref(env), jit))
 

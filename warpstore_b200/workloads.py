@@ -184,3 +184,113 @@ def pricing_summary_query(table: Table, cutoff: int = 2467):
 # bytes each workload reads per row (the roofline's algorithmic bytes)
 PRICING_BYTES_PER_ROW = 4 + 8 * 4 + 1 + 1
 FILTER_GROUPBY_BYTES_PER_ROW = 4 + 8 + 8
+
+
+# ------------------------------------------------------------------ hash join + aggregate
+JOIN_BUILD_ROWS = 15_000_000
+JOIN_PROBE_ROWS = 60_000_000
+JOIN_GROUP_KEYS = 1 << 20
+# build: key 8 + order_date 4; probe: fk 8 + cents 8 + gkey 4
+JOIN_BUILD_BYTES_PER_ROW = 12
+JOIN_PROBE_BYTES_PER_ROW = 20
+
+
+def join_tables(nb: int = JOIN_BUILD_ROWS, np_: int = JOIN_PROBE_ROWS, seed: int = 3):
+    """orders (build): key int64 = a permutation of [0, nb), order_date int32 U[0, 2406);
+    lineitem (probe): fk int64 U[0, nb), cents int64 U[0, 1e6), gkey int32 U[0, 2^20)."""
+    rng = np.random.default_rng(seed)
+    build = Table(nb)
+    build.add("key", abi.T_I64, rng.permutation(nb).astype(np.int64))
+    build.add("order_date", abi.T_I32, rng.integers(0, 2406, nb, dtype=np.int32))
+    probe = Table(np_)
+    probe.add("fk", abi.T_I64, rng.integers(0, nb, np_, dtype=np.int64))
+    probe.add("cents", abi.T_I64, rng.integers(0, 1_000_000, np_, dtype=np.int64))
+    probe.add("gkey", abi.T_I32, rng.integers(0, JOIN_GROUP_KEYS, np_, dtype=np.int32))
+    return build, probe
+
+
+def contiguous_view(t: Table, c: int, device: bool) -> abi.ColView:
+    """One view over all rows of a raw column (its segments lie back to back)."""
+    col = t.cols[c]
+    w = col.data.dtype.itemsize
+    assert col.enc == 0 and all(col.offsets[s] == s * t.seg_rows * w for s in range(t.nseg))
+    return abi.ColView(col.dev.ptr if device else col.host.ctypes.data, col.t, 0, 0, 0)
+
+
+def join_aggregate_plans(cutoff: int = 1203):
+    """(build filter env + program, aggregation env + AggQuery + DenseSpec over the joined rows)."""
+    eb = q.Env()
+    eb.column(abi.T_I64)
+    eb.column(abi.T_I32)
+    where = eb.compile(q.col(1).lt(cutoff))
+    ej = q.Env()
+    gk = ej.column(abi.T_I32)
+    ct = ej.column(abi.T_I64)
+    aq = q.AggQuery(ej, None, [(q.col(gk), True)], [q.Agg("COUNT"), q.Agg("SUM", q.col(ct), "BIGINT", True)])
+    ds = q.dense_spec(aq.plan, [(0, JOIN_GROUP_KEYS - 1)], JOIN_PROBE_ROWS)
+    return eb, where, ej, aq, ds
+
+
+def join_aggregate_run(build: Table, probe: Table, plans, impl: str = "ours", timer=None):
+    """The engine's join pipeline on the device: select build rows (order_date < cutoff), gather their
+    keys, inner hash join with the probe keys, gather the probe's gkey and cents for the pairs, dense
+    GROUP BY gkey: COUNT, SUM(cents).  impl "ours" runs this library's operators, "reference" the
+    reference's (oracle/_ref, tests only).  timer(name) -> context manager timing a stage.
+    Returns (keys, accs in the engine format, pairs)."""
+    import contextlib
+
+    from . import ops
+    eb, where, ej, aq, ds = plans
+    timer = timer or (lambda name: contextlib.nullcontext())
+    build.to_device()
+    probe.to_device()
+    keyv = contiguous_view(build, 0, True)
+    fkv = contiguous_view(probe, 0, True)
+    if impl == "ours":
+        ops.jit_set_mode(abi.JIT_SYNC)
+        fp = abi.AggPlan()
+        fp.hasWhere, fp.where, fp.naggs = 1, where, 1
+        fp.ops[0] = abi.AGG_COUNT
+        fprog = ops.jit_get(eb.env, eb.ncols, fp, abi.JF_FLAGM, "join build filter")
+        aprog = ops.jit_get(ej.env, ej.ncols, aq.plan, abi.JF_DENSE, "join aggregate")
+        with timer("select"):
+            idx, mb, _ = ops.select_multi(eb.env, where, build.batches(True), eb.ncols, fprog)
+        bkeys = ops.DeviceBuffer(max(mb, 1) * 8)
+        with timer("gather build keys"):
+            ops.gather(keyv.p, abi.PT_I64, idx, mb, bkeys.ptr)
+        with timer("join"):
+            ob, op, m = ops.hash_join(abi.ColView(bkeys.ptr, abi.T_I64, 0, 0, 0), mb, fkv, probe.n)
+        gk, ct = ops.DeviceBuffer(max(m, 1) * 4), ops.DeviceBuffer(max(m, 1) * 8)
+        with timer("gather probe columns"):
+            ops.gather(probe.cols[2].dev.ptr, abi.PT_I32, op, m, gk.ptr)
+            ops.gather(probe.cols[1].dev.ptr, abi.PT_I64, op, m, ct.ptr)
+        with timer("aggregate"):
+            agg = ops.GpuAggregator(aq.plan, 1024, ds)
+            agg.add_batches(ej.ncols, [(m, 0, [abi.ColView(gk.ptr, abi.T_I32, 0, 0, 0),
+                                               abi.ColView(ct.ptr, abi.T_I64, 0, 0, 0)])])
+            agg.run(ej.env, aprog)
+            keys, accs, _ = agg.fetch(exact=False)
+        agg.close()
+        for p in (idx, ob, op):
+            ops.tmp_free(p)
+        ops.jit_set_mode(-1)
+        return keys, accs, m
+    from oracle import ref  # the reference's operators (test infrastructure)
+    with timer("select"):
+        idx, mb, _ = ref.select_multi_dev(eb.env, where, build.batches(True), eb.ncols)
+    bkeys = ops.DeviceBuffer(max(mb, 1) * 8)
+    with timer("gather build keys"):
+        ref.gather(keyv.p, abi.PT_I64, idx, mb, bkeys.ptr)
+    with timer("join"):
+        ob, op, m, _ = ref.hash_join_dev(abi.ColView(bkeys.ptr, abi.T_I64, 0, 0, 0), mb, fkv, probe.n)
+    gk, ct = ops.DeviceBuffer(max(m, 1) * 4), ops.DeviceBuffer(max(m, 1) * 8)
+    with timer("gather probe columns"):
+        ref.gather(probe.cols[2].dev.ptr, abi.PT_I32, op, m, gk.ptr)
+        ref.gather(probe.cols[1].dev.ptr, abi.PT_I64, op, m, ct.ptr)
+    with timer("aggregate"):
+        keys, accs, _, ovf, _ = ref.aggregate(ej.env, ej.ncols, aq.plan,
+                                              [(m, 0, [abi.ColView(gk.ptr, abi.T_I32, 0, 0, 0),
+                                                       abi.ColView(ct.ptr, abi.T_I64, 0, 0, 0)])], ds, 1024)
+    for p in (idx, ob, op):
+        ref.free(p)
+    return keys, accs, m
