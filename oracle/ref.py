@@ -24,8 +24,9 @@ def lib() -> C.CDLL:
         l = C.CDLL(LIB)
         l.wsref_error.restype = C.c_char_p
         l.wsref_aggregate.argtypes = [C.POINTER(abi.ExprEnv), C.c_int, C.POINTER(abi.AggPlan), C.POINTER(abi.DenseSpec),
-                                      C.c_int64, C.c_int, P, P, P, C.c_int64, C.POINTER(C.c_int64), P, P, P,
-                                      C.POINTER(C.c_int), C.POINTER(C.c_float)]
+                                      C.c_int64, C.c_int, P, P, P, C.POINTER(C.c_int64), C.POINTER(C.c_int),
+                                      C.POINTER(C.c_float)]
+        l.wsref_take.argtypes = [P, P, P]
         l.wsref_hash_join.argtypes = [abi.ColView, C.c_int64, abi.ColView, C.c_int64, C.c_int64,
                                       C.POINTER(C.c_int64), P, P, C.POINTER(C.c_float)]
         l.wsref_select_multi.argtypes = [C.POINTER(abi.ExprEnv), C.c_int, abi.Prog, C.c_int, P, P, P, C.c_int,
@@ -60,16 +61,15 @@ def aggregate(env: abi.ExprEnv, ncols: int, plan: abi.AggPlan, batches: list, de
     ovf = C.c_int()
     ms = C.c_float()
     dp = C.byref(dense) if dense is not None else None
-    _check(l.wsref_aggregate(C.byref(env), ncols, C.byref(plan), dp, cap, nb, bn, bdel, arr, 0, C.byref(g), None, None,
-                             None, C.byref(ovf), C.byref(ms)))
+    _check(l.wsref_aggregate(C.byref(env), ncols, C.byref(plan), dp, cap, nb, bn, bdel, arr, C.byref(g), C.byref(ovf),
+                             C.byref(ms)))
     if ovf.value:
         return None, None, None, True, ms.value
     n = g.value
     keys = np.zeros((n, plan.nkeys), dtype=np.float64)
     accs = np.zeros((n, plan.naggs), dtype=np.float64)
     hi = np.zeros(plan.naggs, dtype=np.int64)
-    _check(l.wsref_aggregate(C.byref(env), ncols, C.byref(plan), dp, cap, nb, bn, bdel, arr, n, C.byref(g),
-                             keys.ctypes.data, accs.ctypes.data, hi.ctypes.data, C.byref(ovf), C.byref(ms)))
+    _check(l.wsref_take(keys.ctypes.data, accs.ctypes.data, hi.ctypes.data))
     return keys, accs, hi, bool(ovf.value), ms.value
 
 

@@ -40,12 +40,16 @@ const char* wsref_error() { return gErr; }
 
 int wsref_init() { return guard([] { gpuInit(); }); }
 
-// GpuAggregator over batches (views bcols[b * ncols + c]); returns groups in the engine format.  With
-// maxg < groups only *ngroups is set.  *ms: CUDA-event time of run() + overflowed() on the default
-// per-thread stream.
+// Result of the last wsref_aggregate on this thread, copied out by wsref_take.
+static thread_local std::vector<double> gKeys, gAccs;
+static thread_local std::vector<int64_t> gHi;
+
+// GpuAggregator over batches (views bcols[b * ncols + c]): one aggregation, groups kept in the engine
+// format for wsref_take; *ngroups = their number.  *ms: CUDA-event time of run() + overflowed() on the
+// default per-thread stream.
 int wsref_aggregate(const ExprEnv* envIn, int ncols, const AggPlan* plan, const DenseSpec* dense, int64_t cap, int nb,
-                    const int64_t* bn, const uint32_t* const* bdel, const ColView* bcols, int64_t maxg, int64_t* ngroups,
-                    double* keys, double* accs, int64_t* sumHigh, int* overflow, float* ms) {
+                    const int64_t* bn, const uint32_t* const* bdel, const ColView* bcols, int64_t* ngroups,
+                    int* overflow, float* ms) {
   return guard([&] {
     std::vector<uint8_t> envBuf(sizeof(ExprEnv));
     ExprEnv* env = (ExprEnv*)envBuf.data();
@@ -66,20 +70,25 @@ int wsref_aggregate(const ExprEnv* envIn, int ncols, const AggPlan* plan, const 
     cudaEventElapsedTime(ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    gKeys.clear();
+    gAccs.clear();
+    gHi.assign(plan->naggs, 0);
     if (*overflow) {
       *ngroups = agg.groupCount();
       return;
     }
-    std::vector<double> k, a;
-    const int64_t g = agg.fetch(k, a);
-    *ngroups = g;
-    if (g <= maxg) {
-      if (!k.empty()) memcpy(keys, k.data(), k.size() * 8);
-      if (!a.empty()) memcpy(accs, a.data(), a.size() * 8);
-      const auto& hi = agg.sumHigh();
-      if (sumHigh)
-        for (int i = 0; i < plan->naggs; ++i) sumHigh[i] = i < (int)hi.size() ? hi[i] : 0;
-    }
+    *ngroups = agg.fetch(gKeys, gAccs);
+    const auto& hi = agg.sumHigh();
+    for (int i = 0; i < plan->naggs && i < (int)hi.size(); ++i) gHi[i] = hi[i];
+  });
+}
+
+// Copies the kept groups (keys [g][nkeys], accs [g][naggs], sum high words [naggs]).
+int wsref_take(double* keys, double* accs, int64_t* sumHigh) {
+  return guard([&] {
+    if (keys && !gKeys.empty()) memcpy(keys, gKeys.data(), gKeys.size() * 8);
+    if (accs && !gAccs.empty()) memcpy(accs, gAccs.data(), gAccs.size() * 8);
+    if (sumHigh && !gHi.empty()) memcpy(sumHigh, gHi.data(), gHi.size() * 8);
   });
 }
 

@@ -49,15 +49,15 @@ def test_join_aggregate_full_size_vs_reference():
     times = {}
 
     def timer_for(impl):
+        """Wall clock with the device synchronized on both sides: the stages mix kernels with host work
+        (result downloads into pageable memory), which CUDA events alone would not see."""
         @contextmanager
         def t(name):
             torch.cuda.synchronize()
-            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            s0.record()
+            t0 = time.perf_counter()
             yield
-            s1.record()
-            s1.synchronize()
-            times[(impl, name)] = s0.elapsed_time(s1)
+            torch.cuda.synchronize()
+            times[(impl, name)] = 1e3 * (time.perf_counter() - t0)
         return t
 
     res = {}

@@ -225,12 +225,15 @@ __device__ __host__ inline double slotDouble(const DblSpec& s, int a, long long 
   memcpy(&d, &w0, 8);
   return d;
 }
-__global__ void kExactToDouble(const int64_t* exact, int64_t m, DblSpec s, const int16_t* partnerKinds, double* accs) {
+// colMajor: accs[a * m + j] (compact) else accs[j * na + a] (fetch)
+__global__ void kExactToDouble(const int64_t* exact, int64_t m, DblSpec s, const int16_t* partnerKinds, double* accs,
+                               int colMajor) {
   for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < m; j += (int64_t)gridDim.x * blockDim.x)
     for (int a = 0; a < s.na; ++a) {
       const bool none = s.kind[a] == SK_NONE;
       const uint8_t sk = none ? (uint8_t)partnerKinds[a] : s.kind[a];
-      accs[a * m + j] = slotDouble(s, a, exact[(j * s.na + a) * 2], exact[(j * s.na + a) * 2 + 1], none, sk);
+      accs[colMajor ? a * m + j : j * s.na + a] =
+          slotDouble(s, a, exact[(j * s.na + a) * 2], exact[(j * s.na + a) * 2 + 1], none, sk);
     }
 }
 
@@ -380,10 +383,12 @@ struct ws_aggregator {
   bool fetched = false;
   std::vector<int64_t> hi;
   int64_t lastGroups = -1;
-  // groups downloaded by the last fetch (reused until the next run)
+  // groups compacted on the device by the last fetch (reused by the copy after a size query, until
+  // the next run): keys and engine-format doubles row-major, exact words [g][na][2]
   int64_t cachedGroups = -1;
-  std::vector<double> cachedKeys;
-  std::vector<int64_t> cachedExact;
+  DBuf<double> cachedKeys, cachedAccs;
+  DBuf<int64_t> cachedExact;
+  std::vector<int64_t> cachedHi;
 
   u64* count() { return (u64*)ctl.p; }
   int* err() { return (int*)(ctl.p + 8); }
@@ -698,41 +703,46 @@ int ws_agg_group_count(ws_aggregator* A, int64_t* out) {
 int ws_agg_fetch(ws_aggregator* A, int64_t max_groups, double* keys, double* accs, int64_t* exact, int64_t* ngroups) {
   return guardedCall([&] {
     const int nk = A->plan.nkeys, na = A->plan.naggs;
-    if (A->cachedGroups < 0) {  // compact, emit and download once; a second call (the copy after a size query) reuses it
+    if (A->cachedGroups < 0) {  // compact and convert on the device once; the copy after a size query reuses it
       checkFlags(*A, nullptr);
       DBuf<int64_t> idx;
       const int64_t g = nk ? aggCompactIdx(*A, idx) : 1;
-      DBuf<double> dk(std::max<int64_t>(g * nk, 1));
-      DBuf<int64_t> dx(std::max<int64_t>(g * na * 2, 1));
-      if (g) WS_LAUNCH(kEmit, gridFor(g), 256, 0, A->rows.p, nk ? idx.p : nullptr, g, emitSpec(*A), dk.p, dx.p, 0);
-      A->cachedKeys.assign((size_t)(g * nk), 0.0);
-      A->cachedExact.assign((size_t)std::max<int64_t>(g * na * 2, 1), 0);
-      if (nk && g) WS_CK(cudaMemcpyAsync(A->cachedKeys.data(), dk.p, sizeof(double) * g * nk, cudaMemcpyDeviceToHost, stream()));
-      if (g) WS_CK(cudaMemcpyAsync(A->cachedExact.data(), dx.p, sizeof(int64_t) * g * na * 2, cudaMemcpyDeviceToHost, stream()));
-      sync();
+      A->cachedKeys = DBuf<double>(std::max<int64_t>(g * nk, 1));
+      A->cachedExact = DBuf<int64_t>(std::max<int64_t>(g * na * 2, 1));
+      A->cachedAccs = DBuf<double>(std::max<int64_t>(g * na, 1));
+      if (g) {
+        WS_LAUNCH(kEmit, gridFor(g), 256, 0, A->rows.p, nk ? idx.p : nullptr, g, emitSpec(*A), A->cachedKeys.p,
+                  A->cachedExact.p, 0);
+        DBuf<int16_t> pk(WS_MAX_AGGS);
+        int16_t* st = (int16_t*)pinnedStage(2 * WS_MAX_AGGS);
+        for (int a = 0; a < WS_MAX_AGGS; ++a) st[a] = a < na ? A->lay.kind[A->lay.partner[a]] : 0;
+        h2dAsync(pk.p, st, 2 * WS_MAX_AGGS);
+        stageCopied();
+        WS_LAUNCH(kExactToDouble, gridFor(g), 256, 0, A->cachedExact.p, g, dblSpec(*A), pk.p, A->cachedAccs.p, 0);
+      }
+      A->cachedHi.assign(na, 0);
+      if (!nk) {  // high words of exact no-key integer sums (sumHigh)
+        std::vector<int64_t> ex(2 * na);
+        d2hSync(ex.data(), A->cachedExact.p, 16 * na);
+        for (int a = 0; a < na; ++a) {
+          const uint8_t k = A->lay.kind[a] == SK_NONE ? A->lay.kind[A->lay.partner[a]] : A->lay.kind[a];
+          A->cachedHi[a] = k == SK_ISUM ? ex[2 * a + 1] : 0;
+        }
+      } else {
+        sync();
+      }
       A->cachedGroups = g;
     }
     const int64_t g = A->cachedGroups;
     *ngroups = g;
     if (g > max_groups) throw Error("output buffer too small for " + std::to_string(g) + " groups", WS_ERR_SIZE);
-    const std::vector<int64_t>& ex = A->cachedExact;
-    if (nk && keys && g) memcpy(keys, A->cachedKeys.data(), sizeof(double) * g * nk);
-    if (exact && g) memcpy(exact, ex.data(), sizeof(int64_t) * g * na * 2);
-    const DblSpec s = dblSpec(*A);
-    A->hi.assign(na, 0);
-    if (accs)
-      for (int64_t j = 0; j < g; ++j)
-        for (int a = 0; a < na; ++a) {
-          const bool none = A->lay.kind[a] == SK_NONE;
-          const uint8_t sk = none ? A->lay.kind[A->lay.partner[a]] : A->lay.kind[a];
-          const long long w0 = ex[(j * na + a) * 2], w1 = ex[(j * na + a) * 2 + 1];
-          accs[j * na + a] = slotDouble(s, a, w0, w1, none, sk);
-        }
-    if (!nk)
-      for (int a = 0; a < na; ++a) {
-        const uint8_t k = A->lay.kind[a] == SK_NONE ? A->lay.kind[A->lay.partner[a]] : A->lay.kind[a];
-        A->hi[a] = k == SK_ISUM ? ex[a * 2 + 1] : 0;
-      }
+    if (g) {
+      if (nk && keys) WS_CK(cudaMemcpyAsync(keys, A->cachedKeys.p, sizeof(double) * g * nk, cudaMemcpyDeviceToHost, stream()));
+      if (accs) WS_CK(cudaMemcpyAsync(accs, A->cachedAccs.p, sizeof(double) * g * na, cudaMemcpyDeviceToHost, stream()));
+      if (exact) WS_CK(cudaMemcpyAsync(exact, A->cachedExact.p, sizeof(int64_t) * g * na * 2, cudaMemcpyDeviceToHost, stream()));
+      sync();
+    }
+    A->hi = A->cachedHi;
     A->fetched = true;
   });
 }
@@ -766,7 +776,7 @@ int ws_agg_compact(ws_aggregator* A, double** keys, double** accs, int64_t* ngro
       for (int a = 0; a < WS_MAX_AGGS; ++a) st[a] = a < na ? A->lay.kind[A->lay.partner[a]] : 0;
       h2dAsync(pk.p, st, 2 * WS_MAX_AGGS);
       stageCopied();
-      WS_LAUNCH(kExactToDouble, gridFor(g), 256, 0, dx.p, g, dblSpec(*A), pk.p, da.p);
+      WS_LAUNCH(kExactToDouble, gridFor(g), 256, 0, dx.p, g, dblSpec(*A), pk.p, da.p, 1);
     }
     *keys = dk.release();
     *accs = da.release();
