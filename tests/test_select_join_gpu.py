@@ -87,31 +87,33 @@ def test_select_with_deletes_and_gather():
         assert np.array_equal(got, t.cols[c].data[gi].astype(got.dtype))
 
 
-def join_case(nb, np_, key_space, seed, dup=False, nulls=False, i32=False):
+def join_case(nb, np_, key_space, seed, dup=False, nulls=False, i32=False, sparse=False, shift=0):
+    """Build / probe keys over [shift, shift + key_space); `sparse` spreads them over the whole integer
+    range with an odd multiplier (a bijection), so the join takes the hash path, not the dense one."""
     rng = np.random.default_rng(seed)
-    dt = np.int32 if i32 else np.int64
     if dup:
-        bk = rng.integers(0, key_space, nb).astype(dt)
+        bk = rng.integers(0, key_space, nb)
     else:
-        bk = rng.permutation(key_space)[:nb].astype(dt)
-    pk = rng.integers(0, key_space, np_).astype(dt)
+        bk = rng.permutation(key_space)[:nb]
+    pk = rng.integers(0, key_space, np_)
+    bk, pk = bk.astype(np.int64) + shift, pk.astype(np.int64) + shift
+    if sparse:
+        mul = np.uint64(0x9E3779B97F4A7C15)
+        bk, pk = (bk.astype(np.uint64) * mul).view(np.int64), (pk.astype(np.uint64) * mul).view(np.int64)
+    dt = np.int32 if i32 else np.int64
+    bk, pk = bk.astype(dt), pk.astype(dt)  # int32: keeps the low 32 bits (still a bijection of the keys)
+    null = abi.NULL_I32 if i32 else abi.NULL_I64
+    bk[bk == null] += 1
+    pk[pk == null] += 1
     if nulls:
-        null = abi.NULL_I32 if i32 else abi.NULL_I64
         bk[rng.random(nb) < 0.05] = null
         pk[rng.random(np_) < 0.05] = null
     return bk, pk
 
 
-@pytest.mark.parametrize("nb,np_,space,dup,nulls,i32", [
-    (1000, 5000, 1000, False, False, False),
-    (100_000, 1_000_000, 400_000, False, False, False),
-    (50_000, 200_000, 10_000, True, True, False),     # duplicate build keys: many matches per probe
-    (30_000, 100_000, 30_000, False, True, True),     # int32 keys with NULLs
-    (1, 1, 1, False, False, False),
-])
-def test_hash_join(nb, np_, space, dup, nulls, i32):
-    bk, pk = join_case(nb, np_, space, nb + np_, dup, nulls, i32)
+def check_join(bk, pk, i32):
     t = abi.T_I32N if i32 else abi.T_I64N
+    nb, np_ = len(bk), len(pk)
     db, dp = ops.DeviceBuffer.from_array(bk), ops.DeviceBuffer.from_array(pk)
     ob, op, m = ops.hash_join(abi.ColView(db.ptr, t, 0, 0, 0), nb, abi.ColView(dp.ptr, t, 0, 0, 0), np_)
     gb, gp = ops.device_to_array(ob, np.int32, m), ops.device_to_array(op, np.int32, m)
@@ -122,6 +124,48 @@ def test_hash_join(nb, np_, space, dup, nulls, i32):
     g = np.lexsort((gb, gp))
     w = np.lexsort((wb, wp))
     assert np.array_equal(gp[g], wp[w]) and np.array_equal(gb[g], wb[w])
+    return m
+
+
+@pytest.mark.parametrize("sparse", [False, True], ids=["dense-range", "hash"])
+@pytest.mark.parametrize("nb,np_,space,dup,nulls,i32,shift", [
+    (1000, 5000, 1000, False, False, False, 0),
+    (100_000, 1_000_000, 400_000, False, False, False, 0),
+    (50_000, 200_000, 10_000, True, True, False, 0),          # duplicate build keys: many matches per probe
+    (30_000, 100_000, 30_000, False, True, True, 0),          # int32 keys with NULLs
+    (40_000, 100_000, 60_000, True, False, False, -(1 << 40)),  # negative keys, duplicates
+    (1, 1, 1, False, False, False, 0),
+])
+def test_hash_join(nb, np_, space, dup, nulls, i32, shift, sparse):
+    bk, pk = join_case(nb, np_, space, nb + np_, dup, nulls, i32, sparse, shift)
+    check_join(bk, pk, i32)
+
+
+def test_hash_join_all_null_build_and_full_int64_range():
+    pk = np.arange(-5, 5, dtype=np.int64)
+    assert check_join(np.full(100, abi.NULL_I64, dtype=np.int64), pk, False) == 0
+    bk = np.array([np.iinfo(np.int64).min + 1, np.iinfo(np.int64).max, 0, 3], dtype=np.int64)  # range = all of int64
+    pk = np.array([3, np.iinfo(np.int64).max, 7, np.iinfo(np.int64).min + 1, 3], dtype=np.int64)
+    assert check_join(bk, pk, False) == 4
+
+
+def test_hash_join_multipass_matches_single_pass():
+    """A table budget far below the build side forces the hash join into many passes (each pass builds
+    the table of the build keys whose hash falls in it and probes every row); run in a child process
+    because the budget is read once per process."""
+    import subprocess
+    import sys
+    import os
+    code = (
+        "import numpy as np\n"
+        "from tests.test_select_join_gpu import join_case, check_join\n"
+        "bk, pk = join_case(100_000, 400_000, 300_000, 11, dup=True, nulls=True, sparse=True)\n"
+        "print(check_join(bk, pk, False))\n")
+    env = dict(os.environ, WARPSTORE_B200_JOIN_TABLE_BYTES=str(1 << 16))
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", code], env=env, cwd=root, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert int(r.stdout.strip().splitlines()[-1]) > 0
 
 
 def test_hash_join_partitions():
@@ -129,8 +173,12 @@ def test_hash_join_partitions():
     P = 4
     bks, pks = [], []
     for p in range(P):  # co-located: partition p's keys are == p mod P
-        bks.append((rng.permutation(20_000)[:5_000] * P + p).astype(np.int64))
-        pks.append((rng.integers(0, 20_000, 30_000) * P + p).astype(np.int64))
+        b = (rng.permutation(20_000)[:5_000] * P + p).astype(np.int64)
+        q = (rng.integers(0, 20_000, 30_000) * P + p).astype(np.int64)
+        if p % 2:  # odd partitions sparse (hash path), even ones dense
+            b, q = b * 0x3FFFFFFFFFF, q * 0x3FFFFFFFFFF
+        bks.append(b)
+        pks.append(q)
     bk, pk = np.concatenate(bks), np.concatenate(pks)
     boff = [0] + list(np.cumsum([len(x) for x in bks]))
     poff = [0] + list(np.cumsum([len(x) for x in pks]))

@@ -89,48 +89,110 @@ __global__ void kGather(const uint8_t* src, int esize, const int32_t* idx, int64
 }
 
 // ---------------------------------------------------------------- hash join
-// Table: cap (power of two) slots of {int64 key, int32 build row, pad} (16 bytes, one sector per
-// probe step); empty = INT64_MIN (the BIGINT NULL sentinel, never inserted).  Linear probing from
-// mix64(key).  Keys: I32 views widen to int64 (their sentinel is NULL), I64 views as stored, F64 views
-// (bit patterns converted by the engine) truncated, NaN = NULL (src/gpu.cu:180-202).
-constexpr long long kJEmpty = (long long)0x8000000000000000ull;
-struct JSlot {
-  long long key;
+// Table: cap (power of two) slots of {stored key, int32 build row, pad} (16 bytes, two slots per
+// 32-byte sector).  The stored key is key ^ 2^63, so an all-zero slot is empty: the one key that
+// maps to 0 is INT64_MIN, the BIGINT NULL sentinel, which is never inserted.  Linear probing from
+// h = mix64(key): slot h & (cap - 1).
+//
+// A build side whose table would not stay in L2 is split into P = 2^b passes by the top b bits of h:
+// pass p builds the table of the build keys with h >> (64 - b) == p (reusing one buffer) and probes
+// every probe row, skipping the rows of the other passes.  Each pass's random table accesses then hit
+// L2; the probe keys are re-read P times as a sequential stream (loaded with the evict-first hint so
+// that they do not push the table out).
+// Keys: I32 views widen to int64 (their sentinel is NULL), I64 views as stored, F64 views (bit
+// patterns converted by the engine) truncated, NaN = NULL (src/gpu.cu:180-202).
+constexpr u64 kJSign = 0x8000000000000000ull;
+struct __align__(16) JSlot {
+  u64 key;  // key ^ kJSign; 0 = empty
   int row;
   int pad;
 };
 
-__device__ __forceinline__ bool joinKey(const ws_col_view& c, int64_t r, long long& k) {
+__device__ __forceinline__ bool joinKeyStream(const ws_col_view& c, int64_t r, long long& k) {
   if (c.t == 0 || c.t == 3) {
-    const int v = __ldg((const int*)c.p + r);
+    const int v = __ldcs((const int*)c.p + r);
     k = v;
     return v != WS_NULL_I32;
   }
   if (c.t == 1 || c.t == 4) {
-    k = __ldg((const long long*)c.p + r);
+    k = __ldcs((const long long*)c.p + r);
     return k != WS_NULL_I64;
   }
-  const double d = __ldg((const double*)c.p + r);
+  const double d = __ldcs((const double*)c.p + r);
   k = (long long)d;
   return d == d;
 }
 
-__global__ void kJoinInit(JSlot* t, int64_t n) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    t[i].key = kJEmpty, t[i].row = -1;
+struct JPass {
+  int bits;  // log2 of the pass count
+  int pass;
+  __device__ __forceinline__ bool mine(u64 h) const { return bits == 0 || (int)(h >> (64 - bits)) == pass; }
+};
+
+// Build-key statistics of one build partition: st[0] = non-NULL keys, st[1] = min, st[2] = max (as
+// int64), st[3 + p] = keys of hash pass p (when bits > 0).  kJoinStatsInit sets the identities.
+constexpr int kJStatWords = 3 + 64;
+__global__ void kJoinStatsInit(unsigned long long* st) {
+  const int i = threadIdx.x;
+  if (i < kJStatWords) st[i] = i == 1 ? 0x7fffffffffffffffull : i == 2 ? 0x8000000000000000ull : 0ull;
 }
 
-// Inserts build rows [base, base + n); `bounded` probe steps at most (the table has >= 2n slots, so
-// an insert meets an empty slot within cap steps; err is raised otherwise).
-__global__ void kJoinBuild(ws_col_view key, int64_t base, int64_t n, JSlot* t, u64 mask, int* err) {
+__global__ void kJoinStats(ws_col_view key, int64_t base, int64_t n, int bits, unsigned long long* st) {
+  __shared__ unsigned long long h[64];
+  __shared__ unsigned long long cnt;
+  __shared__ long long mn, mx;
+  const int P = 1 << bits;
+  for (int i = threadIdx.x; i < P; i += blockDim.x) h[i] = 0;
+  if (threadIdx.x == 0) cnt = 0, mn = 0x7fffffffffffffffll, mx = (long long)0x8000000000000000ull;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  long long lmn = 0x7fffffffffffffffll, lmx = (long long)0x8000000000000000ull;
+  unsigned long long lc = 0;
+  for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x; i0 < n; i0 += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = i0 + threadIdx.x;
+    long long k = 0;
+    const bool ok = i < n && joinKeyStream(key, base + i, k);
+    if (ok) lmn = min(lmn, k), lmx = max(lmx, k), ++lc;
+    if (bits) {
+      const int part = ok ? (int)(mix64((u64)k) >> (64 - bits)) : -1;
+      const unsigned same = __match_any_sync(0xffffffffu, part);
+      if (part >= 0 && lane == __ffs(same) - 1) atomicAdd(&h[part], (unsigned long long)__popc(same));
+    }
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    lmn = min(lmn, __shfl_xor_sync(0xffffffffu, lmn, o));
+    lmx = max(lmx, __shfl_xor_sync(0xffffffffu, lmx, o));
+    lc += __shfl_xor_sync(0xffffffffu, lc, o);
+  }
+  if (lane == 0 && lc) {
+    atomicMin(&mn, lmn);
+    atomicMax(&mx, lmx);
+    atomicAdd(&cnt, lc);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && cnt) {
+    atomicAdd(&st[0], cnt);
+    atomicMin((long long*)&st[1], mn);
+    atomicMax((long long*)&st[2], mx);
+  }
+  for (int i = threadIdx.x; i < P && bits; i += blockDim.x)
+    if (h[i]) atomicAdd(&st[3 + i], h[i]);
+}
+
+// Inserts the pass's build rows of [base, base + n).  The table has >= 2x the pass's keys, so an
+// insert meets an empty slot within cap steps; err is raised otherwise.
+__global__ void kJoinBuild(ws_col_view key, int64_t base, int64_t n, JPass jp, JSlot* t, u64 mask, int* err) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     long long k;
-    if (!joinKey(key, base + i, k)) continue;
-    u64 s = mix64((u64)k) & mask;
+    if (!joinKeyStream(key, base + i, k)) continue;
+    const u64 h = mix64((u64)k);
+    if (!jp.mine(h)) continue;
+    const u64 sk = (u64)k ^ kJSign;
+    u64 s = h & mask;
     bool done = false;
     for (u64 p = 0; p <= mask; ++p) {
-      const long long prev = (long long)atomicCAS((u64*)&t[s].key, (u64)kJEmpty, (u64)k);
-      if (prev == kJEmpty) {
+      if (atomicCAS(&t[s].key, 0ull, sk) == 0ull) {
         t[s].row = (int)(base + i);
         done = true;
         break;
@@ -141,60 +203,191 @@ __global__ void kJoinBuild(ws_col_view key, int64_t base, int64_t n, JSlot* t, u
   }
 }
 
-// Probe rows [base, base + n): every match becomes a pair.  Lanes keep up to kKeep matches in
-// registers; a warp reserves its output with one atomic on the partition's counter (pairs of a warp
-// are contiguous).  With count != null (exact sizing pass) only the matches are counted.
-constexpr int kKeep = 4;
-__global__ void kJoinProbe(ws_col_view key, int64_t base, int64_t n, const JSlot* t, u64 mask, int64_t outBase,
-                           int64_t capacity, unsigned long long* counter, int32_t* ob, int32_t* op) {
-  const int lane = threadIdx.x & 31;
-  for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x; i0 < n; i0 += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t i = i0 + threadIdx.x;
-    int c = 0;
-    int keep[kKeep];
-    long long k = 0;
-    u64 s0 = 0;
-    bool valid = i < n && joinKey(key, base + i, k);
-    if (valid) {
-      s0 = mix64((u64)k) & mask;
-      u64 s = s0;
-      for (u64 p = 0; p <= mask; ++p) {
-        const JSlot e = t[s];
-        if (e.key == kJEmpty) break;
-        if (e.key == k) {
-          if (c < kKeep) keep[c] = e.row;
-          ++c;
-        }
-        s = (s + 1) & mask;
-      }
+// ---- output: pairs staged per warp in shared memory, flushed with one atomic on the partition's
+// counter per flush (coalesced writes).  Pairs at or past `capacity` are not written: the host
+// reruns with the exact count.
+constexpr int kJThreads = 256, kJPer = 4, kJStage = 256;
+constexpr int kJWarps = kJThreads / 32;
+
+struct JOut {
+  int32_t* ob;
+  int32_t* op;
+  int64_t outBase, capacity;
+  unsigned long long* counter;
+};
+
+// Writes the warp's staged pairs [0, fill) (all lanes of the warp call it).
+__device__ __forceinline__ void jFlush(const JOut& o, const int2* st, int fill, int lane) {
+  if (!fill) return;
+  unsigned long long base = 0;
+  if (lane == 0) base = atomicAdd(o.counter, (unsigned long long)fill);
+  base = __shfl_sync(0xffffffffu, base, 0);
+  for (int i = lane; i < fill; i += 32) {
+    const int64_t at = (int64_t)base + i;
+    if (at < o.capacity) {
+      const int2 pr = st[i];
+      __stcs(o.ob + o.outBase + at, pr.x);
+      __stcs(o.op + o.outBase + at, pr.y);
     }
-    // warp exclusive prefix of c, one reservation per warp
-    int incl = c;
+  }
+}
+
+// Stages one pair per lane that has one (all lanes of the warp call it; fill is warp-uniform).
+__device__ __forceinline__ void jStage(const JOut& o, int2* st, int& fill, bool has, int b, int p, int lane) {
+  const unsigned m = __ballot_sync(0xffffffffu, has);
+  if (!m) return;
+  const int cnt = __popc(m);
+  if (fill + cnt > kJStage) {
+    __syncwarp();
+    jFlush(o, st, fill, lane);
+    __syncwarp();
+    fill = 0;
+  }
+  if (has) st[fill + __popc(m & ((1u << lane) - 1u))] = make_int2(b, p);
+  fill += cnt;
+}
+
+// ---- dense join: build keys in a range of at most a few times their number index a table of
+// int32 build rows directly (table[key - kmin], -1 = none); duplicate keys chain through next[]
+// (next[row - rowBase] = the previously inserted row with that key).  One random 4-byte lookup per
+// probe row, into a table that is 4 bytes per key of the range.
+__global__ void kJoinDenseBuild(ws_col_view key, int64_t base, int64_t n, int* table, long long kmin, int* next,
+                                int* dup) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    long long k;
+    if (!joinKeyStream(key, base + i, k)) continue;
+    const int old = atomicExch(table + ((u64)k - (u64)kmin), (int)(base + i));
+    next[i] = old;
+    if (old >= 0) *dup = 1;
+  }
+}
+
+__global__ void __launch_bounds__(kJThreads) kJoinDenseProbe(ws_col_view key, int64_t base, int64_t n,
+                                                             const int* table, long long kmin, u64 range,
+                                                             const int* next, int64_t rowBase, const int* dupFlag,
+                                                             JOut out) {
+  __shared__ int2 stage[kJWarps][kJStage];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int2* st = stage[warp];
+  int fill = 0;
+  const bool dup = *dupFlag != 0;
+  const int64_t wstep = (int64_t)gridDim.x * kJWarps * 32 * kJPer;
+  for (int64_t w0 = ((int64_t)blockIdx.x * kJWarps + warp) * 32 * kJPer; w0 < n; w0 += wstep) {
+    u64 idx[kJPer];
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int v = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += v;
+    for (int j = 0; j < kJPer; ++j) {
+      const int64_t r = w0 + j * 32 + lane;
+      long long k = 0;
+      const bool ok = r < n && joinKeyStream(key, base + r, k);
+      idx[j] = ok ? (u64)k - (u64)kmin : range;
     }
-    const int total = __shfl_sync(0xffffffffu, incl, 31);
-    unsigned long long wbase = 0;
-    if (lane == 0 && total) wbase = atomicAdd(counter, (unsigned long long)total);
-    wbase = __shfl_sync(0xffffffffu, wbase, 0);
-    if (!ob || c == 0) continue;
-    int64_t o = (int64_t)wbase + incl - c;
-    if (o + c > capacity) continue;  // sized too small: the host reruns with the exact count
-    const int32_t pr = (int32_t)(base + i);
-    if (c <= kKeep) {
-      for (int j = 0; j < c; ++j) ob[outBase + o + j] = keep[j], op[outBase + o + j] = pr;
-    } else {
-      u64 s = s0;
-      for (u64 p = 0; p <= mask; ++p) {
-        const JSlot e = t[s];
-        if (e.key == kJEmpty) break;
-        if (e.key == k) ob[outBase + o] = e.row, op[outBase + o] = pr, ++o;
-        s = (s + 1) & mask;
+    int b[kJPer];
+#pragma unroll
+    for (int j = 0; j < kJPer; ++j) b[j] = idx[j] < range ? __ldg(table + idx[j]) : -1;
+#pragma unroll
+    for (int j = 0; j < kJPer; ++j) jStage(out, st, fill, b[j] >= 0, b[j], (int)(base + w0 + j * 32 + lane), lane);
+    if (dup) {
+      for (;;) {
+        bool any = false;
+#pragma unroll
+        for (int j = 0; j < kJPer; ++j) {
+          b[j] = b[j] >= 0 ? __ldg(next + (b[j] - rowBase)) : -1;
+          any |= b[j] >= 0;
+        }
+        if (!__any_sync(0xffffffffu, any)) break;
+#pragma unroll
+        for (int j = 0; j < kJPer; ++j) jStage(out, st, fill, b[j] >= 0, b[j], (int)(base + w0 + j * 32 + lane), lane);
       }
     }
   }
+  __syncwarp();
+  jFlush(out, st, fill, lane);
+}
+
+// ---- hash join probe: each warp takes kJPer x 32 consecutive probe rows per step (one coalesced
+// load per row slot).  A lane keeps its up-to-kJPer keys of this pass in a small queue and walks them
+// one after another, two slots (one 32-byte sector) per step, so that a warp runs as long as its
+// longest queue rather than the sum of its longest probe chains.  Matches are staged as they are
+// found.
+__global__ void __launch_bounds__(kJThreads) kJoinProbe(ws_col_view key, int64_t base, int64_t n, JPass jp,
+                                                        const JSlot* t, unsigned mask, JOut out) {
+  __shared__ int2 stage[kJWarps][kJStage];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int2* st = stage[warp];
+  int fill = 0;  // warp-uniform
+  const int64_t wstep = (int64_t)gridDim.x * kJWarps * 32 * kJPer;
+  for (int64_t w0 = ((int64_t)blockIdx.x * kJWarps + warp) * 32 * kJPer; w0 < n; w0 += wstep) {
+    // queue of this lane's keys in the pass (q0 is the one being walked)
+    u64 qk[kJPer];
+    unsigned qs[kJPer];
+    int qr[kJPer];
+    int nq = 0;
+#pragma unroll
+    for (int j = 0; j < kJPer; ++j) {
+      const int64_t r = w0 + j * 32 + lane;
+      long long k;
+      if (r < n && joinKeyStream(key, base + r, k)) {
+        const u64 h = mix64((u64)k);
+        if (jp.mine(h)) {
+#pragma unroll
+          for (int q = 0; q < kJPer; ++q)
+            if (q == nq) qk[q] = (u64)k ^ kJSign, qs[q] = (unsigned)(h & mask), qr[q] = (int)(base + r);
+          ++nq;
+        }
+      }
+    }
+    unsigned steps = 0;
+    while (__any_sync(0xffffffffu, nq > 0)) {
+      bool hitA = false, hitB = false, done = true;
+      int rowA = 0, rowB = 0, pr = 0;
+      if (nq > 0) {
+        const unsigned s0 = qs[0];
+        const unsigned even = s0 & ~1u;
+        const ulonglong2 a = __ldg((const ulonglong2*)(t + even));
+        const ulonglong2 b = __ldg((const ulonglong2*)(t + even + 1));
+        pr = qr[0];
+        done = false;
+        // slot `even` counts only when the walk starts there; slot even + 1 always
+        if (s0 == even) {
+          if (a.x == 0) done = true;
+          else if (a.x == qk[0]) hitA = true, rowA = (int)(unsigned)a.y;
+        }
+        if (!done) {
+          if (b.x == 0) done = true;
+          else if (b.x == qk[0]) hitB = true, rowB = (int)(unsigned)b.y;
+        }
+        ++steps;
+        if (!done && steps <= mask) {
+          qs[0] = (even + 2) & mask;
+        } else {
+#pragma unroll
+          for (int q = 0; q < kJPer - 1; ++q) qk[q] = qk[q + 1], qs[q] = qs[q + 1], qr[q] = qr[q + 1];
+          --nq;
+          steps = 0;
+        }
+      }
+      jStage(out, st, fill, hitA, rowA, pr, lane);
+      jStage(out, st, fill, hitB, rowB, pr, lane);
+    }
+  }
+  __syncwarp();
+  jFlush(out, st, fill, lane);
+}
+
+// Table budget per hash pass (bytes): the largest table that stays resident in L2 next to the streams.
+int64_t joinTableBudget() {
+  static const int64_t b = [] {
+    const char* e = getenv("WARPSTORE_B200_JOIN_TABLE_BYTES");
+    const long long v = e ? atoll(e) : 0;
+    return v > 0 ? (int64_t)v : (int64_t)1 << 40;
+  }();
+  return b;
+}
+
+int64_t pow2AtLeast(int64_t x) {
+  int64_t c = 2;
+  while (c < x) c <<= 1;
+  return c;
 }
 
 }  // namespace
@@ -384,21 +577,52 @@ int ws_hash_join_parts(ws_col_view build_key, const int64_t* boff, int nbparts, 
       *out_probe = (int32_t*)tmpAlloc(4);
       return;
     }
-    std::vector<int64_t> reg(pb + 1, 0), cap(pb);
+    // Hash passes per build partition (2^bits) from its row count and the table budget.
+    std::vector<int> bits(pb, 0);
     for (int q = 0; q < pb; ++q) {
-      int64_t c = 2;
-      while (c < (boff[q + 1] - boff[q]) * 2) c <<= 1;
-      cap[q] = c;
-      reg[q + 1] = reg[q] + c;
+      const int64_t nq = boff[q + 1] - boff[q];
+      while (bits[q] < 6 && pow2AtLeast(2 * ((nq >> bits[q]) + 1)) * (int64_t)sizeof(JSlot) > joinTableBudget()) ++bits[q];
     }
-    DBuf<JSlot> table(reg[pb]);
-    DBuf<int> err(1);
-    WS_CK(cudaMemsetAsync(err.p, 0, 4, stream()));
-    WS_LAUNCH(kJoinInit, gridFor(reg[pb]), 256, 0, table.p, reg[pb]);
+    // Build-key statistics (non-NULL count, min, max, keys per hash pass) of every partition.
+    DBuf<unsigned long long> stats((int64_t)pb * kJStatWords);
     for (int q = 0; q < pb; ++q) {
       const int64_t n = boff[q + 1] - boff[q];
-      if (n) WS_LAUNCH(kJoinBuild, gridFor(n), 256, 0, build_key, boff[q], n, table.p + reg[q], (u64)(cap[q] - 1), err.p);
+      WS_LAUNCH(kJoinStatsInit, 1, 128, 0, stats.p + (int64_t)q * kJStatWords);
+      if (n) WS_LAUNCH(kJoinStats, gridFor(n), 256, 0, build_key, boff[q], n, bits[q], stats.p + (int64_t)q * kJStatWords);
     }
+    std::vector<unsigned long long> hs((size_t)pb * kJStatWords);
+    WS_CK(cudaMemcpyAsync(hs.data(), stats.p, 8 * hs.size(), cudaMemcpyDeviceToHost, stream()));
+    sync();
+    // Per partition: dense (key range <= max(4 x keys, 2^16), below 2^31) or hash passes.
+    std::vector<char> dense(pb, 0);
+    std::vector<long long> kmin(pb, 0);
+    std::vector<u64> range(pb, 0);
+    std::vector<std::vector<int64_t>> cap(pb);
+    int64_t denseSlots = 1, nextRows = 1, tableSlots = 2;
+    for (int q = 0; q < pb; ++q) {
+      const unsigned long long* st = hs.data() + (size_t)q * kJStatWords;
+      const int64_t keys = (int64_t)st[0];
+      if (!keys) continue;
+      kmin[q] = (long long)st[1];
+      range[q] = (u64)(long long)st[2] - (u64)(long long)st[1] + 1;  // 0 when the keys span all of int64
+      if (range[q] && range[q] < ((u64)1 << 31) && range[q] <= std::max<u64>(4 * (u64)keys, 1 << 16)) {
+        dense[q] = 1;
+        denseSlots = std::max<int64_t>(denseSlots, (int64_t)range[q]);
+        nextRows = std::max<int64_t>(nextRows, boff[q + 1] - boff[q]);
+        continue;
+      }
+      for (int p = 0; p < (1 << bits[q]); ++p) {
+        const int64_t c = pow2AtLeast(2 * (bits[q] ? (int64_t)st[3 + p] : keys));
+        cap[q].push_back(c);
+        tableSlots = std::max(tableSlots, c);
+      }
+    }
+    bool anyDense = false, anyHash = false;
+    for (int q = 0; q < pb; ++q) anyDense |= dense[q] != 0, anyHash |= !cap[q].empty();
+    DBuf<JSlot> table(anyHash ? tableSlots : 1);
+    DBuf<int> dtable(anyDense ? denseSlots : 1), next(anyDense ? nextRows : 1);
+    DBuf<int> flags(2);  // [0] hash table full, [1] duplicate dense keys
+    WS_CK(cudaMemsetAsync(flags.p, 0, 8, stream()));
     // One probe pass with output capacity = probe rows per partition (enough for every join whose
     // build keys are unique); if a partition produced more, a second pass writes with exact sizes.
     std::vector<int64_t> capOut(pp), outStart(pp + 1, 0);
@@ -408,19 +632,41 @@ int ws_hash_join_parts(ws_col_view build_key, const int64_t* boff, int nbparts, 
     }
     DBuf<unsigned long long> counters(pp);
     std::vector<unsigned long long> cnt(pp);
-    for (int pass = 0; pass < 2; ++pass) {
+    for (int attempt = 0; attempt < 2; ++attempt) {
       WS_CK(cudaMemsetAsync(counters.p, 0, 8 * pp, stream()));
       DBuf<int32_t> ob(std::max<int64_t>(outStart[pp], 1)), op(std::max<int64_t>(outStart[pp], 1));
-      for (int p = 0; p < pp; ++p) {
-        const int q = pb == 1 ? 0 : p;
-        const int64_t n = poff[p + 1] - poff[p];
-        if (n)
-          WS_LAUNCH(kJoinProbe, gridFor(n), 256, 0, probe_key, poff[p], n, table.p + reg[q], (u64)(cap[q] - 1),
-                    outStart[p], capOut[p], counters.p + p, ob.p, op.p);
+      for (int q = 0; q < pb; ++q) {
+        const int64_t nbq = boff[q + 1] - boff[q];
+        const int npass = dense[q] ? 1 : (int)cap[q].size();  // 0: no non-NULL build key
+        for (int pass = 0; pass < npass; ++pass) {
+          const JPass jp{bits[q], pass};
+          const int64_t c = dense[q] ? 0 : cap[q][pass];
+          if (dense[q]) {
+            WS_CK(cudaMemsetAsync(dtable.p, 0xff, 4 * range[q], stream()));
+            WS_CK(cudaMemsetAsync(flags.p + 1, 0, 4, stream()));
+            WS_LAUNCH(kJoinDenseBuild, gridFor(nbq), 256, 0, build_key, boff[q], nbq, dtable.p, kmin[q], next.p,
+                      flags.p + 1);
+          } else {
+            WS_CK(cudaMemsetAsync(table.p, 0, sizeof(JSlot) * c, stream()));
+            WS_LAUNCH(kJoinBuild, gridFor(nbq), 256, 0, build_key, boff[q], nbq, jp, table.p, (u64)(c - 1), flags.p);
+          }
+          for (int p = 0; p < pp; ++p) {  // probe partitions joined with build partition q
+            if (pb != 1 && p != q) continue;
+            const int64_t n = poff[p + 1] - poff[p];
+            if (!n) continue;
+            const JOut jo{ob.p, op.p, outStart[p], capOut[p], counters.p + p};
+            const int grid = gridFor((n + kJPer - 1) / kJPer, kJThreads);
+            if (dense[q])
+              WS_LAUNCH(kJoinDenseProbe, grid, kJThreads, 0, probe_key, poff[p], n, dtable.p, kmin[q], range[q], next.p,
+                        boff[q], flags.p + 1, jo);
+            else
+              WS_LAUNCH(kJoinProbe, grid, kJThreads, 0, probe_key, poff[p], n, jp, table.p, (unsigned)(c - 1), jo);
+          }
+        }
       }
       int e = 0;
       WS_CK(cudaMemcpyAsync(cnt.data(), counters.p, 8 * pp, cudaMemcpyDeviceToHost, stream()));
-      WS_CK(cudaMemcpyAsync(&e, err.p, 4, cudaMemcpyDeviceToHost, stream()));
+      WS_CK(cudaMemcpyAsync(&e, flags.p, 4, cudaMemcpyDeviceToHost, stream()));
       sync();
       if (e) throw Error("internal: join hash table full", WS_ERR_INTERNAL);
       bool fits = true;
@@ -452,7 +698,7 @@ int ws_hash_join_parts(ws_col_view build_key, const int64_t* boff, int nbparts, 
         *m_out = m;
         return;
       }
-      for (int p = 0; p < pp; ++p) {  // exact sizes for the second pass
+      for (int p = 0; p < pp; ++p) {  // exact sizes for the second attempt
         capOut[p] = (int64_t)cnt[p];
         outStart[p + 1] = outStart[p] + capOut[p];
       }
