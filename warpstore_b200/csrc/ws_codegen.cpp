@@ -119,14 +119,14 @@ struct Gen {
       case WS_OP_CONST:
         if (n.isInt) {
           iconsts.insert(n.arg);
-          return {"ik" + arg, true};
+          return {"ik" + arg + "()", true};
         }
         dconsts.insert(n.arg);
-        return {"k" + arg, false};
+        return {"k" + arg + "()", false};
       case WS_OP_ADD: case WS_OP_SUB: case WS_OP_MUL: {
         const Sym a = kid(0), b = kid(1);
         if (n.isInt)
-          return {std::string(n.op == WS_OP_ADD ? "ws::iaddc(" : n.op == WS_OP_SUB ? "ws::isubc(" : "ws::imulc(") + a.e + "," + b.e + ",ovf)", true};
+          return {std::string(n.op == WS_OP_ADD ? "ws::iaddf(" : n.op == WS_OP_SUB ? "ws::isubf(" : "ws::imulf(") + a.e + "," + b.e + ",ofl)", true};
         const char* o = n.op == WS_OP_ADD ? "+" : n.op == WS_OP_SUB ? "-" : "*";
         return {"(" + D(a) + o + D(b) + ")", false};
       }
@@ -206,7 +206,7 @@ struct Gen {
 
 const char* valType(const ColUse& u) {
   if (u.t == 2) return "double";
-  if ((u.t == 0 || u.t == 3) && !u.enc) return "int";
+  if (u.t == 0 || u.t == 3) return "int";  // encoded int32 columns decode to int32 values too
   return "ws::i64";
 }
 
@@ -256,6 +256,13 @@ std::string genEvaluator(const ws_expr_env& env, int ncols, const ws_agg_plan& p
   o << "  static constexpr int NK = " << std::max(nk, 1) << ", NA = " << na << ", RW = " << (agg ? lay.rw : 1)
     << ", FRW = " << std::max(agg ? lay.frw : 1, 1) << ";\n";
   o << "  static constexpr bool STAGED = " << (staged.empty() ? "false" : "true") << ";\n";
+  // resident CTAs of the direct-load private-row kernel (a register budget of 85 per thread)
+  static const int privMinBlocks = [] {
+    const char* e = getenv("WARPSTORE_B200_PRIV_MIN_BLOCKS");
+    const int v = e ? atoi(e) : 0;
+    return v >= 1 && v <= 4 ? v : 2;
+  }();
+  o << "  static constexpr int PRIV_MIN_BLOCKS = " << privMinBlocks << ";\n";
   o << "  static constexpr int NSC = " << std::max<size_t>(staged.size(), 1) << ", STAGE_BYTES = " << stageBytes << ";\n";
   o << "  struct Stage { const unsigned char* d[NSC]; int w[NSC]; unsigned bytes; int ok; };\n";
   o << "  __device__ static void stageBind(const ws::Launch& l, int b, Stage& st) {\n";
@@ -269,18 +276,19 @@ std::string genEvaluator(const ws_expr_env& env, int ncols, const ws_agg_plan& p
     o << "    ws::bulkG2S(dst + " << soff[j] << ", st.d[" << j << "] + tr0 * st.w[" << j << "], ws::kTile * st.w[" << j
       << "], bar);\n";
   o << "  }\n";
-  o << "  const ws::Launch& L;\n  int* ovf;\n  bool fastOk;\n  ws::i64 rb;\n";
-  for (int k : g.iconsts) o << "  ws::i64 ik" << k << ";\n";
-  for (int k : g.dconsts) o << "  double k" << k << ";\n";
+  // ofl: overflow of this thread's checked integer arithmetic (rows that passed or were filtered),
+  // stored to the plan's flag once by finish()
+  o << "  const ws::Launch& L;\n  mutable unsigned ofl;\n  bool fastOk;\n  ws::i64 rb;\n";
+  // plan constants are read from the launch descriptor (constant bank) where used, not kept in registers
+  for (int k : g.iconsts)
+    o << "  __device__ __forceinline__ ws::i64 ik" << k << "() const { return __double_as_longlong(L.env.consts[" << k << "]); }\n";
+  for (int k : g.dconsts) o << "  __device__ __forceinline__ double k" << k << "() const { return L.env.consts[" << k << "]; }\n";
   for (size_t j = 0; j < g.temps.size(); ++j) o << "  " << (g.temps[j].second ? "ws::i64" : "double") << " t" << j << "[4];\n";
   for (auto& [c, u] : g.cols) {
     o << "  ws::ColRef v" << c << ";\n";
     if (!u.vec) o << "  " << valType(u) << " c" << c << "[4];\n";
   }
-  o << "  __device__ QEv(const ws::Launch& l) : L(l), ovf(l.env.ovf), fastOk(false), rb(0) {\n";
-  for (int k : g.iconsts) o << "    ik" << k << " = __double_as_longlong(l.env.consts[" << k << "]);\n";
-  for (int k : g.dconsts) o << "    k" << k << " = l.env.consts[" << k << "];\n";
-  o << "  }\n";
+  o << "  __device__ QEv(const ws::Launch& l) : L(l), ofl(0), fastOk(false), rb(0) {}\n";
   o << "  __device__ __forceinline__ int nk() const { return " << nk << "; }\n";
   o << "  __device__ __forceinline__ int na() const { return " << na << "; }\n";
   o << "  __device__ __forceinline__ int rowWords() const { return " << (agg ? lay.rw : 1) << "; }\n";
@@ -309,32 +317,36 @@ std::string genEvaluator(const ws_expr_env& env, int ncols, const ws_agg_plan& p
     if (!u.vec) fast += " && ws::aligned4(v" + std::to_string(c) + ")";
   }
   o << "    fastOk = " << fast << ";\n  }\n";
-  // loads of 4 consecutive rows
-  o << "  __device__ __forceinline__ void load(ws::i64 r0, bool fast, int nv) {\n    rb = r0;\n";
-  for (auto& [c, u] : g.cols) {
-    if (u.vec) continue;
-    const std::string C = std::to_string(c), v = "v" + C, a = "c" + C;
-    if (u.t == 2) {
-      if (u.enc)
-        o << "    if (" << v << ".enc) ws::load4encD(" << a << "," << v << ".d + r0 * " << v << ".width," << v << ".dict," << v
-          << ".enc," << v << ".base," << v << ".p10,fast,nv); else ";
-      o << "    ws::load4f64(" << a << ",(const double*)" << v << ".d + r0,fast,nv);\n";
-    } else if (u.t == 0 || u.t == 3) {
-      if (u.enc) {
-        o << "    if (" << v << ".enc) ws::load4enc(" << a << "," << v << ".d + r0 * " << v << ".width," << v << ".enc," << v
-          << ".base,(ws::i64)WS_NULL_I32,fast,nv); else { int t_[4]; ws::load4i32(t_,(const int*)" << v
-          << ".d + r0,fast,nv); for (int j = 0; j < 4; ++j) " << a << "[j] = t_[j]; }\n";
+  // loads of 4 consecutive rows: one branch between the all-vector form (whole aligned groups) and the
+  // element-wise form (ragged last group, unaligned views)
+  auto emitLoads = [&](const char* fast) {
+    for (auto& [c, u] : g.cols) {
+      if (u.vec) continue;
+      const std::string C = std::to_string(c), v = "v" + C, a = "c" + C, F = std::string(",") + fast + ",nv)";
+      if (u.t == 2) {
+        if (u.enc)
+          o << "      if (" << v << ".enc) ws::load4encD(" << a << "," << v << ".d + r0 * " << v << ".width," << v << ".dict," << v
+            << ".enc," << v << ".base," << v << ".p10" << F << "; else ";
+        o << "      ws::load4f64(" << a << ",(const double*)" << v << ".d + r0" << F << ";\n";
+      } else if (u.t == 0 || u.t == 3) {
+        if (u.enc)
+          o << "      if (" << v << ".enc) { ws::i64 t_[4]; ws::load4enc(t_," << v << ".d + r0 * " << v << ".width," << v
+            << ".enc," << v << ".base,(ws::i64)WS_NULL_I32" << F << "; for (int j = 0; j < 4; ++j) " << a
+            << "[j] = (int)t_[j]; } else ";
+        o << "      ws::load4i32(" << a << ",(const int*)" << v << ".d + r0" << F << ";\n";
       } else {
-        o << "    ws::load4i32(" << a << ",(const int*)" << v << ".d + r0,fast,nv);\n";
+        if (u.enc)
+          o << "      if (" << v << ".enc) ws::load4enc(" << a << "," << v << ".d + r0 * " << v << ".width," << v << ".enc," << v
+            << ".base,(ws::i64)WS_NULL_I64" << F << "; else ";
+        o << "      ws::load4i64(" << a << ",(const ws::i64*)" << v << ".d + r0" << F << ";\n";
       }
-    } else {
-      if (u.enc)
-        o << "    if (" << v << ".enc) ws::load4enc(" << a << "," << v << ".d + r0 * " << v << ".width," << v << ".enc," << v
-          << ".base,(ws::i64)WS_NULL_I64,fast,nv); else ";
-      o << "    ws::load4i64(" << a << ",(const ws::i64*)" << v << ".d + r0,fast,nv);\n";
     }
-  }
-  o << "  }\n";
+  };
+  o << "  __device__ __forceinline__ void load(ws::i64 r0, bool fast, int nv) {\n    rb = r0;\n    if (fast) {\n";
+  emitLoads("true");
+  o << "    } else {\n";
+  emitLoads("false");
+  o << "    }\n  }\n";
   // the same rows from a shared-memory stage (whole tile; rt = the thread's first row in it)
   o << "  __device__ __forceinline__ void loadStage(const unsigned char* st, int rt) {\n";
   for (size_t j = 0; j < staged.size(); ++j) {
@@ -347,8 +359,9 @@ std::string genEvaluator(const ws_expr_env& env, int ncols, const ws_agg_plan& p
       o << "    ws::stage4f64(" << a << "," << src << ");\n";
     } else if (u.t == 0 || u.t == 3) {
       if (u.enc)
-        o << "    if (" << v << ".enc) ws::stage4enc(" << a << "," << src << "," << v << ".enc," << v
-          << ".base,(ws::i64)WS_NULL_I32); else { int t_[4]; ws::stage4i32(t_," << src << "); for (int j = 0; j < 4; ++j) " << a << "[j] = t_[j]; }\n";
+        o << "    if (" << v << ".enc) { ws::i64 t_[4]; ws::stage4enc(t_," << src << "," << v << ".enc," << v
+          << ".base,(ws::i64)WS_NULL_I32); for (int j = 0; j < 4; ++j) " << a << "[j] = (int)t_[j]; } else ws::stage4i32(" << a
+          << "," << src << ");\n";
       else o << "    ws::stage4i32(" << a << "," << src << ");\n";
     } else {
       if (u.enc) o << "    if (" << v << ".enc) ws::stage4enc(" << a << "," << src << "," << v << ".enc," << v << ".base,(ws::i64)WS_NULL_I64); else ";
@@ -356,12 +369,14 @@ std::string genEvaluator(const ws_expr_env& env, int ncols, const ws_agg_plan& p
     }
   }
   o << "  }\n";
-  // per-row common subexpressions, computed for all 4 rows without branches (rows that did not pass
-  // the filter compute unused values and raise no overflow flag)
+  // per-row common subexpressions (rows that did not pass the filter compute unused values and
+  // raise no overflow flag)
   o << "  __device__ __forceinline__ void prep(int i, bool live) {\n";
-  if (!g.temps.empty()) o << "    int* ovf = live ? this->ovf : nullptr;\n";
+  if (!g.temps.empty()) o << "    unsigned ofl = 0;\n";
   for (size_t j = 0; j < g.temps.size(); ++j) o << "    t" << j << "[i] = " << g.temps[j].first << ";\n";
+  if (!g.temps.empty()) o << "    this->ofl |= live ? ofl : 0u;\n";
   o << "  }\n";
+  o << "  __device__ __forceinline__ void finish() const { if (ofl) *L.env.ovf = 1; }\n";
   o << "  __device__ __forceinline__ bool where(int i) const { return "
     << (where.isInt ? "(" + where.e + ") != 0" : "ws::truthy(" + where.e + ")") << "; }\n";
   o << "  __device__ __forceinline__ ws::i64 ikey(int k, int i) const { switch (k) {";
@@ -427,9 +442,21 @@ std::string nvrtcCubin(const std::string& src, const std::vector<std::string>& o
   const char* names[] = {"ws_types.h", "ws_dev.cuh", "ws_kern.cuh"};
   if (nvrtcCreateProgram(&prog, src.c_str(), "ws_query.cu", 3, hdrs, names) != NVRTC_SUCCESS)
     throw Error("codegen: nvrtcCreateProgram failed", WS_ERR_INTERNAL);
+  // WARPSTORE_B200_JIT_VERBOSE=1: print the compiler's resource report (registers, spills) per kernel
+  static const bool verbose = getenv("WARPSTORE_B200_JIT_VERBOSE") && atoi(getenv("WARPSTORE_B200_JIT_VERBOSE")) > 0;
   std::vector<const char*> opts;
   for (auto& o : optsIn) opts.push_back(o.c_str());
+  if (verbose) opts.push_back("--ptxas-options=-v");
   const nvrtcResult rc = nvrtcCompileProgram(prog, (int)opts.size(), opts.data());
+  if (verbose && rc == NVRTC_SUCCESS) {
+    size_t n = 0;
+    nvrtcGetProgramLogSize(prog, &n);
+    std::string log(n, '\0');
+    nvrtcGetProgramLog(prog, log.data());
+    int maj = 0, mnr = 0;
+    nvrtcVersion(&maj, &mnr);
+    fprintf(stderr, "[warpstore_b200 jit] NVRTC %d.%d\n%s\n", maj, mnr, log.c_str());
+  }
   if (rc != NVRTC_SUCCESS) {
     size_t n = 0;
     nvrtcGetProgramLogSize(prog, &n);
@@ -530,7 +557,8 @@ void compileProgram(ws_jit_program& p) {
   p.module = compileModule(body, &disk);
   p.fromDisk = disk;
   static const char* names[K_COUNT_] = {"wsq_nokeys", "wsq_dense_shared", "wsq_dense_global", "wsq_hash",
-                                        "wsq_select_count", "wsq_select_write", "wsq_dense_priv"};
+                                        "wsq_select_count", "wsq_select_write", "wsq_dense_priv",
+                                        "wsq_dense_priv_staged"};
   for (int k = 0; k < K_COUNT_; ++k) {
     CUfunction f = nullptr;
     if (drv().moduleGetFunction(&f, p.module, names[k]) == CUDA_SUCCESS) p.kernels.fn[k] = f;

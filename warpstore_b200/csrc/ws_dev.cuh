@@ -74,6 +74,24 @@ WS_DI i64 imulc(i64 a, i64 b, int* f) {
   if (__mul64hi(a, b) != (r >> 63) && f) *f = 1;
   return r;
 }
+// The same checked operations with the overflow accumulated into a register (bit 0 of `of`; no
+// branch and no store per operation): generated evaluators OR it into their flag once per thread.
+WS_DI i64 iaddf(i64 a, i64 b, unsigned& of) {
+  const i64 r = (i64)((u64)a + (u64)b);
+  of |= (unsigned)((u64)((a ^ r) & (b ^ r)) >> 63);
+  return r;
+}
+WS_DI i64 isubf(i64 a, i64 b, unsigned& of) {
+  const i64 r = (i64)((u64)a - (u64)b);
+  of |= (unsigned)((u64)((a ^ b) & (a ^ r)) >> 63);
+  return r;
+}
+WS_DI i64 imulf(i64 a, i64 b, unsigned& of) {
+  if (a == (i64)(int)a && b == (i64)(int)b) return (i64)(int)a * (i64)(int)b;  // 32 x 32 bits: exact
+  const i64 r = (i64)((u64)a * (u64)b);
+  of |= (unsigned)(__mul64hi(a, b) != (r >> 63));
+  return r;
+}
 
 WS_DI i64 insetI(const uint32_t* bits, int size, i64 c) {
   return (c >= 0 && c < size) ? (i64)((__ldg(bits + (c >> 5)) >> (c & 31)) & 1u) : 0ll;

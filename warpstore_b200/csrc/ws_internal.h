@@ -127,7 +127,12 @@ EnvK envK(const ws_expr_env& env);
 
 // ---------------------------------------------------------------- kernels
 // The scan kernels of one evaluator: the interpreter's (built into the library) or a compiled plan's.
-enum KernelId { K_NOKEYS = 0, K_DENSE_SHARED, K_DENSE_GLOBAL, K_HASH, K_SELECT_COUNT, K_SELECT_WRITE, K_DENSE_PRIV, K_COUNT_ };
+// K_DENSE_PRIV: direct loads, kThreads threads, bounded for several resident CTAs per SM;
+// K_DENSE_PRIV_STAGED: the same body with a producer warp staging tiles by TMA (kStagedThreads).
+enum KernelId {
+  K_NOKEYS = 0, K_DENSE_SHARED, K_DENSE_GLOBAL, K_HASH, K_SELECT_COUNT, K_SELECT_WRITE, K_DENSE_PRIV,
+  K_DENSE_PRIV_STAGED, K_COUNT_
+};
 struct KernelSet {
   CUfunction fn[K_COUNT_] = {};
   bool interp = true;

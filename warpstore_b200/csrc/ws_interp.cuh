@@ -166,6 +166,7 @@ static __device__ __noinline__ Word vmRun(const TInstr* code, int start, int len
 
 struct InterpEv {
   static constexpr int NK = WS_INTERP_KEYS, NA = WS_INTERP_AGGS, RW = 1 + 2 * WS_INTERP_AGGS, FRW = WS_INTERP_AGGS;
+  static constexpr int PRIV_MIN_BLOCKS = 1;  // the VM needs its registers
   static constexpr bool STAGED = false;
   static constexpr int STAGE_BYTES = 0;
   const Launch& L;
@@ -176,6 +177,7 @@ struct InterpEv {
   WS_DI void bind(const Launch&, int b) { cv = L.cols + (i64)b * L.ncols; }
   WS_DI void load(i64 r, bool, int) { r0 = r; }
   WS_DI void prep(int, bool) {}
+  WS_DI void finish() {}  // the VM raises overflow itself
   WS_DI int nk() const { return L.nkeys; }
   WS_DI int na() const { return L.naggs; }
   WS_DI int rowWords() const { return L.rowWords; }

@@ -8,6 +8,7 @@
 //   int nk(), na(), rowWords(), kind(a), woff(a); bool keyInt(k);
 //   void load(i64 r0, bool fast, int nv);   rows r0 .. r0+3 (nv valid) into registers
 //   bool where(i); i64 ikey(k, i); double dkey(k, i); bool ival(a, i, i64&); double dval(a, i)
+//   void prep(i, bool live); void finish()
 //
 // Work decomposition: a batch (segment / write buffer) is cut into tiles of kTile rows; a CTA of
 // kThreads threads takes one tile per iteration, each thread 4 consecutive rows (128-bit loads of
@@ -32,42 +33,52 @@ WS_DI u64 mix64(u64 x) {  // splitmix64 finalizer (Steele, Lea, Flood 2014)
   return x;
 }
 
-// The 4 loaded rows of a thread: filter each live row, evaluate the common subexpressions of all 4
-// rows together (independent chains the scheduler can interleave), then hand the passing rows to f.
+// The 4 loaded rows of a thread, one after another: filter the row, evaluate its common
+// subexpressions (prep), hand it to f when it passes.  Evaluating and consuming each row before the
+// next keeps one row's temporaries live at a time (fewer registers, more resident warps).
 template <class Ev, class F>
 WS_DI void rowGroup(Ev& ev, unsigned live, int b, i64 r0, F&& f) {
-  bool ok[4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i) ok[i] = ((live >> i) & 1u) && ev.where(i);
-#pragma unroll
-  for (int i = 0; i < 4; ++i) ev.prep(i, ok[i]);
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-    if (ok[i]) f(i, b, r0 + i);
+  for (int i = 0; i < 4; ++i) {
+    const bool ok = ((live >> i) & 1u) && ev.where(i);
+    ev.prep(i, ok);
+    if (ok) f(i, b, r0 + i);
+  }
 }
 
-// Visits every live row (not deleted, passing the filter) of the tiles this CTA owns.
+// First tile of batch b (tiles [t0, t1) of the launch) that this CTA owns: the CTA takes every
+// tile t with t = blockIdx.x (mod gridDim.x).
+WS_DI i64 firstOwnedTile(i64 t0) {
+  const i64 G = gridDim.x;
+  i64 r = ((i64)blockIdx.x - t0) % G;
+  if (r < 0) r += G;
+  return t0 + r;
+}
+
+// Visits every live row (not deleted, passing the filter) of the tiles this CTA owns, batch by batch
+// (the batch's size, bitmap and column views are read once per batch, not per tile).
 // f(i, batch, row) is called with i = the row's position (0..3) in the evaluator's 4-row group.
 template <class Ev, class F>
 WS_DI void forEachRow(const Launch& L, Ev& ev, F&& f) {
-  int b = 0, bound = -1;
-  for (i64 t = blockIdx.x; t < L.ntiles; t += gridDim.x) {
-    while (t >= __ldg(L.tileStart + b + 1)) ++b;
-    if (b != bound) {
-      ev.bind(L, b);
-      bound = b;
-    }
+  for (int b = 0; b < L.nb; ++b) {
+    const i64 t0 = __ldg(L.tileStart + b), t1 = __ldg(L.tileStart + b + 1);
+    i64 t = firstOwnedTile(t0);
+    if (t >= t1) continue;
+    ev.bind(L, b);
     const i64 n = __ldg(L.n + b);
-    const i64 r0 = (t - __ldg(L.tileStart + b)) * kTile + threadIdx.x * 4;
-    const i64 left = n - r0;
-    if (left <= 0) continue;
-    const int nv = left >= 4 ? 4 : (int)left;
-    ev.load(r0, ev.fastOk && nv == 4, nv);
-    unsigned live = (1u << nv) - 1;
     const uint32_t* del = L.del[b];
-    if (del) live &= ~(__ldg(del + (r0 >> 5)) >> (r0 & 31)) & 0xfu;
-    rowGroup(ev, live, b, r0, f);
+    for (; t < t1; t += gridDim.x) {
+      const i64 r0 = (t - t0) * kTile + threadIdx.x * 4;
+      const i64 left = n - r0;
+      if (left <= 0) continue;
+      const int nv = left >= 4 ? 4 : (int)left;
+      ev.load(r0, ev.fastOk && nv == 4, nv);
+      unsigned live = (1u << nv) - 1;
+      if (del) live &= ~(__ldg(del + (r0 >> 5)) >> (r0 & 31)) & 0xfu;
+      rowGroup(ev, live, b, r0, f);
+    }
   }
+  ev.finish();
 }
 
 // Same visit, with each tile's column chunks brought into shared memory by bulk asynchronous copies
@@ -158,6 +169,7 @@ WS_DI void forEachRowStaged(const Launch& L, Ev& ev, unsigned char* stages, int 
     __syncwarp();
     if (lane == 0) mbarArrive(smemAddr(&empty[s]));  // this warp is done with the stage
   }
+  ev.finish();
 }
 
 // Visits rows, staged through shared memory when the evaluator supports it and stages were given.
@@ -497,7 +509,7 @@ WS_DI bool denseIndex(const Launch& L, const Ev& ev, int i, i64& g) {
 // Dynamic shared memory: [stages (staged scans)][private rows G * FRW * blockDim][spill G * NA * 2].
 // Each (group, word) is then reduced over the CTA's threads in a fixed order; partial rows per CTA,
 // the last CTA reduces them.
-template <class Ev>
+template <class Ev, bool kStaged>
 __device__ void aggDensePriv(const Launch& L) {
   constexpr int RW = Ev::RW, FW = Ev::FRW, T = kThreads;
   extern __shared__ __align__(16) u64 wsSmem[];
@@ -517,7 +529,7 @@ __device__ void aggDensePriv(const Launch& L) {
     for (int j = tid; j < G * 2 * Ev::NA; j += blockDim.x) spill[j] = 0;
   }
   __syncthreads();
-  scanRows(L, ev, [&](int i, int, i64) {
+  auto row = [&](int i, int, i64) {
     i64 gi;
     if (!denseIndex(L, ev, i, gi)) {
       L.err[0] = 1;
@@ -525,8 +537,8 @@ __device__ void aggDensePriv(const Launch& L) {
     }
     u64 x[FW];
     fastOfInput(ev, i, x);
-    u64* sp = spill + gi * 2 * Ev::NA;
-    u64* p = priv + (size_t)gi * fw * T + tid;
+    u64* sp = spill + (unsigned)gi * (2u * Ev::NA);
+    u64* p = priv + ((unsigned)gi * (unsigned)fw * T + tid);
 #pragma unroll
     for (int a = 0; a < Ev::NA; ++a) {
       if (a >= ev.na()) break;
@@ -541,7 +553,10 @@ __device__ void aggDensePriv(const Launch& L) {
         default: break;
       }
     }
-  });
+  };
+  // the direct-load entry carries no staged path (its register budget allows more resident CTAs)
+  if constexpr (kStaged) scanRows(L, ev, row);
+  else forEachRow(L, ev, row);
   __syncthreads();
   const int rw = ev.rowWords();
   for (int g = 0; g < G; ++g) {
@@ -731,21 +746,20 @@ template <class Ev>
 __device__ void selectCount(const Launch& L) {
   __shared__ int wcount[kThreads / 32];
   Ev ev(L);
-  int b = 0, bound = -1;
-  for (i64 t = blockIdx.x; t < L.ntiles; t += gridDim.x) {
-    while (t >= __ldg(L.tileStart + b + 1)) ++b;
-    if (b != bound) {
-      ev.bind(L, b);
-      bound = b;
-    }
-    const i64 n = __ldg(L.n + b);
-    const i64 r0 = (t - __ldg(L.tileStart + b)) * kTile + threadIdx.x * 4;
+  for (int b = 0; b < L.nb; ++b) {
+  const i64 t0 = __ldg(L.tileStart + b), t1 = __ldg(L.tileStart + b + 1);
+  i64 t = firstOwnedTile(t0);
+  if (t >= t1) continue;
+  ev.bind(L, b);
+  const i64 n = __ldg(L.n + b);
+  const uint32_t* del = L.del[b];
+  for (; t < t1; t += gridDim.x) {
+    const i64 r0 = (t - t0) * kTile + threadIdx.x * 4;
     int c = 0;
     if (r0 < n) {
       const int nv = n - r0 >= 4 ? 4 : (int)(n - r0);
       ev.load(r0, ev.fastOk && nv == 4, nv);
       unsigned live = (1u << nv) - 1;
-      const uint32_t* del = L.del[b];
       if (del) live &= ~(__ldg(del + (r0 >> 5)) >> (r0 & 31)) & 0xfu;
 #pragma unroll
       for (int i = 0; i < 4; ++i) c += ((live >> i) & 1u) && ev.where(i);
@@ -761,6 +775,8 @@ __device__ void selectCount(const Launch& L) {
     }
     __syncthreads();
   }
+  }
+  ev.finish();
 }
 
 template <class Ev>
@@ -768,21 +784,20 @@ __device__ void selectWrite(const Launch& L) {
   __shared__ int woff[kThreads / 32];
   Ev ev(L);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int b = 0, bound = -1;
-  for (i64 t = blockIdx.x; t < L.ntiles; t += gridDim.x) {
-    while (t >= __ldg(L.tileStart + b + 1)) ++b;
-    if (b != bound) {
-      ev.bind(L, b);
-      bound = b;
-    }
-    const i64 n = __ldg(L.n + b);
-    const i64 r0 = (t - __ldg(L.tileStart + b)) * kTile + threadIdx.x * 4;
+  for (int b = 0; b < L.nb; ++b) {
+  const i64 t0 = __ldg(L.tileStart + b), t1 = __ldg(L.tileStart + b + 1);
+  i64 t = firstOwnedTile(t0);
+  if (t >= t1) continue;
+  ev.bind(L, b);
+  const i64 n = __ldg(L.n + b);
+  const uint32_t* del = L.del[b];
+  for (; t < t1; t += gridDim.x) {
+    const i64 r0 = (t - t0) * kTile + threadIdx.x * 4;
     unsigned sel = 0;
     if (r0 < n) {
       const int nv = n - r0 >= 4 ? 4 : (int)(n - r0);
       ev.load(r0, ev.fastOk && nv == 4, nv);
       unsigned live = (1u << nv) - 1;
-      const uint32_t* del = L.del[b];
       if (del) live &= ~(__ldg(del + (r0 >> 5)) >> (r0 & 31)) & 0xfu;
 #pragma unroll
       for (int i = 0; i < 4; ++i)
@@ -809,6 +824,8 @@ __device__ void selectWrite(const Launch& L) {
       if ((sel >> i) & 1u) L.outIdx[out0 + k++] = (int32_t)(g0 + i);
     __syncthreads();
   }
+  }
+  ev.finish();
 }
 
 }  // namespace ws
@@ -816,14 +833,19 @@ __device__ void selectWrite(const Launch& L) {
 // Kernel entry points (extern "C" names so generated modules can be looked up by name).  The Launch
 // descriptor is a __grid_constant__ parameter: the evaluator keeps a reference to it without forcing a
 // per-thread copy.
-#define WS_K_ENTRY(PREFIX, NAME, BODY)                                                                    \
-  extern "C" __global__ void __launch_bounds__(ws::kStagedThreads) PREFIX##_##NAME(const __grid_constant__ ws::Launch L) { \
-    BODY(L);                                                                                               \
+#define WS_K_ENTRY_B(PREFIX, NAME, BODY, THREADS, MINB)                                                      \
+  extern "C" __global__ void __launch_bounds__(THREADS, MINB) PREFIX##_##NAME(const __grid_constant__ ws::Launch L) { \
+    BODY(L);                                                                                                 \
   }
+#define WS_K_ENTRY(PREFIX, NAME, BODY) WS_K_ENTRY_B(PREFIX, NAME, BODY, ws::kStagedThreads, 1)
 #define WS_K_NOKEYS(EV, PREFIX) WS_K_ENTRY(PREFIX, nokeys, ws::aggNoKeys<EV>)
 #define WS_K_DENSE_SHARED(EV, PREFIX) WS_K_ENTRY(PREFIX, dense_shared, ws::aggDenseShared<EV>)
 #define WS_K_DENSE_GLOBAL(EV, PREFIX) WS_K_ENTRY(PREFIX, dense_global, ws::aggDenseGlobal<EV>)
-#define WS_K_DENSE_PRIV(EV, PREFIX) WS_K_ENTRY(PREFIX, dense_priv, ws::aggDensePriv<EV>)
+// The direct-load private-row kernel asks for EV::PRIV_MIN_BLOCKS resident CTAs of kThreads (a
+// register budget); the staged one keeps the producer warp.
+#define WS_K_DENSE_PRIV(EV, PREFIX)                                                                      \
+  WS_K_ENTRY_B(PREFIX, dense_priv, (ws::aggDensePriv<EV, false>), ws::kThreads, EV::PRIV_MIN_BLOCKS)     \
+  WS_K_ENTRY(PREFIX, dense_priv_staged, (ws::aggDensePriv<EV, true>))
 #define WS_K_HASH(EV, PREFIX) WS_K_ENTRY(PREFIX, hash, ws::aggHash<EV>)
 #define WS_K_SELECT_COUNT(EV, PREFIX) WS_K_ENTRY(PREFIX, select_count, ws::selectCount<EV>)
 #define WS_K_SELECT_WRITE(EV, PREFIX) WS_K_ENTRY(PREFIX, select_write, ws::selectWrite<EV>)

@@ -16,7 +16,7 @@ const KernelSet& interpKernels() {
     KernelSet k;
     const void* syms[K_COUNT_] = {(const void*)wsi_nokeys, (const void*)wsi_dense_shared, (const void*)wsi_dense_global,
                                   (const void*)wsi_hash, (const void*)wsi_select_count, (const void*)wsi_select_write,
-                                  (const void*)wsi_dense_priv};
+                                  (const void*)wsi_dense_priv, (const void*)wsi_dense_priv_staged};
     for (int i = 0; i < K_COUNT_; ++i) {
       cudaFunction_t f;
       WS_CK(cudaGetFuncBySymbol(&f, syms[i]));
@@ -496,12 +496,14 @@ static void aggRun(ws_aggregator& A, const ws_expr_env& env, const ws_jit_progra
     L.G = A.dense.G;
     const int64_t G = A.dense.G;
     // few groups: private register rows per thread in shared memory (+ staged tiles when they fit)
-    const size_t privBytes = (size_t)G * A.lay.frw * kThreads * 8 + (size_t)G * WS_MAX_AGGS * 16;
+    // private rows [G][frw][kThreads] + int128 spill counters [G][NA][2] (NA: the evaluator's slot bound)
+    const int naEv = ks.interp ? WS_INTERP_AGGS : A.plan.naggs;
+    const size_t privBytes = (size_t)G * A.lay.frw * kThreads * 8 + (size_t)G * naEv * 16;
     if (G * A.lay.frw <= 48 && ks.fn[K_DENSE_PRIV]) {
-      CUfunction f = ks.fn[K_DENSE_PRIV];
       const size_t budget = 220 * 1024;
       int S2 = stageBytes > 0 ? (int)std::min<int64_t>(maxStages, (int64_t)(budget - privBytes) / stageBytes) : 0;
-      if (S2 < 2) S2 = 0;
+      if (S2 < 2 || !ks.fn[K_DENSE_PRIV_STAGED]) S2 = 0;
+      CUfunction f = S2 ? ks.fn[K_DENSE_PRIV_STAGED] : ks.fn[K_DENSE_PRIV];
       L.stages = S2;
       const int threads = S2 ? kStagedThreads : kThreads;
       const size_t smem = (size_t)S2 * stageBytes + privBytes;
