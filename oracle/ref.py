@@ -27,6 +27,10 @@ def lib() -> C.CDLL:
                                       C.c_int64, C.c_int, P, P, P, C.POINTER(C.c_int64), C.POINTER(C.c_int),
                                       C.POINTER(C.c_float)]
         l.wsref_take.argtypes = [P, P, P]
+        l.wsref_aggregate_compact.argtypes = [C.POINTER(abi.ExprEnv), C.c_int, C.POINTER(abi.AggPlan),
+                                              C.POINTER(abi.DenseSpec), C.c_int64, C.c_int, P, P, P,
+                                              C.POINTER(C.c_int64), C.POINTER(C.c_int), C.POINTER(P), C.POINTER(P),
+                                              C.POINTER(C.c_float)]
         l.wsref_hash_join.argtypes = [abi.ColView, C.c_int64, abi.ColView, C.c_int64, C.c_int64,
                                       C.POINTER(C.c_int64), P, P, C.POINTER(C.c_float)]
         l.wsref_select_multi.argtypes = [C.POINTER(abi.ExprEnv), C.c_int, abi.Prog, C.c_int, P, P, P, C.c_int,
@@ -50,7 +54,7 @@ def _check(rc):
 
 def aggregate(env: abi.ExprEnv, ncols: int, plan: abi.AggPlan, batches: list, dense=None, cap: int = 1024):
     """Reference GpuAggregator over device batches [(n, del_ptr, views)]: (keys [g, nk], accs [g, na],
-    sum_high [na], overflowed, milliseconds of run())."""
+    sum_high [na], overflowed, milliseconds of run()); when overflowed, (None, None, group count, True, ms)."""
     l = lib()
     nb = len(batches)
     bn = (C.c_int64 * max(nb, 1))(*[b[0] for b in batches])
@@ -63,14 +67,31 @@ def aggregate(env: abi.ExprEnv, ncols: int, plan: abi.AggPlan, batches: list, de
     dp = C.byref(dense) if dense is not None else None
     _check(l.wsref_aggregate(C.byref(env), ncols, C.byref(plan), dp, cap, nb, bn, bdel, arr, C.byref(g), C.byref(ovf),
                              C.byref(ms)))
-    if ovf.value:
-        return None, None, None, True, ms.value
+    if ovf.value:  # overflowed: the third element is the group count seen
+        return None, None, g.value, True, ms.value
     n = g.value
     keys = np.zeros((n, plan.nkeys), dtype=np.float64)
     accs = np.zeros((n, plan.naggs), dtype=np.float64)
     hi = np.zeros(plan.naggs, dtype=np.int64)
     _check(l.wsref_take(keys.ctypes.data, accs.ctypes.data, hi.ctypes.data))
     return keys, accs, hi, bool(ovf.value), ms.value
+
+
+def aggregate_compact(env: abi.ExprEnv, ncols: int, plan: abi.AggPlan, batches: list, dense=None, cap: int = 1024):
+    """Reference GpuAggregator leaving the groups on the device: (keys_ptr, accs_ptr, g, overflowed, ms);
+    free the pointers with free()."""
+    l = lib()
+    nb = len(batches)
+    bn = (C.c_int64 * max(nb, 1))(*[b[0] for b in batches])
+    bdel = (P * max(nb, 1))(*[b[1] or None for b in batches])
+    cols = [v for b in batches for v in b[2]]
+    arr = (abi.ColView * max(len(cols), 1))(*cols)
+    g, ovf, ms = C.c_int64(), C.c_int(), C.c_float()
+    k, a = P(), P()
+    dp = C.byref(dense) if dense is not None else None
+    _check(l.wsref_aggregate_compact(C.byref(env), ncols, C.byref(plan), dp, cap, nb, bn, bdel, arr, C.byref(g),
+                                     C.byref(ovf), C.byref(k), C.byref(a), C.byref(ms)))
+    return k.value, a.value, g.value, bool(ovf.value), ms.value
 
 
 def hash_join(bk: abi.ColView, nb: int, pk: abi.ColView, np_: int):

@@ -83,6 +83,45 @@ int wsref_aggregate(const ExprEnv* envIn, int ncols, const AggPlan* plan, const 
   });
 }
 
+// GpuAggregator over batches leaving the groups on the device, column-major (GpuAggregator::compact);
+// *keys / *accs are freed with wsref_free.  With *overflow set nothing is compacted.
+int wsref_aggregate_compact(const ExprEnv* envIn, int ncols, const AggPlan* plan, const DenseSpec* dense, int64_t cap,
+                            int nb, const int64_t* bn, const uint32_t* const* bdel, const ColView* bcols,
+                            int64_t* ngroups, int* overflow, double** keys, double** accs, float* ms) {
+  return guard([&] {
+    std::vector<uint8_t> envBuf(sizeof(ExprEnv));
+    ExprEnv* env = (ExprEnv*)envBuf.data();
+    memcpy(env, envIn, sizeof(ExprEnv));
+    GpuAggregator agg(*plan, cap, dense);
+    for (int b = 0; b < nb; ++b) {
+      for (int c = 0; c < ncols; ++c) env->cols[c] = bcols[(int64_t)b * ncols + c];
+      agg.addBatch(*env, ncols, bn[b], bdel ? bdel[b] : nullptr);
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, cudaStreamPerThread);
+    agg.run(*env, nullptr);
+    cudaEventRecord(e1, cudaStreamPerThread);
+    *overflow = agg.overflowed() ? 1 : 0;
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *keys = *accs = nullptr;
+    if (*overflow) {
+      *ngroups = agg.groupCount();
+      return;
+    }
+    DevVec<double> k, a;
+    *ngroups = agg.compact(k, a);
+    *keys = k.p;
+    *accs = a.p;
+    k.p = nullptr;
+    a.p = nullptr;
+  });
+}
+
 // Copies the kept groups (keys [g][nkeys], accs [g][naggs], sum high words [naggs]).
 int wsref_take(double* keys, double* accs, int64_t* sumHigh) {
   return guard([&] {

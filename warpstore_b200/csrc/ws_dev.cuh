@@ -582,6 +582,7 @@ struct Launch {
   u64 mask;                   // cap - 1
   u64* count;                 // occupied rows
   int smemSlots;              // per-CTA shared table slots (power of 2)
+  int spillRows;              // per-CTA shared buffer of rows bound for the global table (hash GROUP BY)
   int probeLimit;             // global probe limit before reporting overflow
   // selection
   i64* tileCount;             // [ntiles] selected rows per tile (count pass) / exclusive offsets (write pass)

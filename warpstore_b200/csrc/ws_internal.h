@@ -54,6 +54,8 @@ void* tmpAlloc(size_t bytes);    // stream-ordered pool allocation on stream()
 void tmpFree(void* p);
 void h2dAsync(void* d, const void* h, size_t b);
 void d2hSync(void* h, const void* d, size_t b);
+// The same for large copies into pageable memory: pipelined through pinned staging (synchronous).
+void d2hLarge(void* h, const void* d, size_t b);
 void sync();
 void countLaunch(int n = 1);     // kernels launched by this library (ws_kernel_launches)
 void setStream(cudaStream_t s);

@@ -58,6 +58,36 @@ WS_DI i64 firstOwnedTile(i64 t0) {
 // Visits every live row (not deleted, passing the filter) of the tiles this CTA owns, batch by batch
 // (the batch's size, bitmap and column views are read once per batch, not per tile).
 // f(i, batch, row) is called with i = the row's position (0..3) in the evaluator's 4-row group.
+// tileEnd() is called by every thread of the CTA after each of the CTA's tiles (a CTA-uniform point);
+// it returns the same value in every thread, true to end the visit there.
+template <class Ev, class F, class E>
+WS_DI void forEachRowTiles(const Launch& L, Ev& ev, F&& f, E&& tileEnd) {
+  for (int b = 0; b < L.nb; ++b) {
+    const i64 t0 = __ldg(L.tileStart + b), t1 = __ldg(L.tileStart + b + 1);
+    i64 t = firstOwnedTile(t0);
+    if (t >= t1) continue;
+    ev.bind(L, b);
+    const i64 n = __ldg(L.n + b);
+    const uint32_t* del = L.del[b];
+    for (; t < t1; t += gridDim.x) {
+      const i64 r0 = (t - t0) * kTile + threadIdx.x * 4;
+      const i64 left = n - r0;
+      if (left > 0) {
+        const int nv = left >= 4 ? 4 : (int)left;
+        ev.load(r0, ev.fastOk && nv == 4, nv);
+        unsigned live = (1u << nv) - 1;
+        if (del) live &= ~(__ldg(del + (r0 >> 5)) >> (r0 & 31)) & 0xfu;
+        rowGroup(ev, live, b, r0, f);
+      }
+      if (tileEnd()) {
+        ev.finish();
+        return;
+      }
+    }
+  }
+  ev.finish();
+}
+
 template <class Ev, class F>
 WS_DI void forEachRow(const Launch& L, Ev& ev, F&& f) {
   for (int b = 0; b < L.nb; ++b) {
@@ -683,22 +713,33 @@ WS_DI void globalInsert(const Launch& L, const Ev& ev, u64 kw, const double* kv,
 }
 
 // Rows are pre-aggregated in a per-CTA shared-memory table (smemSlots rows, bounded probing), which
-// absorbs hot keys; a row that finds no slot goes to the global table directly.  The shared table is
-// merged into the global table when the CTA finishes.
+// absorbs hot keys.  A row that finds no slot there is appended to a per-CTA shared buffer (one
+// shared atomic per warp); after each tile the whole CTA inserts the buffered rows into the global
+// table together, one row per thread, so the global probes and atomics of the cold keys run with all
+// lanes active instead of a few diverged lanes at a time.  (A row finding the buffer full goes to
+// the global table directly.)  The shared table is merged into the global table when the CTA finishes.
+// Shared memory: [S][rw] table | [S][nk] key values (multi-key) | [B][rw] buffer | [B][nk] key values.
 template <class Ev>
 __device__ void aggHash(const Launch& L) {
   extern __shared__ __align__(16) u64 wsSmem[];
+  __shared__ int spillN, stopFlag;
   Ev ev(L);
-  const int rw = ev.rowWords();
-  const int S = L.smemSlots;
+  const int rw = ev.rowWords(), nk = ev.nk();
+  const int S = L.smemSlots, B = L.spillRows;
+  const bool multi = nk > 1;
+  u64* tab = wsSmem;
+  double* skv = (double*)(tab + (size_t)S * rw);
+  u64* buf = tab + (size_t)S * rw + (multi ? (size_t)S * nk : 0);
+  double* bkv = (double*)(buf + (size_t)B * rw);
   for (int s = threadIdx.x; s < S; s += blockDim.x) {
-    u64* row = wsSmem + (size_t)s * rw;
+    u64* row = tab + (size_t)s * rw;
     rowIdentity(ev, row);
     row[0] = kEmpty;
   }
-  double* skv = (double*)(wsSmem + (size_t)S * rw);  // [S][nk] key values of multi-key groups
+  if (threadIdx.x == 0) spillN = 0;
   __syncthreads();
-  forEachRow(L, ev, [&](int i, int, i64) {
+  const int lane = threadIdx.x & 31;
+  auto rowFn = [&](int i, int, i64) {
     double kv[Ev::NK];
     const u64 kw = keyWord(ev, i, kv);
     u64 x[kMaxRowWords];
@@ -707,13 +748,13 @@ __device__ void aggHash(const Launch& L) {
       unsigned s = (unsigned)(mix64(kw) & (u64)(S - 1));
 #pragma unroll 1
       for (int p = 0; p < 8; ++p) {
-        u64* row = wsSmem + (size_t)s * rw;
+        u64* row = tab + (size_t)s * rw;
         u64 prev = row[0];
         if (prev == kEmpty) {
           prev = atomicCAS(row, kEmpty, kw);
           if (prev == kEmpty) {
-            if (ev.nk() > 1)
-              for (int k = 0; k < ev.nk(); ++k) skv[(size_t)s * ev.nk() + k] = kv[k];
+            if (multi)
+              for (int k = 0; k < nk; ++k) skv[(size_t)s * nk + k] = kv[k];
             prev = kw;
           }
         }
@@ -724,15 +765,57 @@ __device__ void aggHash(const Launch& L) {
         s = (s + 1) & (S - 1);
       }
     }
-    globalInsert(L, ev, kw, kv, x);
-  });
+    // bound for the global table: reserve a buffer entry (one shared atomic per warp)
+    const unsigned m = __activemask();
+    const int leader = __ffs(m) - 1, rank = __popc(m & ((1u << lane) - 1));
+    int base = 0;
+    if (lane == leader) base = atomicAdd(&spillN, __popc(m));
+    base = __shfl_sync(m, base, leader);
+    const int at = base + rank;
+    if (at < B) {
+      u64* e = buf + (size_t)at * rw;
+      for (int w = 1; w < rw; ++w) e[w] = x[w];
+      e[0] = kw;
+      if (multi)
+        for (int k = 0; k < nk; ++k) bkv[(size_t)at * nk + k] = kv[k];
+    } else {
+      globalInsert(L, ev, kw, kv, x);
+    }
+  };
+  // Inserts the buffered rows; returns true (in every thread) once the global table has overflowed:
+  // the run's result is discarded then (the caller reruns with a bigger table), so the CTA stops.
+  // Barriers: the count and the flag are read between the first two, so no thread changes them (the
+  // next tile's appends, the next flush's flag) before every thread has read them: the decisions
+  // below are CTA-uniform.
+  auto flush = [&]() -> bool {
+    if (threadIdx.x == 0) stopFlag = *(volatile int*)(L.err + 1);
+    __syncthreads();
+    const int n = min(spillN, B);
+    const bool stop = stopFlag != 0;
+    __syncthreads();
+    if (n == 0 || stop) return stop;
+    if (threadIdx.x == 0) spillN = 0;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+      const u64* e = buf + (size_t)j * rw;
+      double kv[WS_MAX_KEYS];
+      if (multi)
+        for (int k = 0; k < nk; ++k) kv[k] = bkv[(size_t)j * nk + k];
+      else
+        kv[0] = __longlong_as_double((i64)e[0]);
+      globalInsert(L, ev, e[0], kv, e);
+    }
+    __syncthreads();  // the buffer is refilled by the next tile
+    return false;
+  };
+  forEachRowTiles(L, ev, rowFn, flush);
+  if (flush()) return;  // overflowed: the shared table is not merged either
   __syncthreads();
   for (int s = threadIdx.x; s < S; s += blockDim.x) {
-    const u64* row = wsSmem + (size_t)s * rw;
+    const u64* row = tab + (size_t)s * rw;
     if (row[0] == kEmpty) continue;
     double kv[WS_MAX_KEYS];
-    if (ev.nk() > 1)
-      for (int k = 0; k < ev.nk(); ++k) kv[k] = skv[(size_t)s * ev.nk() + k];
+    if (multi)
+      for (int k = 0; k < nk; ++k) kv[k] = skv[(size_t)s * nk + k];
     else
       kv[0] = __longlong_as_double((i64)row[0]);
     globalInsert(L, ev, row[0], kv, row);

@@ -534,7 +534,10 @@ static void aggRun(ws_aggregator& A, const ws_expr_env& env, const ws_jit_progra
   L.probeLimit = (int)std::min<int64_t>(A.cap, 1 << 16);
   const size_t slots = hashSmemSlots(A, 64 * 1024);
   L.smemSlots = (int)slots;
-  const size_t smem = slots * ((size_t)A.lay.rw * 8 + (A.plan.nkeys > 1 ? (size_t)A.plan.nkeys * 8 : 0));
+  const size_t per = (size_t)A.lay.rw * 8 + (A.plan.nkeys > 1 ? (size_t)A.plan.nkeys * 8 : 0);
+  // spill buffer: up to a tile's rows, within 40 KB
+  L.spillRows = (int)std::min<size_t>(kTile, (40 * 1024) / per);
+  const size_t smem = (slots + (size_t)L.spillRows) * per;
   launchScan(f, persistentGrid(f, smem, d.ntiles), smem, L);
 }
 
@@ -739,10 +742,9 @@ int ws_agg_fetch(ws_aggregator* A, int64_t max_groups, double* keys, double* acc
     *ngroups = g;
     if (g > max_groups) throw Error("output buffer too small for " + std::to_string(g) + " groups", WS_ERR_SIZE);
     if (g) {
-      if (nk && keys) WS_CK(cudaMemcpyAsync(keys, A->cachedKeys.p, sizeof(double) * g * nk, cudaMemcpyDeviceToHost, stream()));
-      if (accs) WS_CK(cudaMemcpyAsync(accs, A->cachedAccs.p, sizeof(double) * g * na, cudaMemcpyDeviceToHost, stream()));
-      if (exact) WS_CK(cudaMemcpyAsync(exact, A->cachedExact.p, sizeof(int64_t) * g * na * 2, cudaMemcpyDeviceToHost, stream()));
-      sync();
+      if (nk && keys) d2hLarge(keys, A->cachedKeys.p, sizeof(double) * g * nk);
+      if (accs) d2hLarge(accs, A->cachedAccs.p, sizeof(double) * g * na);
+      if (exact) d2hLarge(exact, A->cachedExact.p, sizeof(int64_t) * g * na * 2);
     }
     A->hi = A->cachedHi;
     A->fetched = true;

@@ -1,7 +1,10 @@
 // Device runtime of libwarpstore_b200: initialisation, per-thread streams, the stream-ordered memory
 // pool, pinned staging, error reporting and the launch helpers (reference: src/gpu.cu:23-240).
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
+#include <deque>
+#include <thread>
 
 #include "ws_internal.h"
 
@@ -128,6 +131,106 @@ void d2hSync(void* h, const void* d, size_t b) {
 void sync() { WS_CK(cudaStreamSynchronize(stream())); }
 void countLaunch(int n) { gLaunches += n; }
 
+// ---- large device -> pageable host copies
+// A copy into pageable memory runs at a fraction of the link speed (the driver stages it and the
+// destination pages fault in on one thread).  Large copies go through a per-thread pinned ring
+// instead: chunk i is copied by DMA into a ring slot while chunks already landed are copied out of
+// their slots by a small pool of host threads.
+namespace {
+constexpr size_t kRingChunk = 8u << 20;
+constexpr int kRingSlots = 4;
+struct PinnedRing {
+  uint8_t* buf = nullptr;
+  cudaEvent_t ev[kRingSlots] = {};
+};
+thread_local PinnedRing tRing;
+
+class CopyPool {
+ public:
+  explicit CopyPool(int n) {
+    for (int i = 0; i < n; ++i) th_.emplace_back([this] { loop(); });
+  }
+  int size() const { return (int)th_.size(); }
+  // memcpy of n bytes split across the pool and the calling thread; returns when all parts are done
+  void copy(uint8_t* dst, const uint8_t* src, size_t n) {
+    const int parts = size() + 1;
+    const size_t per = (n + parts - 1) / parts;
+    std::atomic<int> left{0};
+    {
+      std::lock_guard<std::mutex> l(mu_);
+      for (int p = 1; p < parts; ++p) {
+        const size_t lo = std::min(n, per * p), hi = std::min(n, lo + per);
+        if (hi > lo) {
+          ++left;
+          q_.push_back({dst + lo, src + lo, hi - lo, &left});
+        }
+      }
+    }
+    cv_.notify_all();
+    memcpy(dst, src, std::min(n, per));
+    std::unique_lock<std::mutex> l(mu_);
+    done_.wait(l, [&] { return left.load() == 0; });
+  }
+
+ private:
+  struct Job {
+    uint8_t* dst;
+    const uint8_t* src;
+    size_t n;
+    std::atomic<int>* left;
+  };
+  void loop() {
+    for (;;) {
+      Job j;
+      {
+        std::unique_lock<std::mutex> l(mu_);
+        cv_.wait(l, [&] { return !q_.empty(); });
+        j = q_.front();
+        q_.pop_front();
+      }
+      memcpy(j.dst, j.src, j.n);
+      std::lock_guard<std::mutex> l(mu_);
+      if (--*j.left == 0) done_.notify_all();
+    }
+  }
+  std::vector<std::thread> th_;
+  std::mutex mu_;
+  std::condition_variable cv_, done_;
+  std::deque<Job> q_;
+};
+CopyPool& copyPool() {  // process-wide; never destroyed (its threads idle until exit)
+  static CopyPool* p = new CopyPool((int)std::max(1u, std::min(7u, std::thread::hardware_concurrency() / 2)));
+  return *p;
+}
+}  // namespace
+
+void d2hLarge(void* h, const void* d, size_t b) {
+  if (b < 2 * kRingChunk) {
+    d2hSync(h, d, b);
+    return;
+  }
+  PinnedRing& r = tRing;
+  if (!r.buf) {
+    WS_CK(cudaHostAlloc((void**)&r.buf, kRingChunk * kRingSlots, cudaHostAllocDefault));
+    for (auto& e : r.ev) WS_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  const size_t nchunks = (b + kRingChunk - 1) / kRingChunk;
+  auto issue = [&](size_t i) {
+    const int slot = (int)(i % kRingSlots);
+    const size_t lo = i * kRingChunk, n = std::min(kRingChunk, b - lo);
+    WS_CK(cudaMemcpyAsync(r.buf + (size_t)slot * kRingChunk, (const uint8_t*)d + lo, n, cudaMemcpyDeviceToHost, stream()));
+    WS_CK(cudaEventRecord(r.ev[slot], stream()));
+  };
+  for (size_t i = 0; i < std::min<size_t>(kRingSlots, nchunks); ++i) issue(i);
+  for (size_t i = 0; i < nchunks; ++i) {
+    const int slot = (int)(i % kRingSlots);
+    WS_CK(cudaEventSynchronize(r.ev[slot]));
+    const size_t lo = i * kRingChunk, n = std::min(kRingChunk, b - lo);
+    copyPool().copy((uint8_t*)h + lo, r.buf + (size_t)slot * kRingChunk, n);
+    if (i + kRingSlots < nchunks) issue(i + kRingSlots);
+  }
+}
+
 // Per-thread pinned staging buffer; an event marks the last copy out of it so reuse waits only then.
 namespace {
 thread_local uint8_t* tStage = nullptr;
@@ -241,7 +344,7 @@ int ws_h2d(void* dst, const void* src, size_t bytes) {
     }
   });
 }
-int ws_d2h(void* dst, const void* src, size_t bytes) { return guarded([&] { d2hSync(dst, src, bytes); }); }
+int ws_d2h(void* dst, const void* src, size_t bytes) { return guarded([&] { d2hLarge(dst, src, bytes); }); }
 int ws_d2d(void* dst, const void* src, size_t bytes) {
   return guarded([&] {
     if (bytes) WS_CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, stream()));

@@ -17,6 +17,7 @@ Workloads (sizes as benchmarked):
 """
 from __future__ import annotations
 
+import ctypes
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -294,3 +295,239 @@ def join_aggregate_run(build: Table, probe: Table, plans, impl: str = "ours", ti
     for p in (idx, ob, op):
         ref.free(p)
     return keys, accs, m
+
+
+# ---------------------------------------------------------------- high-cardinality GROUP BY
+# 100,000,000 rows; key int64 = a bijective 64-bit mix of a Zipf(s=1.1) rank over 10,000,000 ranks
+# (sparse keys, so the engine hashes rather than indexing dense arrays); payload int64 U[0, 1e9);
+# s int32 dictionary codes U[0, 5,000,000) (a string column's codes); WHERE payload < c (c drawn from
+# the seed) GROUP BY key: COUNT(*), SUM(payload) [, COUNT(DISTINCT s)].
+HC_ROWS = 100_000_000
+HC_RANKS = 10_000_000
+HC_DICT = 5_000_000
+HC_ZIPF_S = 1.1
+HC_BYTES_PER_ROW = 16  # key + payload (the distinct pass also reads s: 20)
+
+
+def zipf_ranks(rng: np.random.Generator, n: int, nranks: int, s: float) -> np.ndarray:
+    """n draws of a rank in [0, nranks) with P(r) proportional to (r + 1)^-s (inverse CDF)."""
+    w = np.arange(1, nranks + 1, dtype=np.float64) ** -s
+    cdf = np.cumsum(w)
+    cdf /= cdf[-1]
+    out = np.empty(n, dtype=np.int64)
+    step = 1 << 24
+    for lo in range(0, n, step):  # bounded temporaries
+        hi = min(n, lo + step)
+        out[lo:hi] = np.searchsorted(cdf, rng.random(hi - lo), side="right")
+    np.minimum(out, nranks - 1, out=out)
+    return out
+
+
+def mix64_np(x: np.ndarray) -> np.ndarray:
+    """splitmix64 finalizer over uint64 (a bijection)."""
+    z = x.astype(np.uint64)
+    with np.errstate(over="ignore"):
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    return z
+
+
+def high_cardinality(n: int = HC_ROWS, nranks: int = HC_RANKS, ndict: int = HC_DICT, seed: int = 4) -> Table:
+    rng = np.random.default_rng(seed)
+    ranks = zipf_ranks(rng, n, nranks, HC_ZIPF_S)
+    key = mix64_np(ranks.astype(np.uint64) + np.uint64(seed * 0x9E3779B9 + 1)).view(np.int64)
+    key[key == abi.NULL_I64] += 1  # never the BIGINT NULL sentinel
+    del ranks
+    t = Table(n)
+    t.add("key", abi.T_I64, key)
+    t.add("payload", abi.T_I64, rng.integers(0, 1_000_000_000, n, dtype=np.int64))
+    t.add("s", abi.T_I32, rng.integers(0, ndict, n, dtype=np.int32))
+    return t
+
+
+def high_cardinality_cut(seed: int = 4) -> int:
+    """The predicate constant c of `payload < c` for a run (selectivity 30%..90%)."""
+    return int(np.random.default_rng(seed + 1000).integers(300_000_000, 900_000_001))
+
+
+def high_cardinality_query(t: Table, cut: int, distinct: bool = False):
+    """(env, AggQuery, distinct program or None): GROUP BY key COUNT(*), SUM(payload)."""
+    e = env_for(t)
+    aq = q.AggQuery(e, q.col(1).lt(cut), [(q.col(0), True)], [q.Agg("COUNT"), q.Agg("SUM", q.col(1), "BIGINT", True)],
+                    distinct=distinct)
+    dprog = e.compile(q.col(2)) if distinct else None
+    return e, aq, dprog
+
+
+def plain_capacity(plan: abi.AggPlan, est: int) -> int:
+    """The engine's hash table capacity for an estimate of the group count: pow2 >= 2 est, at least
+    1024, the table kept <= 1 GiB (src/engine_select.cpp:1230-1235)."""
+    cap = 1024
+    max_cap = (1 << 30) // (8 + 8 * plan.nkeys + 8 * plan.naggs)
+    while cap < est * 2 and cap * 2 <= max_cap:
+        cap <<= 1
+    return cap
+
+
+def grow_capacity(cap: int, groups: int) -> int:
+    """Capacity after an overflow: pow2 >= max(4 cap, 4 groups) (src/engine_select.cpp:1514-1522)."""
+    want = max(cap * 4, groups * 4)
+    c = 1
+    while c < want:
+        c <<= 1
+    return c
+
+
+def hash_aggregate_run(batches: list, e, aq, cap: int, impl: str = "ours", jit=None):
+    """GROUP BY over device batches with the engine's overflow retry: (keys, accs engine format,
+    final capacity, runs)."""
+    from . import ops
+    runs = 0
+    while True:
+        runs += 1
+        if impl == "ours":
+            agg = ops.GpuAggregator(aq.plan, cap)
+            agg.add_batches(e.ncols, batches)
+            agg.run(e.env, jit)
+            if agg.overflowed():
+                g = agg.group_count()
+                agg.close()
+                cap = grow_capacity(cap, g)
+                continue
+            keys, accs, _ = agg.fetch(exact=False)
+            agg.close()
+            return keys, accs, cap, runs
+        from oracle import ref  # the reference's operators (test infrastructure)
+        keys, accs, g, ovf, _ = ref.aggregate(e.env, e.ncols, aq.plan, batches, None, cap)
+        if ovf:
+            cap = grow_capacity(cap, g)
+            continue
+        return keys, accs, cap, runs
+
+
+def distinct_plans(e, aq, dprog, dist_int: bool = True):
+    """Phase-1 plan of COUNT(DISTINCT x): the plan's keys plus x, every aggregate as a partial per
+    (keys, x) (src/engine_select.cpp:1404-1409)."""
+    p1 = abi.AggPlan()
+    ctypes.memmove(ctypes.byref(p1), ctypes.byref(aq.plan), ctypes.sizeof(abi.AggPlan))
+    nk = aq.plan.nkeys
+    p1.nkeys = nk + 1
+    p1.keys[nk] = dprog
+    p1.keyInt[nk] = 1 if dist_int else 0
+    p1.densePriv = 0
+    return p1
+
+
+def distinct_phase2(plan: abi.AggPlan, p1: abi.AggPlan, keys_ptr: int, accs_ptr: int, g1: int, dist_int: bool = True):
+    """Phase 2 over the compacted (keys, x) groups (column-major device arrays): GROUP BY the keys,
+    COUNT / SUM partials summed, MIN by MIN, MAX by MAX, plus one slot counting the pairs whose x is
+    not NULL (src/engine_select.cpp:1436-1470).  Returns (env2, ncols2, plan2)."""
+    nk, na = plan.nkeys, p1.naggs
+    env2 = abi.ExprEnv()
+    nc = 0
+    for k in range(nk + 1):
+        is_int = (plan.keyInt[k] != 0) if k < nk else dist_int
+        env2.cols[k] = abi.ColView(keys_ptr + k * g1 * 8, abi.T_I64 if is_int else abi.T_F64, 0, 0, 0)
+        env2.code[nc] = abi.Instr(abi.OP_COL, 1 if is_int else 0, k)
+        nc += 1
+    p2 = abi.AggPlan()
+    p2.nkeys = nk
+    for k in range(nk):
+        p2.keys[k] = abi.Prog(k, 1)
+        p2.keyInt[k] = plan.keyInt[k]
+    for a in range(na):
+        env2.cols[nk + 1 + a] = abi.ColView(accs_ptr + a * g1 * 8, abi.T_I64 if p1.aggBits[a] else abi.T_F64, 0, 0, 0)
+        p2.aggs[a] = abi.Prog(nc, 1)
+        env2.code[nc] = abi.Instr(abi.OP_COL, 0, nk + 1 + a)
+        nc += 1
+        p2.ops[a] = abi.AGG_SUM if p1.ops[a] == abi.AGG_COUNT else p1.ops[a]
+        p2.aggInt[a] = p2.aggBits[a] = p1.aggBits[a]
+        p2.aggPart[a] = 0
+    if dist_int:
+        p2.aggs[na] = abi.Prog(nc, 1)
+        env2.code[nc] = abi.Instr(abi.OP_CONST, 0, 0)
+        env2.consts[0] = 1.0
+        nc += 1
+    else:
+        p2.aggs[na] = abi.Prog(nc, 3)
+        env2.code[nc] = abi.Instr(abi.OP_COL, 0, nk)
+        env2.code[nc + 1] = abi.Instr(abi.OP_ISNULL, 0, 0)
+        env2.code[nc + 2] = abi.Instr(abi.OP_NOT, 0, 0)
+        nc += 3
+    p2.ops[na] = abi.AGG_SUM
+    p2.aggInt[na] = 0
+    p2.naggs = na + 1
+    return env2, nk + 1 + na, p2
+
+
+def distinct_aggregate_run(batches: list, e, aq, dprog, rows_in: int, impl: str = "ours", timer=None):
+    """GROUP BY keys with COUNT(DISTINCT x) as the engine runs it: phase 1 hash GROUP BY (keys, x)
+    with capacity pow2 >= min(rows, 2^22) and the overflow retry, compaction on the device, phase 2
+    GROUP BY keys over the distinct pairs (src/engine_select.cpp:1397-1492).  Returns (keys, accs in
+    the engine format with the distinct count as the last slot, phase-1 runs, distinct pairs)."""
+    import contextlib
+
+    from . import ops
+    timer = timer or (lambda name: contextlib.nullcontext())
+    p1 = distinct_plans(e, aq, dprog)
+    cap1 = 1024
+    while cap1 < min(max(rows_in, 1), 1 << 22):
+        cap1 <<= 1
+    runs = 0
+    if impl == "ours":
+        ops.jit_set_mode(abi.JIT_SYNC)
+        try:
+            jit1 = ops.jit_get(e.env, e.ncols, p1, abi.JF_GROUPED, "aggregate (distinct pairs)")
+            with timer("phase 1 (keys, x)"):
+                while True:
+                    runs += 1
+                    a1 = ops.GpuAggregator(p1, cap1)
+                    a1.add_batches(e.ncols, batches)
+                    a1.run(e.env, jit1)
+                    if a1.overflowed():
+                        g = a1.group_count()
+                        a1.close()
+                        cap1 = grow_capacity(cap1, g)
+                        continue
+                    kp, ap, g1 = a1.compact()
+                    a1.close()
+                    break
+            with timer("phase 2 (keys)"):
+                env2, nc2, p2 = distinct_phase2(aq.plan, p1, kp, ap, g1)
+                cap2 = 1024
+                while cap2 < 2 * g1:
+                    cap2 <<= 1
+                jit2 = ops.jit_get(env2, nc2, p2, abi.JF_GROUPED, "count distinct")
+                a2 = ops.GpuAggregator(p2, cap2)
+                a2.add_batches(nc2, [(g1, 0, [env2.cols[c] for c in range(nc2)])])
+                a2.run(env2, jit2)
+                if a2.overflowed():
+                    raise RuntimeError("phase 2 overflowed a table of twice the pair count")
+                keys, accs, _ = a2.fetch(exact=False)
+                a2.close()
+            ops.tmp_free(kp)
+            ops.tmp_free(ap)
+        finally:
+            ops.jit_set_mode(-1)
+        return keys, accs, runs, g1
+    from oracle import ref  # the reference's operators (test infrastructure)
+    with timer("phase 1 (keys, x)"):
+        while True:
+            runs += 1
+            kp, ap, g1, ovf, _ = ref.aggregate_compact(e.env, e.ncols, p1, batches, None, cap1)
+            if ovf:
+                cap1 = grow_capacity(cap1, g1)
+                continue
+            break
+    with timer("phase 2 (keys)"):
+        env2, nc2, p2 = distinct_phase2(aq.plan, p1, kp, ap, g1)
+        cap2 = 1024
+        while cap2 < 2 * g1:
+            cap2 <<= 1
+        keys, accs, _, ovf, _ = ref.aggregate(env2, nc2, p2, [(g1, 0, [env2.cols[c] for c in range(nc2)])], None, cap2)
+        if ovf:
+            raise RuntimeError("phase 2 overflowed a table of twice the pair count")
+    ref.free(kp)
+    ref.free(ap)
+    return keys, accs, runs, g1
