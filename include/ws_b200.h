@@ -125,6 +125,45 @@ int ws_hash_join_parts(ws_col_view build_key, const int64_t* boff, int nbparts, 
                        int64_t* m);
 int ws_hash_join(ws_col_view build_key, int64_t nb, ws_col_view probe_key, int64_t np, int32_t** out_build,
                  int32_t** out_probe, int64_t* m);
+/* gpuHashJoinOuter (src/gpu.h:187-188): every probe row appears, with build row -1 when it matched
+ * nothing (NULL keys never match); full != 0 also appends each build row that matched nothing, with
+ * probe row -1.  Pairs are freed with ws_tmp_free. */
+int ws_hash_join_outer(ws_col_view build_key, int64_t nb, ws_col_view probe_key, int64_t np, int full,
+                       int32_t** out_build, int32_t** out_probe, int64_t* m);
+/* gpuCrossJoin (src/gpu.h:189): out_a[i] = i / nb, out_b[i] = i % nb; more than 200,000,000 pairs is
+ * an error (WS_ERR_INTERNAL, as the engine's). */
+int ws_cross_join(int64_t na, int64_t nb, int32_t** out_a, int32_t** out_b, int64_t* m);
+/* gpuKeyBitmap (src/gpu.h:174): bits[] (nbits bits, cleared first) gets bit (key - lo) of every
+ * non-NULL key in [lo, lo + nbits). */
+int ws_key_bitmap(ws_col_view key, int64_t n, int64_t lo, int64_t nbits, uint32_t* bits);
+/* gpuSetBits (src/gpu.h:176): sets bit idx[j] for every j (deleted-row bitmaps). */
+int ws_set_bits(uint32_t* bits, const int32_t* idx, int64_t m);
+
+/* ---- codes, gathers with NULLs, evaluation at rows (src/gpu.h:145-172, :190-195) */
+/* gpuRemapCodes: out[i] = map[in[i]]; NULL stays NULL, codes outside [0, map_n) give -2. */
+int ws_remap_codes(const int32_t* in, int64_t n, const int32_t* map, int64_t map_n, int32_t* out);
+/* gpuBitsToDouble: dst[j] = (double) of the int64 stored bit for bit in src[j]. */
+int ws_bits_to_double(const double* src, int64_t n, double* dst);
+/* gpuGatherNull: like ws_gather, index -1 writes the type's NULL (ptype WS_PT_I32 / I64 / F64). */
+int ws_gather_null(const void* src, int ptype, const int32_t* idx, int64_t m, void* dst);
+/* gpuGatherBytes: elements of esize bytes (a multiple of 4); index -1 gives a NULL element (every
+ * 32-bit word a NaN float when nulls != 0, else zeros). */
+int ws_gather_bytes(const void* src, int esize, const int32_t* idx, int64_t m, void* dst, int nulls);
+/* gpuGatherEnc: raw values of an encoded segment column (view.enc != 0) at idx, as ptype. */
+int ws_gather_enc(ws_col_view view, int ptype, const int32_t* idx, int64_t m, void* dst);
+/* gpuEvalAt: out[j] = prog at row idx[j] (row j when idx is null), as a double (NULL = NaN). */
+int ws_eval_at(const ws_expr_env* env, int ncols, ws_prog prog, const int32_t* idx, int64_t m, double* out);
+/* gpuEvalAtInt: the same as int64 (NULL = the BIGINT sentinel): a single integer column exactly,
+ * integer programs exactly (checked arithmetic), other programs rounded from their double value. */
+int ws_eval_at_int(const ws_expr_env* env, int ncols, ws_prog prog, const int32_t* idx, int64_t m, int64_t* out);
+
+/* ---- ORDER BY (src/gpu.h:197-199) */
+/* gpuSortPerm: stable permutation sorting rows 0..m-1 by keys[0] (most significant) .. keys[nkeys-1],
+ * each ascending or descending (desc[k] != 0); NULL (NaN) sorts as -inf (first ascending, last
+ * descending), -0 as 0.  *out_perm (m int32, ws_tmp_free) receives the row order. */
+int ws_sort_perm(const double* const* keys, const int* desc, int nkeys, int64_t m, int32_t** out_perm);
+/* gpuMapRank: keys[j] = rank[(int)keys[j]] (dictionary code -> lexicographic rank), NULL -> -1. */
+int ws_map_rank(double* keys, const int32_t* rank, int64_t m);
 
 /* ---- compiled plans (src/jit.h:33-75) */
 typedef struct ws_jit_info {

@@ -232,5 +232,61 @@ inline int64_t gpuHashJoin(ColView buildKey, int64_t nb, ColView probeKey, int64
                            DevVec<int32_t>& outProbe) {
   return gpuHashJoinParts(buildKey, {0, nb}, probeKey, {0, np}, outBuild, outProbe, nullptr);
 }
+inline int64_t gpuHashJoinOuter(ColView buildKey, int64_t nb, ColView probeKey, int64_t np, DevVec<int32_t>& outBuild,
+                                DevVec<int32_t>& outProbe, bool full) {
+  int32_t *ob = nullptr, *op = nullptr;
+  int64_t m = 0;
+  wsCheck(ws_hash_join_outer(*(const ws_col_view*)&buildKey, nb, *(const ws_col_view*)&probeKey, np, full ? 1 : 0, &ob,
+                             &op, &m));
+  outBuild = DevVec<int32_t>(ob, m);
+  outProbe = DevVec<int32_t>(op, m);
+  return m;
+}
+inline int64_t gpuCrossJoin(int64_t na, int64_t nb, DevVec<int32_t>& outA, DevVec<int32_t>& outB) {
+  int32_t *a = nullptr, *b = nullptr;
+  int64_t m = 0;
+  wsCheck(ws_cross_join(na, nb, &a, &b, &m));
+  outA = DevVec<int32_t>(a, m);
+  outB = DevVec<int32_t>(b, m);
+  return m;
+}
+inline void gpuKeyBitmap(ColView key, int64_t n, int64_t lo, int64_t nbits, uint32_t* bits) {
+  wsCheck(ws_key_bitmap(*(const ws_col_view*)&key, n, lo, nbits, bits));
+}
+inline void gpuSetBits(uint32_t* bits, const int32_t* idx, int64_t m) { wsCheck(ws_set_bits(bits, idx, m)); }
+
+// ---- codes, NULL-aware gathers, evaluation at rows (src/gpu.h:145-172, :190-195)
+inline void gpuRemapCodes(const int32_t* in, int64_t n, const int32_t* map, int64_t mapN, int32_t* out) {
+  wsCheck(ws_remap_codes(in, n, map, mapN, out));
+}
+inline void gpuBitsToDouble(const double* src, int64_t n, double* dst) { wsCheck(ws_bits_to_double(src, n, dst)); }
+template <class PType>
+inline void gpuGatherNull(const void* src, PType t, const int32_t* idx, int64_t m, void* dst) {
+  wsCheck(ws_gather_null(src, (int)t, idx, m, dst));
+}
+inline void gpuGatherBytes(const void* src, int esize, const int32_t* idx, int64_t m, void* dst, bool nulls) {
+  wsCheck(ws_gather_bytes(src, esize, idx, m, dst, nulls ? 1 : 0));
+}
+template <class PType>
+inline void gpuGatherEnc(const ColView& v, PType t, const int32_t* idx, int64_t m, void* dst) {
+  wsCheck(ws_gather_enc(*(const ws_col_view*)&v, (int)t, idx, m, dst));
+}
+inline void gpuEvalAt(const ExprEnv& env, Prog prog, const int32_t* idx, int64_t m, double* out) {
+  wsCheck(ws_eval_at((const ws_expr_env*)&env, WS_MAX_COLS, *(const ws_prog*)&prog, idx, m, out));
+}
+inline void gpuEvalAtInt(const ExprEnv& env, Prog prog, const int32_t* idx, int64_t m, int64_t* out) {
+  wsCheck(ws_eval_at_int((const ws_expr_env*)&env, WS_MAX_COLS, *(const ws_prog*)&prog, idx, m, out));
+}
+
+// ---- ORDER BY (src/gpu.h:197-199)
+inline DevVec<int32_t> gpuSortPerm(const std::vector<std::pair<const double*, bool>>& keys, int64_t m) {
+  std::vector<const double*> k;
+  std::vector<int> d;
+  for (auto& [p, desc] : keys) k.push_back(p), d.push_back(desc ? 1 : 0);
+  int32_t* perm = nullptr;
+  wsCheck(ws_sort_perm(k.data(), d.data(), (int)k.size(), m, &perm));
+  return DevVec<int32_t>(perm, m);
+}
+inline void gpuMapRank(double* keys, const int32_t* rank, int64_t m) { wsCheck(ws_map_rank(keys, rank, m)); }
 
 }  // namespace gdb

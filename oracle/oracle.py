@@ -41,6 +41,11 @@ def lib() -> C.CDLL:
         l.ws_oracle_hash_join.restype = C.c_int64
         l.ws_oracle_hash_join.argtypes = [abi.ColView, C.c_int64, abi.ColView, C.c_int64, C.c_int, P, P]
         l.ws_oracle_gather_multi.argtypes = [P, P, C.c_int, C.c_int, C.c_int, P, C.c_int64, P]
+        l.ws_oracle_hash_join_outer.restype = C.c_int64
+        l.ws_oracle_hash_join_outer.argtypes = [abi.ColView, C.c_int64, abi.ColView, C.c_int64, C.c_int, P, P]
+        l.ws_oracle_sort_perm.argtypes = [P, P, C.c_int, C.c_int64, P]
+        l.ws_oracle_eval_at.argtypes = [C.POINTER(abi.ExprEnv), P, abi.Prog, P, C.c_int64, C.c_int, P,
+                                        C.POINTER(C.c_int)]
         l.ws_oracle_eval.restype = C.c_double
         l.ws_oracle_eval.argtypes = [C.POINTER(abi.ExprEnv), P, abi.Prog, C.c_int64, C.POINTER(C.c_int64),
                                      C.POINTER(C.c_int), C.POINTER(C.c_int)]
@@ -132,3 +137,36 @@ def eval_row(env: abi.ExprEnv, cols, prog: abi.Prog, row: int):
     arr = (abi.ColView * len(cols))(*cols)
     d = lib().ws_oracle_eval(C.byref(env), arr, prog, row, C.byref(iv), C.byref(ii), C.byref(ov))
     return d, iv.value, bool(ii.value), bool(ov.value)
+
+
+def hash_join_outer(build_key: abi.ColView, nb: int, probe_key: abi.ColView, np_: int, full: bool):
+    l = lib()
+    m = l.ws_oracle_hash_join_outer(build_key, nb, probe_key, np_, int(full), None, None)
+    ob = np.empty(max(m, 1), dtype=np.int32)
+    op = np.empty(max(m, 1), dtype=np.int32)
+    l.ws_oracle_hash_join_outer(build_key, nb, probe_key, np_, int(full), ob.ctypes.data, op.ctypes.data)
+    return ob[:m], op[:m]
+
+
+def sort_perm(keys: list, desc: list) -> np.ndarray:
+    """Stable sort permutation of host double columns (first = most significant)."""
+    keys = [np.ascontiguousarray(k, dtype=np.float64) for k in keys]
+    m = len(keys[0]) if keys else 0
+    kp = (P * max(len(keys), 1))(*[k.ctypes.data for k in keys])
+    dp = (C.c_int * max(len(desc), 1))(*[int(d) for d in desc])
+    perm = np.empty(max(m, 1), dtype=np.int32)
+    lib().ws_oracle_sort_perm(kp, dp, len(keys), m, perm.ctypes.data)
+    return perm[:m]
+
+
+def eval_at(env: abi.ExprEnv, cols: list, prog: abi.Prog, idx, m: int, as_int: bool = False):
+    """(values [m] float64 or int64, overflow flag) of one expression at rows idx (or 0..m-1)."""
+    arr = (abi.ColView * max(len(cols), 1))(*cols)
+    out = np.empty(max(m, 1), dtype=np.int64 if as_int else np.float64)
+    ix = None
+    if idx is not None:
+        idx = np.ascontiguousarray(idx, dtype=np.int32)
+        ix = idx.ctypes.data
+    ov = C.c_int()
+    lib().ws_oracle_eval_at(C.byref(env), arr, prog, ix, m, int(as_int), out.ctypes.data, C.byref(ov))
+    return out[:m], bool(ov.value)

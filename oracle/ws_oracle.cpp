@@ -988,4 +988,93 @@ void ws_oracle_gather_multi(const ws_col_view* src, const int64_t* boff, int nb,
   }
 }
 
+
+/* ---- outer join, sort permutation, evaluation at rows (restatements of src/gpu.cu:1197-1293,
+ * :1323-1361, :862-888, :1011-1019) */
+
+int64_t ws_oracle_hash_join_outer(ws_col_view build_key, int64_t nb, ws_col_view probe_key, int64_t np, int full,
+                                  int32_t* out_build, int32_t* out_probe) {
+  std::unordered_map<int64_t, std::vector<int32_t>> table;
+  table.reserve((size_t)nb * 2);
+  for (int64_t i = 0; i < nb; ++i) {
+    int64_t k;
+    if (joinKey(build_key, i, k)) table[k].push_back((int32_t)i);
+  }
+  for (auto& kv : table) std::sort(kv.second.begin(), kv.second.end());
+  std::vector<uint8_t> matched(full ? (size_t)nb : 0, 0);
+  int64_t o = 0;
+  auto emit = [&](int32_t b, int32_t p) {
+    if (out_build) out_build[o] = b, out_probe[o] = p;
+    ++o;
+  };
+  for (int64_t j = 0; j < np; ++j) {  // probe order: matches, or one pair with build row -1
+    int64_t k;
+    auto it = joinKey(probe_key, j, k) ? table.find(k) : table.end();
+    if (it == table.end()) {
+      emit(-1, (int32_t)j);
+      continue;
+    }
+    for (int32_t b : it->second) {
+      emit(b, (int32_t)j);
+      if (full) matched[b] = 1;
+    }
+  }
+  if (full)
+    for (int64_t i = 0; i < nb; ++i)
+      if (!matched[i]) emit((int32_t)i, -1);
+  return o;
+}
+
+static uint64_t orderKeyOf(double v, bool desc) {
+  if (v != v) v = -INFINITY;  // NULL first (ascending)
+  if (v == 0.0) v = 0.0;
+  uint64_t b;
+  memcpy(&b, &v, 8);
+  b = (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+  return desc ? ~b : b;
+}
+
+void ws_oracle_sort_perm(const double* const* keys, const int* desc, int nkeys, int64_t m, int32_t* perm) {
+  std::vector<std::vector<uint64_t>> k(nkeys, std::vector<uint64_t>((size_t)m));
+  for (int c = 0; c < nkeys; ++c)
+    for (int64_t i = 0; i < m; ++i) k[c][i] = orderKeyOf(keys[c][i], desc[c] != 0);
+  for (int64_t i = 0; i < m; ++i) perm[i] = (int32_t)i;
+  std::stable_sort(perm, perm + m, [&](int32_t a, int32_t b) {
+    for (int c = 0; c < nkeys; ++c)
+      if (k[c][a] != k[c][b]) return k[c][a] < k[c][b];
+    return false;
+  });
+}
+
+void ws_oracle_eval_at(const ws_expr_env* env, const ws_col_view* cols, ws_prog prog, const int32_t* idx, int64_t m,
+                       int as_int, void* out, int* ovf) {
+  Tree t = buildTree(*env, prog);
+  const Node& n = t.nodes[t.root];
+  const ws_instr in0 = env->code[prog.start];
+  const bool single = prog.len == 1 && in0.op == WS_OP_COL && cols[in0.arg].t != 2;
+  BlockEval ev{*env, cols, 0};
+  for (int64_t j = 0; j < m; ++j) {
+    const int64_t r = idx ? idx[j] : j;
+    Vals v;
+    ev.eval(t, t.root, r, 1, v);
+    if (!as_int) {
+      ((double*)out)[j] = n.isInt ? (double)v.i[0] : v.d[0];
+      continue;
+    }
+    int64_t o;
+    if (single) {  // the column's stored value; INT NULL widened to the BIGINT NULL
+      const ws_col_view& c = cols[in0.arg];
+      int64_t x = colInt(c, r);
+      if ((c.t == 0 || c.t == 3) && x == (int64_t)(int32_t)0x80000000) x = (int64_t)0x8000000000000000ull;
+      o = x;
+    } else if (n.isInt) {
+      o = v.i[0];
+    } else {
+      o = v.d[0] != v.d[0] ? (int64_t)0x8000000000000000ull : llround(v.d[0]);
+    }
+    ((int64_t*)out)[j] = o;
+  }
+  if (ovf) *ovf = ev.ovf;
+}
+
 }  // extern "C"

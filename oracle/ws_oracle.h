@@ -62,6 +62,17 @@ int64_t ws_oracle_hash_join(ws_col_view build_key, int64_t nb, ws_col_view probe
 void ws_oracle_gather_multi(const ws_col_view* src, const int64_t* boff, int nb, int ptype, int esize,
                             const int32_t* idx, int64_t m, void* dst);
 
+/* Outer join (src/gpu.cu:1197-1293): the inner pairs, (-1, probe row) for each unmatched probe row, and
+ * with full (build row, -1) for each build row that matched nothing.  Returns the count. */
+int64_t ws_oracle_hash_join_outer(ws_col_view build_key, int64_t nb, ws_col_view probe_key, int64_t np, int full,
+                                  int32_t* out_build, int32_t* out_probe);
+/* Stable multi-key sort permutation (src/gpu.cu:1323-1361): NULL as -inf, -0 as 0, desc[k] inverts. */
+void ws_oracle_sort_perm(const double* const* keys, const int* desc, int nkeys, int64_t m, int32_t* perm);
+/* Evaluation at rows (src/gpu.cu:862-888, :1011-1019): doubles, or int64 when as_int (exact integer
+ * programs, a single integer column as stored, else the double rounded; NULL = the BIGINT sentinel). */
+void ws_oracle_eval_at(const ws_expr_env* env, const ws_col_view* cols, ws_prog prog, const int32_t* idx, int64_t m,
+                       int as_int, void* out, int* ovf);
+
 #ifdef __cplusplus
 }
 #endif

@@ -62,6 +62,20 @@ SIGNATURES = {
     "ws_hash_join_parts": (C.c_int, [abi.ColView, P, C.c_int, abi.ColView, P, C.c_int, C.POINTER(P), C.POINTER(P),
                                      P, I64P]),
     "ws_hash_join": (C.c_int, [abi.ColView, C.c_int64, abi.ColView, C.c_int64, C.POINTER(P), C.POINTER(P), I64P]),
+    "ws_hash_join_outer": (C.c_int, [abi.ColView, C.c_int64, abi.ColView, C.c_int64, C.c_int, C.POINTER(P),
+                                     C.POINTER(P), I64P]),
+    "ws_cross_join": (C.c_int, [C.c_int64, C.c_int64, C.POINTER(P), C.POINTER(P), I64P]),
+    "ws_key_bitmap": (C.c_int, [abi.ColView, C.c_int64, C.c_int64, C.c_int64, P]),
+    "ws_set_bits": (C.c_int, [P, P, C.c_int64]),
+    "ws_remap_codes": (C.c_int, [P, C.c_int64, P, C.c_int64, P]),
+    "ws_bits_to_double": (C.c_int, [P, C.c_int64, P]),
+    "ws_gather_null": (C.c_int, [P, C.c_int, P, C.c_int64, P]),
+    "ws_gather_bytes": (C.c_int, [P, C.c_int, P, C.c_int64, P, C.c_int]),
+    "ws_gather_enc": (C.c_int, [abi.ColView, C.c_int, P, C.c_int64, P]),
+    "ws_eval_at": (C.c_int, [C.POINTER(abi.ExprEnv), C.c_int, abi.Prog, P, C.c_int64, P]),
+    "ws_eval_at_int": (C.c_int, [C.POINTER(abi.ExprEnv), C.c_int, abi.Prog, P, C.c_int64, P]),
+    "ws_sort_perm": (C.c_int, [P, P, C.c_int, C.c_int64, C.POINTER(P)]),
+    "ws_map_rank": (C.c_int, [P, P, C.c_int64]),
     "ws_jit_set_mode": (C.c_int, [C.c_int]),
     "ws_jit_mode": (C.c_int, []),
     "ws_jit_set_default_mode": (C.c_int, [C.c_int]),

@@ -214,6 +214,9 @@ struct JOut {
   int32_t* op;
   int64_t outBase, capacity;
   unsigned long long* counter;
+  int outer;         // every probe row without a match gives one pair (-1, probe row)
+  uint8_t* matched;  // non-null: matched[build row - rowBase] = 1 for every build row that matched
+  int64_t rowBase;   // first build row of the partition (matched[] index base)
 };
 
 // Writes the warp's staged pairs [0, fill) (all lanes of the warp call it).
@@ -285,7 +288,13 @@ __global__ void __launch_bounds__(kJThreads) kJoinDenseProbe(ws_col_view key, in
 #pragma unroll
     for (int j = 0; j < kJPer; ++j) b[j] = idx[j] < range ? __ldg(table + idx[j]) : -1;
 #pragma unroll
-    for (int j = 0; j < kJPer; ++j) jStage(out, st, fill, b[j] >= 0, b[j], (int)(base + w0 + j * 32 + lane), lane);
+    for (int j = 0; j < kJPer; ++j) {
+      const bool inRange = w0 + j * 32 + lane < n;
+      // an unmatched probe row of an outer join pairs with build row -1
+      const bool hit = b[j] >= 0, miss = out.outer && inRange && !hit;
+      if (hit && out.matched) out.matched[b[j] - out.rowBase] = 1;
+      jStage(out, st, fill, hit || miss, hit ? b[j] : -1, (int)(base + w0 + j * 32 + lane), lane);
+    }
     if (dup) {
       for (;;) {
         bool any = false;
@@ -296,7 +305,10 @@ __global__ void __launch_bounds__(kJThreads) kJoinDenseProbe(ws_col_view key, in
         }
         if (!__any_sync(0xffffffffu, any)) break;
 #pragma unroll
-        for (int j = 0; j < kJPer; ++j) jStage(out, st, fill, b[j] >= 0, b[j], (int)(base + w0 + j * 32 + lane), lane);
+        for (int j = 0; j < kJPer; ++j) {
+          if (b[j] >= 0 && out.matched) out.matched[b[j] - out.rowBase] = 1;
+          jStage(out, st, fill, b[j] >= 0, b[j], (int)(base + w0 + j * 32 + lane), lane);
+        }
       }
     }
   }
@@ -326,7 +338,10 @@ __global__ void __launch_bounds__(kJThreads) kJoinProbe(ws_col_view key, int64_t
     for (int j = 0; j < kJPer; ++j) {
       const int64_t r = w0 + j * 32 + lane;
       long long k;
-      if (r < n && joinKeyStream(key, base + r, k)) {
+      const bool valid = r < n && joinKeyStream(key, base + r, k);
+      // outer join: a NULL-key probe row matches nothing; it is emitted once, in pass 0
+      jStage(out, st, fill, out.outer && jp.pass == 0 && r < n && !valid, -1, (int)(base + r), lane);
+      if (valid) {
         const u64 h = mix64((u64)k);
         if (jp.mine(h)) {
 #pragma unroll
@@ -337,8 +352,9 @@ __global__ void __launch_bounds__(kJThreads) kJoinProbe(ws_col_view key, int64_t
       }
     }
     unsigned steps = 0;
+    bool headHit = false;  // the key at the head of the queue has matched
     while (__any_sync(0xffffffffu, nq > 0)) {
-      bool hitA = false, hitB = false, done = true;
+      bool hitA = false, hitB = false, done = true, unmatched = false;
       int rowA = 0, rowB = 0, pr = 0;
       if (nq > 0) {
         const unsigned s0 = qs[0];
@@ -357,17 +373,23 @@ __global__ void __launch_bounds__(kJThreads) kJoinProbe(ws_col_view key, int64_t
           else if (b.x == qk[0]) hitB = true, rowB = (int)(unsigned)b.y;
         }
         ++steps;
+        headHit |= hitA || hitB;
+        if (hitA && out.matched) out.matched[rowA - out.rowBase] = 1;
+        if (hitB && out.matched) out.matched[rowB - out.rowBase] = 1;
         if (!done && steps <= mask) {
           qs[0] = (even + 2) & mask;
         } else {
+          unmatched = out.outer && !headHit;
 #pragma unroll
           for (int q = 0; q < kJPer - 1; ++q) qk[q] = qk[q + 1], qs[q] = qs[q + 1], qr[q] = qr[q + 1];
           --nq;
           steps = 0;
+          headHit = false;
         }
       }
       jStage(out, st, fill, hitA, rowA, pr, lane);
       jStage(out, st, fill, hitB, rowB, pr, lane);
+      jStage(out, st, fill, unmatched, -1, pr, lane);
     }
   }
   __syncwarp();
@@ -561,22 +583,92 @@ int ws_gather(const void* src, int ptype, const int32_t* idx, int64_t m, void* d
   });
 }
 
-int ws_hash_join_parts(ws_col_view build_key, const int64_t* boff, int nbparts, ws_col_view probe_key,
-                       const int64_t* poff, int npparts, int32_t** out_build, int32_t** out_probe, int64_t* out_off,
-                       int64_t* m_out) {
-  return guardedCall([&] {
+}  // extern "C"
+
+namespace ws {
+namespace {
+
+// Pairs (b, -1) for every build row with matched[b] == 0 (ascending), after `m` pairs of the output.
+__global__ void kUnmatchedCount(const uint8_t* matched, int64_t n, int64_t* counts) {
+  __shared__ int wsum[8];
+  const int64_t i0 = (int64_t)blockIdx.x * 1024 + threadIdx.x * 4;
+  int c = 0;
+  for (int i = 0; i < 4; ++i) c += i0 + i < n && !matched[i0 + i];
+  for (int o = 16; o; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int w = 0; w < 8; ++w) t += wsum[w];
+    counts[blockIdx.x] = t;
+  }
+}
+__global__ void kUnmatchedWrite(const uint8_t* matched, int64_t n, const int64_t* offs, int64_t m, int32_t* ob,
+                                int32_t* op) {
+  __shared__ int wsum[8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t i0 = (int64_t)blockIdx.x * 1024 + threadIdx.x * 4;
+  int c = 0;
+  for (int i = 0; i < 4; ++i) c += i0 + i < n && !matched[i0 + i];
+  int incl = c;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  int before = 0;
+  for (int w = 0; w < warp; ++w) before += wsum[w];
+  int64_t at = m + offs[blockIdx.x] + before + incl - c;
+  for (int i = 0; i < 4; ++i)
+    if (i0 + i < n && !matched[i0 + i]) ob[at] = (int32_t)(i0 + i), op[at] = -1, ++at;
+}
+// Every probe row of [base, base + n) paired with build row -1 (outer join, no build key at all).
+__global__ void kAllUnmatched(int64_t base, int64_t n, int32_t* ob, int32_t* op, unsigned long long* counter) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x)
+    ob[j] = -1, op[j] = (int32_t)(base + j);
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(counter, (unsigned long long)n);
+}
+__global__ void kCross(int64_t na, int64_t nb, int32_t* oa, int32_t* ob) {
+  const int64_t n = na * nb;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    oa[i] = (int32_t)(i / nb);
+    ob[i] = (int32_t)(i % nb);
+  }
+}
+
+}  // namespace
+
+// Inner (outer = 0) or outer equi join over build / probe partitions; see ws_hash_join_parts and
+// ws_hash_join_outer.  full: also the build rows that matched nothing, paired with probe row -1.
+static void joinImpl(ws_col_view build_key, const int64_t* boff, int pb, ws_col_view probe_key, const int64_t* poff,
+                     int pp, int outer, bool full, int32_t** out_build, int32_t** out_probe, int64_t* out_off,
+                     int64_t* m_out) {
+  {
     *out_build = *out_probe = nullptr;
-    const int pb = nbparts, pp = npparts;
     if (pb < 1 || pp < 1 || (pb != 1 && pb != pp)) throw Error("internal: partition count mismatch in join", WS_ERR_INTERNAL);
     const int64_t nb = boff[pb], np = poff[pp];
     if (out_off)
       for (int p = 0; p <= pp; ++p) out_off[p] = 0;
     *m_out = 0;
     if (nb == 0 || np == 0) {
-      *out_build = (int32_t*)tmpAlloc(4);
-      *out_probe = (int32_t*)tmpAlloc(4);
+      // inner: nothing; outer: every probe row unmatched; full: every build row too
+      const int64_t m = outer ? np + (full ? nb : 0) : 0;
+      if (m > INT32_MAX) throw Error("join result too large (>2^31 rows)", WS_ERR_INTERNAL);
+      DBuf<int32_t> ob(std::max<int64_t>(m, 1)), op(std::max<int64_t>(m, 1));
+      DBuf<unsigned long long> ctr(1);
+      if (outer && np) WS_LAUNCH(kAllUnmatched, gridFor(np), 256, 0, (int64_t)0, np, ob.p, op.p, ctr.p);
+      if (outer && full && nb) WS_LAUNCH(kAllUnmatched, gridFor(nb), 256, 0, (int64_t)0, nb, op.p + np, ob.p + np, ctr.p);
+      if (out_off)
+        for (int p = 0; p <= pp; ++p) out_off[p] = outer ? poff[p] : 0;
+      *out_build = ob.release();
+      *out_probe = op.release();
+      *m_out = m;
       return;
     }
+    DBuf<uint8_t> matchedBuf(full ? nb : 1);
+    uint8_t* matched = full ? matchedBuf.p : nullptr;
+    if (full) WS_CK(cudaMemsetAsync(matched, 0, nb, stream()));
     // Hash passes per build partition (2^bits) from its row count and the table budget.
     std::vector<int> bits(pb, 0);
     for (int q = 0; q < pb; ++q) {
@@ -638,6 +730,14 @@ int ws_hash_join_parts(ws_col_view build_key, const int64_t* boff, int nbparts, 
       for (int q = 0; q < pb; ++q) {
         const int64_t nbq = boff[q + 1] - boff[q];
         const int npass = dense[q] ? 1 : (int)cap[q].size();  // 0: no non-NULL build key
+        if (npass == 0 && outer)
+          for (int p = 0; p < pp; ++p) {
+            if (pb != 1 && p != q) continue;
+            const int64_t n = poff[p + 1] - poff[p];
+            if (n && n <= capOut[p])
+              WS_LAUNCH(kAllUnmatched, gridFor(n), 256, 0, poff[p], n, ob.p + outStart[p], op.p + outStart[p],
+                        counters.p + p);
+          }
         for (int pass = 0; pass < npass; ++pass) {
           const JPass jp{bits[q], pass};
           const int64_t c = dense[q] ? 0 : cap[q][pass];
@@ -654,7 +754,7 @@ int ws_hash_join_parts(ws_col_view build_key, const int64_t* boff, int nbparts, 
             if (pb != 1 && p != q) continue;
             const int64_t n = poff[p + 1] - poff[p];
             if (!n) continue;
-            const JOut jo{ob.p, op.p, outStart[p], capOut[p], counters.p + p};
+            const JOut jo{ob.p, op.p, outStart[p], capOut[p], counters.p + p, outer, matched, boff[q]};
             const int grid = gridFor((n + kJPer - 1) / kJPer, kJThreads);
             if (dense[q])
               WS_LAUNCH(kJoinDenseProbe, grid, kJThreads, 0, probe_key, poff[p], n, dtable.p, kmin[q], range[q], next.p,
@@ -676,6 +776,25 @@ int ws_hash_join_parts(ws_col_view build_key, const int64_t* boff, int nbparts, 
         m += (int64_t)cnt[p];
       }
       if (m > INT32_MAX) throw Error("join result too large (>2^31 rows)", WS_ERR_INTERNAL);
+      if (fits && full) {  // single partition: append the build rows that matched nothing
+        const int64_t nchunks = (nb + 1023) / 1024;
+        DBuf<int64_t> counts(nchunks + 1);
+        WS_LAUNCH(kUnmatchedCount, (unsigned)nchunks, 256, 0, matched, nb, counts.p);
+        WS_LAUNCH(kScanTiles, 1, 1024, 0, counts.p, nchunks);
+        int64_t extra = 0;
+        d2hSync(&extra, counts.p + nchunks, 8);
+        if (m + extra > INT32_MAX) throw Error("join result too large (>2^31 rows)", WS_ERR_INTERNAL);
+        DBuf<int32_t> cb(std::max<int64_t>(m + extra, 1)), cp(std::max<int64_t>(m + extra, 1));
+        if (m) {
+          WS_CK(cudaMemcpyAsync(cb.p, ob.p, 4 * m, cudaMemcpyDeviceToDevice, stream()));
+          WS_CK(cudaMemcpyAsync(cp.p, op.p, 4 * m, cudaMemcpyDeviceToDevice, stream()));
+        }
+        if (extra) WS_LAUNCH(kUnmatchedWrite, (unsigned)nchunks, 256, 0, matched, nb, counts.p, m, cb.p, cp.p);
+        *out_build = cb.release();
+        *out_probe = cp.release();
+        *m_out = m + extra;
+        return;
+      }
       if (fits) {
         // make the partitions' pairs contiguous
         std::vector<int64_t> dst(pp + 1, 0);
@@ -704,6 +823,18 @@ int ws_hash_join_parts(ws_col_view build_key, const int64_t* boff, int nbparts, 
       }
     }
     throw Error("internal: join output sizing failed", WS_ERR_INTERNAL);
+  }
+}
+
+}  // namespace ws
+
+extern "C" {
+
+int ws_hash_join_parts(ws_col_view build_key, const int64_t* boff, int nbparts, ws_col_view probe_key,
+                       const int64_t* poff, int npparts, int32_t** out_build, int32_t** out_probe, int64_t* out_off,
+                       int64_t* m_out) {
+  return guardedCall([&] {
+    joinImpl(build_key, boff, nbparts, probe_key, poff, npparts, 0, false, out_build, out_probe, out_off, m_out);
   });
 }
 
@@ -711,6 +842,29 @@ int ws_hash_join(ws_col_view build_key, int64_t nb, ws_col_view probe_key, int64
                  int32_t** out_probe, int64_t* m) {
   const int64_t bo[2] = {0, nb}, po[2] = {0, np};
   return ws_hash_join_parts(build_key, bo, 1, probe_key, po, 1, out_build, out_probe, nullptr, m);
+}
+
+int ws_hash_join_outer(ws_col_view build_key, int64_t nb, ws_col_view probe_key, int64_t np, int full,
+                       int32_t** out_build, int32_t** out_probe, int64_t* m) {
+  return guardedCall([&] {
+    const int64_t bo[2] = {0, nb}, po[2] = {0, np};
+    joinImpl(build_key, bo, 1, probe_key, po, 1, 1, full != 0, out_build, out_probe, nullptr, m);
+  });
+}
+
+int ws_cross_join(int64_t na, int64_t nb, int32_t** out_a, int32_t** out_b, int64_t* m) {
+  return guardedCall([&] {
+    *out_a = *out_b = nullptr;
+    const int64_t n = na * nb;
+    if (na < 0 || nb < 0) throw Error("negative row count", WS_ERR_ARG);
+    if (n > 200000000)
+      throw Error("cross join too large (" + std::to_string(n) + " rows); add a join condition", WS_ERR_INTERNAL);
+    DBuf<int32_t> a(std::max<int64_t>(n, 1)), b(std::max<int64_t>(n, 1));
+    if (n) WS_LAUNCH(kCross, gridFor(n), 256, 0, na, nb, a.p, b.p);
+    *out_a = a.release();
+    *out_b = b.release();
+    *m = n;
+  });
 }
 
 }  // extern "C"

@@ -277,7 +277,72 @@ def hash_join(build_key: abi.ColView, nb: int, probe_key: abi.ColView, np_: int)
     return hash_join_parts(build_key, [0, nb], probe_key, [0, np_])[:3]
 
 
-__all__ = ["DeviceBuffer", "GpuAggregator", "WsError", "agg_nokeys_noalloc", "device_to_array", "gather", "gather_multi", "gpu_init",
-           "hash_join", "hash_join_parts", "jit_get", "jit_info", "jit_set_cache_dir", "jit_set_default_mode",
-           "jit_set_mode", "kernel_launches", "select_multi", "sync", "tmp_free", "codegen_source",
-           "codegen_compile_check"]
+def hash_join_outer(build_key: abi.ColView, nb: int, probe_key: abi.ColView, np_: int, full: bool = False):
+    """(build idx ptr, probe idx ptr, m): unmatched probe rows pair with -1; `full` appends the build
+    rows that matched nothing (probe -1).  Free the pointers with tmp_free."""
+    b, p, m = P(), P(), C.c_int64()
+    check(lib().ws_hash_join_outer(build_key, nb, probe_key, np_, int(full), C.byref(b), C.byref(p), C.byref(m)))
+    return b.value, p.value, m.value
+
+
+def cross_join(na: int, nb: int):
+    a, b, m = P(), P(), C.c_int64()
+    check(lib().ws_cross_join(na, nb, C.byref(a), C.byref(b), C.byref(m)))
+    return a.value, b.value, m.value
+
+
+def key_bitmap(key: abi.ColView, n: int, lo: int, nbits: int, bits_ptr: int):
+    check(lib().ws_key_bitmap(key, n, lo, nbits, bits_ptr))
+
+
+def set_bits(bits_ptr: int, idx_ptr: int, m: int):
+    check(lib().ws_set_bits(bits_ptr, idx_ptr, m))
+
+
+def remap_codes(in_ptr: int, n: int, map_ptr: int, map_n: int, out_ptr: int):
+    check(lib().ws_remap_codes(in_ptr, n, map_ptr, map_n, out_ptr))
+
+
+def bits_to_double(src_ptr: int, n: int, dst_ptr: int):
+    check(lib().ws_bits_to_double(src_ptr, n, dst_ptr))
+
+
+def gather_null(src_ptr: int, ptype: int, idx_ptr: int, m: int, dst_ptr: int):
+    check(lib().ws_gather_null(src_ptr, ptype, idx_ptr, m, dst_ptr))
+
+
+def gather_bytes(src_ptr: int, esize: int, idx_ptr: int, m: int, dst_ptr: int, nulls: bool = True):
+    check(lib().ws_gather_bytes(src_ptr, esize, idx_ptr, m, dst_ptr, int(nulls)))
+
+
+def gather_enc(view: abi.ColView, ptype: int, idx_ptr: int, m: int, dst_ptr: int):
+    check(lib().ws_gather_enc(view, ptype, idx_ptr, m, dst_ptr))
+
+
+def eval_at(env: abi.ExprEnv, ncols: int, prog: abi.Prog, idx_ptr: int | None, m: int, out_ptr: int):
+    check(lib().ws_eval_at(C.byref(env), ncols, prog, idx_ptr, m, out_ptr))
+
+
+def eval_at_int(env: abi.ExprEnv, ncols: int, prog: abi.Prog, idx_ptr: int | None, m: int, out_ptr: int):
+    check(lib().ws_eval_at_int(C.byref(env), ncols, prog, idx_ptr, m, out_ptr))
+
+
+def sort_perm(key_ptrs: list, desc: list, m: int) -> int:
+    """Device pointer to the stable sort permutation (m int32) of rows by the double key columns
+    (first = most significant); free with tmp_free."""
+    kp = (P * max(len(key_ptrs), 1))(*key_ptrs)
+    dp = (C.c_int * max(len(desc), 1))(*[int(d) for d in desc])
+    out = P()
+    check(lib().ws_sort_perm(kp, dp, len(key_ptrs), m, C.byref(out)))
+    return out.value
+
+
+def map_rank(keys_ptr: int, rank_ptr: int, m: int):
+    check(lib().ws_map_rank(keys_ptr, rank_ptr, m))
+
+
+__all__ = ["DeviceBuffer", "GpuAggregator", "WsError", "agg_nokeys_noalloc", "bits_to_double", "codegen_compile_check",
+           "codegen_source", "cross_join", "device_to_array", "eval_at", "eval_at_int", "gather", "gather_bytes",
+           "gather_enc", "gather_multi", "gather_null", "gpu_init", "hash_join", "hash_join_outer", "hash_join_parts",
+           "jit_get", "jit_info", "jit_set_cache_dir", "jit_set_default_mode", "jit_set_mode", "kernel_launches",
+           "key_bitmap", "map_rank", "remap_codes", "select_multi", "set_bits", "sort_perm", "sync", "tmp_free"]
