@@ -157,6 +157,14 @@ int ws_eval_at(const ws_expr_env* env, int ncols, ws_prog prog, const int32_t* i
  * integer programs exactly (checked arithmetic), other programs rounded from their double value. */
 int ws_eval_at_int(const ws_expr_env* env, int ncols, ws_prog prog, const int32_t* idx, int64_t m, int64_t* out);
 
+/* ---- segment encoding (the flush path, src/storage.cu:1138-1192) */
+/* Encodes an integer column of n rows (t: WS_T_I32 / I64 / I32N / I64N; device memory) as one
+ * segment column in a format the scan kernels decode: enc WS_ENC_BITPACK (7), WS_ENC_RLE (8), or 0 to
+ * choose the smaller of the two.  *out (ws_tmp_free) receives *bytes bytes; *enc_used the format.
+ * Bit-packing a range wider than 32 bits is WS_ERR_RANGE.  No counterpart in the reference, whose
+ * encoder runs on the host and writes the formats 1-6. */
+int ws_encode_column(const void* src, int t, int64_t n, int enc, void** out, int64_t* bytes, int* enc_used);
+
 /* ---- ORDER BY (src/gpu.h:197-199) */
 /* gpuSortPerm: stable permutation sorting rows 0..m-1 by keys[0] (most significant) .. keys[nkeys-1],
  * each ascending or descending (desc[k] != 0); NULL (NaN) sorts as -inf (first ascending, last

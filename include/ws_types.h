@@ -94,7 +94,8 @@ typedef struct ws_instr {
  *    6 DECIMAL (int64 scaled by 10^scale).
  * enc: 0 raw; 1/2/3 uint8/uint16/uint32 offsets from the int64 base in the header (all-ones code =
  *    NULL); 4 F64 dictionary (256 doubles after the header, then uint8 codes); 5/6 decimal-valued
- *    F64 as uint16/uint32 offsets from the base, divided by the header's double 10^s.
+ *    F64 as uint16/uint32 offsets from the base, divided by the header's double 10^s (the engine's
+ *    formats); 7 bit-packed and 8 run-length integer columns (this library's formats, ws_dev.cuh).
  * off: first row of a range scan (encoded columns; raw pointers are offset by the caller). */
 typedef struct ws_col_view {
   const void* p;
@@ -161,6 +162,10 @@ typedef struct ws_dense_spec {
 
 /* physical column types of gathers (src/common.h:24) */
 enum ws_ptype { WS_PT_I32 = 0, WS_PT_I64 = 1, WS_PT_F64 = 2, WS_PT_VEC = 5 };
+/* ws_col_view.t values */
+enum ws_view_type { WS_T_I32 = 0, WS_T_I64 = 1, WS_T_F64 = 2, WS_T_I32N = 3, WS_T_I64N = 4, WS_T_VEC = 5, WS_T_DEC = 6 };
+/* ws_col_view.enc values of this library's integer formats */
+enum ws_enc { WS_ENC_BITPACK = 7, WS_ENC_RLE = 8 };
 
 /* operator kinds a plan is compiled for (src/jit.h:14) */
 enum ws_jit_fn { WS_JF_NOKEYS = 0, WS_JF_GROUPED = 1, WS_JF_DENSE = 2, WS_JF_FLAG = 3, WS_JF_FLAGM = 4 };

@@ -47,6 +47,30 @@ inline bool truthy(double v) { return v == v && v != 0; }
 // ---------------------------------------------------------------- column decoding
 // src/devtypes.h:91-158 (encIntB, encDbl, colInt, colDbl) and :217-245 (loadCol).
 int64_t colInt(const ws_col_view& c, int64_t r) {
+  if (c.enc == 7) {  // bit-packed: [int64 base][int32 bits][int32 0], codes LSB-first in 32-bit words
+    const unsigned char* p = (const unsigned char*)c.p;
+    int64_t base;
+    int32_t b;
+    memcpy(&base, p, 8);
+    memcpy(&b, p + 8, 4);
+    const uint64_t bit = (uint64_t)(r + c.off) * (uint64_t)b;
+    uint64_t two = 0;
+    memcpy(&two, p + WS_ENC_HEADER + (bit >> 5) * 4, 8);
+    const uint64_t mask = b == 32 ? 0xffffffffull : ((1ull << b) - 1);
+    const uint64_t code = (two >> (bit & 31)) & mask;
+    const int64_t nul = (c.t == 0 || c.t == 3) ? (int64_t)WS_NULL_I32 : WS_NULL_I64;
+    return code == mask ? nul : base + (int64_t)code;
+  }
+  if (c.enc == 8) {  // run-length: [int64 runs][int64 0], int32 ends[runs] (padded to 8 B), int64 vals[runs]
+    const unsigned char* p = (const unsigned char*)c.p;
+    int64_t runs;
+    memcpy(&runs, p, 8);
+    const int32_t* ends = (const int32_t*)(p + WS_ENC_HEADER);
+    const int64_t* vals = (const int64_t*)(p + WS_ENC_HEADER + ((runs * 4 + 7) & ~7ll));
+    const int64_t i = r + c.off;
+    const int64_t k = std::upper_bound(ends, ends + runs, (int32_t)i) - ends;
+    return k < runs ? vals[k] : ((c.t == 0 || c.t == 3) ? (int64_t)WS_NULL_I32 : WS_NULL_I64);
+  }
   if (c.enc) {
     const unsigned char* d = (const unsigned char*)c.p + WS_ENC_HEADER;
     const int64_t i = r + c.off;

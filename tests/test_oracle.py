@@ -101,3 +101,29 @@ def test_dates_match_python(built):
         assert oracle.eval_row(e.env, views, py, r)[1] == date.year
         for k, f in fns.items():
             assert oracle.eval_row(e.env, views, progs[k], r)[0] == f(date), (k, date)
+
+
+@pytest.mark.parametrize("enc", [7, 8], ids=["bitpack", "rle"])
+def test_bitpack_and_rle_segments_decode(enc):
+    """The library's integer segment formats (enc 7 bit-packed, enc 8 run-length): every stored row
+    decodes to its value, NULLs included, across several segments."""
+    rng = np.random.default_rng(enc)
+    n = 50_003
+    a = rng.integers(-10**6, 10**6, n).astype(np.int64)
+    a[rng.random(n) < 0.1] = abi.NULL_I64
+    r = np.repeat(rng.integers(0, 100, n // 40 + 1), 40)[:n].astype(np.int32)
+    r[rng.random(n) < 0.01] = abi.NULL_I32
+    t = W.Table(n, seg_rows=1 << 13)
+    t.add("a", abi.T_I64N, a, enc=enc)
+    t.add("r", abi.T_I32N, r, enc=enc)
+    e = W.env_for(t)
+    progs = [e.compile(q.col(0)), e.compile(q.col(1))]
+    for s in range(t.nseg):
+        vs = t.views(s, False)
+        lo = s * t.seg_rows
+        for row in rng.integers(0, t.seg_len(s), 40):
+            for c, src, nul in ((0, a, abi.NULL_I64), (1, r, abi.NULL_I32)):
+                d, _, _, _ = oracle.eval_row(e.env, vs, progs[c], int(row))
+                want = src[lo + row]
+                assert (d != d) == (want == nul)
+                assert d != d or d == float(want)

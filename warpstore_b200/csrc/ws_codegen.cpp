@@ -269,7 +269,7 @@ std::string genEvaluator(const ws_expr_env& env, int ncols, const ws_agg_plan& p
   o << "    const ws_col_view* cv = l.cols + (ws::i64)b * l.ncols;\n    st.bytes = 0; st.ok = 1;\n";
   for (size_t j = 0; j < staged.size(); ++j)
     o << "    { const ws::ColRef v = ws::resolveCol(cv[" << staged[j] << "]); st.d[" << j << "] = v.d; st.w[" << j
-      << "] = v.width; st.bytes += ws::kTile * v.width; st.ok &= (((unsigned long long)v.d & 15) == 0); }\n";
+      << "] = v.width; st.bytes += ws::kTile * v.width; st.ok &= (((unsigned long long)v.d & 15) == 0) && v.width > 0; }\n";
   o << "  }\n";
   o << "  __device__ static void stageIssue(const Stage& st, ws::i64 tr0, unsigned dst, unsigned bar) {\n";
   for (size_t j = 0; j < staged.size(); ++j)
@@ -279,6 +279,7 @@ std::string genEvaluator(const ws_expr_env& env, int ncols, const ws_agg_plan& p
   // ofl: overflow of this thread's checked integer arithmetic (rows that passed or were filtered),
   // stored to the plan's flag once by finish()
   o << "  const ws::Launch& L;\n  mutable unsigned ofl;\n  bool fastOk;\n  ws::i64 rb;\n";
+  o << "  const ws_col_view* cvb;  // the bound batch's views (bit-packed / run-length columns decode from them)\n";
   // plan constants are read from the launch descriptor (constant bank) where used, not kept in registers
   for (int k : g.iconsts)
     o << "  __device__ __forceinline__ ws::i64 ik" << k << "() const { return __double_as_longlong(L.env.consts[" << k << "]); }\n";
@@ -288,7 +289,7 @@ std::string genEvaluator(const ws_expr_env& env, int ncols, const ws_agg_plan& p
     o << "  ws::ColRef v" << c << ";\n";
     if (!u.vec) o << "  " << valType(u) << " c" << c << "[4];\n";
   }
-  o << "  __device__ QEv(const ws::Launch& l) : L(l), ofl(0), fastOk(false), rb(0) {}\n";
+  o << "  __device__ QEv(const ws::Launch& l) : L(l), ofl(0), fastOk(false), rb(0), cvb(nullptr) {}\n";
   o << "  __device__ __forceinline__ int nk() const { return " << nk << "; }\n";
   o << "  __device__ __forceinline__ int na() const { return " << na << "; }\n";
   o << "  __device__ __forceinline__ int rowWords() const { return " << (agg ? lay.rw : 1) << "; }\n";
@@ -310,7 +311,7 @@ std::string genEvaluator(const ws_expr_env& env, int ncols, const ws_agg_plan& p
   o << " } return false; }\n";
   // batch binding: resolve the views of the columns used, check vector-load alignment
   o << "  __device__ __forceinline__ void bind(const ws::Launch& l, int b) {\n";
-  o << "    const ws_col_view* cv = l.cols + (ws::i64)b * l.ncols;\n";
+  o << "    const ws_col_view* cv = l.cols + (ws::i64)b * l.ncols;\n    cvb = cv;\n";
   std::string fast = "true";
   for (auto& [c, u] : g.cols) {
     o << "    v" << c << " = ws::resolveCol(cv[" << c << "]);\n";
@@ -330,14 +331,18 @@ std::string genEvaluator(const ws_expr_env& env, int ncols, const ws_agg_plan& p
         o << "      ws::load4f64(" << a << ",(const double*)" << v << ".d + r0" << F << ";\n";
       } else if (u.t == 0 || u.t == 3) {
         if (u.enc)
-          o << "      if (" << v << ".enc) { ws::i64 t_[4]; ws::load4enc(t_," << v << ".d + r0 * " << v << ".width," << v
+          o << "      if (" << v << ".enc >= 7) { ws::i64 u_[4]; ws::load4encView(u_,cvb + " << C
+            << ",r0,(ws::i64)WS_NULL_I32,nv); for (int j = 0; j < 4; ++j) " << a << "[j] = (int)u_[j]; } else if ("
+            << v << ".enc) { ws::i64 t_[4]; ws::load4enc(t_," << v << ".d + r0 * " << v << ".width," << v
             << ".enc," << v << ".base,(ws::i64)WS_NULL_I32" << F << "; for (int j = 0; j < 4; ++j) " << a
             << "[j] = (int)t_[j]; } else ";
         o << "      ws::load4i32(" << a << ",(const int*)" << v << ".d + r0" << F << ";\n";
       } else {
         if (u.enc)
-          o << "      if (" << v << ".enc) ws::load4enc(" << a << "," << v << ".d + r0 * " << v << ".width," << v << ".enc," << v
-            << ".base,(ws::i64)WS_NULL_I64" << F << "; else ";
+          o << "      if (" << v << ".enc >= 7) { ws::i64 u_[4]; ws::load4encView(u_,cvb + " << C
+            << ",r0,(ws::i64)WS_NULL_I64,nv); for (int j = 0; j < 4; ++j) " << a << "[j] = u_[j]; }"
+            << " else if (" << v << ".enc) ws::load4enc(" << a << "," << v << ".d + r0 * " << v << ".width," << v << ".enc,"
+            << v << ".base,(ws::i64)WS_NULL_I64" << F << "; else ";
         o << "      ws::load4i64(" << a << ",(const ws::i64*)" << v << ".d + r0" << F << ";\n";
       }
     }

@@ -477,6 +477,66 @@ WS_DI void bulkG2S(unsigned dst, const void* src, unsigned bytes, unsigned bar) 
                : "memory");
 }
 
+// ---- bit-packed (enc 7) and run-length (enc 8) integer segments (formats of this library; the
+// engine's own FOR / dictionary / decimal encodings are enc 1-6).
+//   enc 7: header [int64 base][int32 bits b (1..32)][int32 0], then the codes packed LSB-first in
+//          little-endian 32-bit words (code of stored row i = bits [i*b, i*b + b)), then 16 pad bytes;
+//          value = base + code, the all-ones code is NULL.
+//   enc 8: header [int64 runs][int64 0], then int32 ends[runs] (exclusive end row of each run,
+//          ascending; padded to 8 bytes), then int64 vals[runs] (the stored value, NULL sentinels
+//          included).
+// Row r of a view with range-scan offset `off` is stored row r + off.  Decoded out of line (the
+// reference decodes its encoded columns out of line too) so the inline FOR loads stay small.
+WS_DI unsigned bitpackCode(const unsigned* w, i64 i, int b) {
+  const u64 bit = (u64)i * (unsigned)b;
+  const u64 word = bit >> 5;
+  const unsigned sh = (unsigned)(bit & 31);
+  const u64 two = (u64)__ldg(w + word) | ((u64)__ldg(w + word + 1) << 32);
+  return (unsigned)(two >> sh) & (b == 32 ? 0xffffffffu : ((1u << b) - 1u));
+}
+WS_DI i64 rleRun(const int* ends, i64 runs, i64 i) {  // first run whose end is above stored row i
+  i64 lo = 0, hi = runs;
+  while (lo < hi) {
+    const i64 mid = (lo + hi) >> 1;
+    if ((i64)__ldg(ends + mid) <= i) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+// Rows r0 .. r0+nv-1 of an enc 7 / enc 8 integer view.
+static __device__ __noinline__ void load4encView(i64* o, const ws_col_view* vp, i64 r0, i64 nul, int nv) {
+  const ws_col_view v = *vp;
+  const unsigned char* p = (const unsigned char*)v.p;
+  const i64 i0 = r0 + v.off;
+  if (v.enc == 7) {
+    const i64 base = *(const i64*)p;
+    const int b = *(const int*)(p + 8);
+    const unsigned* w = (const unsigned*)(p + WS_ENC_HEADER);
+    const unsigned nulc = b == 32 ? 0xffffffffu : ((1u << b) - 1u);
+    for (int k = 0; k < 4; ++k) {
+      if (k >= nv) {
+        o[k] = 0;
+        continue;
+      }
+      const unsigned c = bitpackCode(w, i0 + k, b);
+      o[k] = c == nulc ? nul : base + (i64)c;
+    }
+    return;
+  }
+  const i64 runs = *(const i64*)p;
+  const int* ends = (const int*)(p + WS_ENC_HEADER);
+  const i64* vals = (const i64*)(p + WS_ENC_HEADER + ((runs * 4 + 7) & ~7ll));
+  i64 run = rleRun(ends, runs, i0);
+  for (int k = 0; k < 4; ++k) {
+    if (k >= nv) {
+      o[k] = 0;
+      continue;
+    }
+    while (run < runs && (i64)__ldg(ends + run) <= i0 + k) ++run;
+    o[k] = run < runs ? __ldg(vals + run) : nul;
+  }
+}
+
 // Resolved view of one column of the current batch: where row 0's data starts and how it is encoded.
 struct ColRef {
   const unsigned char* d;  // data of row 0 (raw: the view pointer; encoded: header skipped + off applied)
@@ -498,7 +558,7 @@ WS_DI ColRef resolveCol(const ws_col_view& v) {
     c.width = (v.t == 0 || v.t == 3) ? 4 : 8;
     return c;
   }
-  c.width = (v.enc == 1 || v.enc == 4) ? 1 : (v.enc == 2 || v.enc == 5) ? 2 : 4;
+  c.width = (v.enc == 1 || v.enc == 4) ? 1 : (v.enc == 2 || v.enc == 5) ? 2 : v.enc >= 7 ? 0 : 4;  // 7 / 8: packed
   c.base = p ? *(const i64*)p : 0;
   c.p10 = p ? *(const double*)(p + 8) : 1.0;
   c.dict = (const double*)(p + WS_ENC_HEADER);
@@ -506,6 +566,7 @@ WS_DI ColRef resolveCol(const ws_col_view& v) {
   return c;
 }
 WS_DI bool aligned4(const ColRef& c) {
+  if (c.width == 0) return true;  // enc 7 / 8 decode element-wise
   const unsigned a = c.width * 4 < 16 ? c.width * 4 : 16;
   return ((unsigned long long)c.d & (a - 1)) == 0;
 }

@@ -11,8 +11,13 @@ namespace ws {
 WS_DI i64 colIntAt(const ws_col_view& v, i64 r) {
   const bool i32 = v.t == 0 || v.t == 3;
   if (!v.enc) return i32 ? (i64)__ldg((const int*)v.p + r) : __ldg((const i64*)v.p + r);
-  const ColRef c = resolveCol(v);
   const i64 nul = i32 ? (i64)WS_NULL_I32 : (i64)WS_NULL_I64;
+  if (v.enc >= 7) {
+    i64 o[4];
+    load4encView(o, &v, r, nul, 1);
+    return o[0];
+  }
+  const ColRef c = resolveCol(v);
   unsigned code;
   if (c.enc == 1) {
     code = __ldg(c.d + r);

@@ -337,12 +337,20 @@ def sort_perm(key_ptrs: list, desc: list, m: int) -> int:
     return out.value
 
 
+def encode_column(src_ptr: int, t: int, n: int, enc: int = 0):
+    """(device ptr, bytes, enc used) of an integer column encoded as one segment column (enc 7
+    bit-packed, 8 run-length, 0 the smaller); free the pointer with tmp_free."""
+    out, nb, used = P(), C.c_int64(), C.c_int()
+    check(lib().ws_encode_column(src_ptr, t, n, enc, C.byref(out), C.byref(nb), C.byref(used)))
+    return out.value, nb.value, used.value
+
+
 def map_rank(keys_ptr: int, rank_ptr: int, m: int):
     check(lib().ws_map_rank(keys_ptr, rank_ptr, m))
 
 
 __all__ = ["DeviceBuffer", "GpuAggregator", "WsError", "agg_nokeys_noalloc", "bits_to_double", "codegen_compile_check",
-           "codegen_source", "cross_join", "device_to_array", "eval_at", "eval_at_int", "gather", "gather_bytes",
+           "codegen_source", "cross_join", "device_to_array", "encode_column", "eval_at", "eval_at_int", "gather", "gather_bytes",
            "gather_enc", "gather_multi", "gather_null", "gpu_init", "hash_join", "hash_join_outer", "hash_join_parts",
            "jit_get", "jit_info", "jit_set_cache_dir", "jit_set_default_mode", "jit_set_mode", "kernel_launches",
            "key_bitmap", "map_rank", "remap_codes", "select_multi", "set_bits", "sort_perm", "sync", "tmp_free"]

@@ -46,12 +46,56 @@ def encode_for(x: np.ndarray, width: int, null=None) -> tuple[np.ndarray, int]:
     return out, base
 
 
+def encode_bitpack(x: np.ndarray, null=None) -> np.ndarray:
+    """Bit-packed segment column (enc 7): header [int64 base][int32 bits][int32 0], codes x - base in
+    `bits` bits each, LSB-first in little-endian 32-bit words, the all-ones code for NULL, 16 pad bytes."""
+    x = x.astype(np.int64)
+    isnull = (x == null) if null is not None else np.zeros(x.size, bool)
+    valid = x[~isnull]
+    base = int(valid.min()) if valid.size else 0
+    rng = (int(valid.max()) - base) if valid.size else 0
+    b = 1
+    while (rng + 1) >> b:
+        b += 1
+    if b > 32:
+        raise ValueError("range too wide to bit-pack")
+    mask = (1 << b) - 1
+    codes = np.where(isnull, mask, x - base).astype(np.uint64)
+    nwords = (x.size * b + 31) // 32
+    words = np.zeros(nwords + 4, dtype=np.uint64)
+    start = np.arange(x.size, dtype=np.uint64) * np.uint64(b)
+    w, sh = (start >> np.uint64(5)).astype(np.int64), start & np.uint64(31)
+    np.bitwise_or.at(words, w, (codes << sh) & np.uint64(0xFFFFFFFF))
+    spill = (sh + np.uint64(b)) > np.uint64(32)
+    np.bitwise_or.at(words, w[spill] + 1, codes[spill] >> (np.uint64(32) - sh[spill]))
+    out = np.zeros(16 + 4 * nwords + 16, dtype=np.uint8)
+    out[:8] = np.frombuffer(np.int64(base).tobytes(), np.uint8)
+    out[8:12] = np.frombuffer(np.int32(b).tobytes(), np.uint8)
+    out[16:16 + 4 * nwords] = np.frombuffer(words[:nwords].astype(np.uint32).tobytes(), np.uint8)
+    return out
+
+
+def encode_rle(x: np.ndarray) -> np.ndarray:
+    """Run-length segment column (enc 8): header [int64 runs][int64 0], int32 exclusive run ends
+    (padded to 8 bytes), int64 run values (NULL sentinels included), 16 pad bytes."""
+    x = x.astype(np.int64)
+    starts = np.flatnonzero(np.concatenate([[True], x[1:] != x[:-1]])) if x.size else np.zeros(0, np.int64)
+    runs = starts.size
+    ends = np.concatenate([starts[1:], [x.size]]).astype(np.int32) if runs else np.zeros(0, np.int32)
+    eb = (runs * 4 + 7) & ~7
+    out = np.zeros(16 + eb + 8 * runs + 16, dtype=np.uint8)
+    out[:8] = np.frombuffer(np.int64(runs).tobytes(), np.uint8)
+    out[16:16 + 4 * runs] = np.frombuffer(ends.tobytes(), np.uint8)
+    out[16 + eb:16 + eb + 8 * runs] = np.frombuffer(x[starts].tobytes(), np.uint8)
+    return out
+
+
 @dataclass
 class Column:
     name: str
     t: int                 # view type (abi.T_*)
     data: np.ndarray       # host values (full table)
-    enc: int = 0           # 0 raw, 1/2/3 encoded (uint8/16/32)
+    enc: int = 0           # 0 raw, 1/2/3 encoded (uint8/16/32), 7 bit-packed, 8 run-length
     scale: int = 0
     seg_bytes: list = field(default_factory=list)   # per segment: host bytes of the stored segment column
     host: np.ndarray | None = None                   # all segments' bytes back to back (aligned)
@@ -82,7 +126,11 @@ class Table:
         off = 0
         for s in range(self.nseg):
             lo, hi = s * self.seg_rows, min(self.n, (s + 1) * self.seg_rows)
-            if enc:
+            if enc == 7:
+                b = encode_bitpack(data[lo:hi], null)
+            elif enc == 8:
+                b = encode_rle(data[lo:hi])
+            elif enc:
                 b, _ = encode_for(data[lo:hi], width, null)
             else:
                 b = np.frombuffer(np.ascontiguousarray(data[lo:hi]).tobytes(), dtype=np.uint8)
