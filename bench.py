@@ -34,6 +34,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 PEAK_FALLBACK_GBS = 6650.0
+# DRAM bytes (read + write) per row of the workload's scan kernel, from one ncu capture of a smaller
+# case of the same kernel (8,388,608 and 25,000,000 rows), scaled to a launch by its rows: the traffic
+# grows in proportion to the rows scanned
+NCU_DRAM_BYTES_PER_ROW = {"pricing_summary_60m": 38.52, "high_cardinality_100m": 22.94}
 
 
 def measured_peak():
@@ -149,7 +153,16 @@ def make_workload(name: str, rank: int, rows: int | None = None):
         return t, e, aq, ds, W.PRICING_BYTES_PER_ROW, 1024, {
             "workload": "pricing_summary_60m", "rows": t.n, "segments": t.nseg, "segment_rows": t.seg_rows,
             "columns": "ship_date i32, quantity/price/discount/tax i64, flag1/flag2 u8-encoded",
-            "groups": 6, "aggregation": "dense", "l2": "inputs 2.28 GB >> 126 MB L2 (no flush needed)"}
+            "groups": 6, "aggregation": "dense",
+            "l2": f"inputs {t.n * W.PRICING_BYTES_PER_ROW / 1e9:.2f} GB > 126 MB L2 (no flush needed)"}
+    if name == "high_cardinality_100m":
+        n = rows or W.HC_ROWS
+        t = W.high_cardinality(n, W.HC_RANKS if n == W.HC_ROWS else max(n // 10, 1000), W.HC_DICT, seed=4 + rank)
+        e, aq, _ = W.high_cardinality_query(t, W.high_cardinality_cut(4 + rank))
+        return t, e, aq, None, W.HC_BYTES_PER_ROW, W.plain_capacity(aq.plan, t.n), {
+            "workload": "high_cardinality_100m", "rows": t.n, "segments": t.nseg, "segment_rows": t.seg_rows,
+            "columns": "key i64 (Zipf s=1.1 over 10M ranks, mixed), payload i64, s i32",
+            "aggregation": "hash", "l2": f"inputs {t.n * 20 / 1e9:.2f} GB > 126 MB L2 (no flush needed)"}
     if name == "filter_groupby_1m":
         t = W.filter_groupby_1m(1 << 20, seed=0 + rank)
         e, aq = W.filter_groupby_1m_query(t)
@@ -271,6 +284,9 @@ def run_ours(args, ws, rank, local):
 
     peak, peak_kind = measured_peak()
     algo_bytes = bpr * table.n
+    traffic = args.traffic
+    if traffic is None and cfg["workload"] in NCU_DRAM_BYTES_PER_ROW:
+        traffic = round(NCU_DRAM_BYTES_PER_ROW[cfg["workload"]] * table.n)
     achieved = algo_bytes / (kernel_ms / 1e3) / 1e9
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -284,7 +300,7 @@ def run_ours(args, ws, rank, local):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
             "data": "synthetic (seeded numpy)", "config": dict(cfg, parallelism=f"replicas{ws}"),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "traffic": args.traffic, "peak_kind": f"{peak_kind} hbm_gbs",
+                         "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": f"{peak_kind} hbm_gbs",
                          "kernel_ms": round(kernel_ms, 4), "algorithmic_bytes": algo_bytes},
             "e2e": {"value": round(e2e_value, 4), "unit": "G rows/s", "h2d_bytes_per_step": table.nbytes(),
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_ms, 3)},
@@ -334,7 +350,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="pricing_summary_60m", choices=["pricing_summary_60m", "filter_groupby_1m"])
+    ap.add_argument("--workload", default="pricing_summary_60m",
+                    choices=["pricing_summary_60m", "filter_groupby_1m", "high_cardinality_100m"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--traffic", type=float, default=None, help="ncu dram bytes per launch, when known")
