@@ -165,6 +165,22 @@ int ws_eval_at_int(const ws_expr_env* env, int ncols, ws_prog prog, const int32_
  * encoder runs on the host and writes the formats 1-6. */
 int ws_encode_column(const void* src, int t, int64_t n, int enc, void** out, int64_t* bytes, int* enc_used);
 
+/* ---- group-count estimation for hash table sizing (no counterpart in the reference, which sizes
+ * tables from dictionary sizes and segment min/max: src/engine_select.cpp:1154-1167) */
+/* HyperLogLog sketch (2^p registers, p 4..12) of the GROUP BY key(s) of the rows that pass the plan's
+ * filter, over the global rows k * stride of the batches (stride = max(1, rows / sample_rows)):
+ * register j = max over sampled hashes h = mix64(key bits) with top p bits j of (leading zeros of
+ * h << p) + 1.  regs_out: host array of 2^p words; *sampled / *passing: sampled rows (not deleted) and
+ * those that pass the filter. */
+int ws_hll_sketch(const ws_expr_env* env, int ncols, const ws_agg_plan* plan, int nb, const int64_t* bn,
+                  const uint32_t* const* bdel, const ws_col_view* bcols, int p, int64_t sample_rows, uint32_t* regs_out,
+                  int64_t* sampled, int64_t* passing);
+/* y[r] of a 3-layer MLP over host feature rows x[rows][features]: relu(x W1 + b1) -> relu(. W2 + b2) ->
+ * . W3 + b3, weights as BF16 bits (W1 [features][hidden], W2 [hidden][hidden], W3 [hidden]), biases and
+ * accumulation FP32; features <= 64, hidden a multiple of 32 up to 128. */
+int ws_mlp_infer(const float* x, int rows, int features, int hidden, const uint16_t* w1_bf16, const float* b1,
+                 const uint16_t* w2_bf16, const float* b2, const uint16_t* w3_bf16, float b3, float* y);
+
 /* ---- ORDER BY (src/gpu.h:197-199) */
 /* gpuSortPerm: stable permutation sorting rows 0..m-1 by keys[0] (most significant) .. keys[nkeys-1],
  * each ascending or descending (desc[k] != 0); NULL (NaN) sorts as -inf (first ascending, last

@@ -125,6 +125,16 @@ def test_high_cardinality_full_size_vs_reference():
                     yield
 
             dres[impl] = W.distinct_aggregate_run(t.batches(True), e2, aq2, dprog, t.n, impl, stage)
+        # learned sizing of the phase-1 table (ours): same result, fewer overflow reruns
+        W.distinct_aggregate_run(t.batches(True), e2, aq2, dprog, t.n, "ours", sizing="learned")  # warm
+
+        @contextmanager
+        def lstage(name):
+            with timed(("learned", name)):
+                yield
+
+        dres["learned"] = W.distinct_aggregate_run(t.batches(True), e2, aq2, dprog, t.n, "ours", lstage, sizing="learned")
+        assert dres["learned"][3] == dres["ours"][3]
         assert dres["ours"][3] == dres["reference"][3]
         assert_same(engine_arrays(aq2, *dres["ours"][:2], distinct=True),
                     engine_arrays(aq2, *dres["reference"][:2], distinct=True), "count distinct")
@@ -133,5 +143,8 @@ def test_high_cardinality_full_size_vs_reference():
             r, o = times[("reference", s)], times[("ours", s)]
             print(f"[timing]   {s:20s} reference {r:9.3f} ms   ours {o:9.3f} ms   ratio {r / o:.2f}x")
         print(f"[timing]   distinct pairs {dres['ours'][3]}, phase-1 runs (overflow retries) {dres['ours'][2]}")
+        print(f"[timing]   phase 1 with learned sizing: {times[('learned', 'phase 1 (keys, x)')]:9.3f} ms "
+              f"({dres['learned'][2]} run(s)), ratio to the reference "
+              f"{times[('reference', 'phase 1 (keys, x)')] / times[('learned', 'phase 1 (keys, x)')]:.2f}x")
     finally:
         t.free_device()

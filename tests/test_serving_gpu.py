@@ -1,0 +1,46 @@
+"""The request loop: every query's result in the mix (overlapping on the device with others) equals
+its result alone — integer slots exactly, DOUBLE sums within 1e-12 relative — in both serving forms;
+QPS and p50 / p99 of the two forms are printed."""
+import numpy as np
+import pytest
+
+from warpstore_b200 import abi, ops
+from warpstore_b200 import serving as S
+
+from .helpers import DOUBLE_RTOL
+
+pytestmark = pytest.mark.gpu
+
+
+def same(a_keys, a_ex, b_keys, b_ex):
+    ka, kb = np.ascontiguousarray(a_keys).view(np.int64), np.ascontiguousarray(b_keys).view(np.int64)
+    oa, ob = np.lexsort(ka.T[::-1]), np.lexsort(kb.T[::-1])
+    assert np.array_equal(ka[oa], kb[ob])
+    xa, xb = a_ex[oa], b_ex[ob]
+    ints = [0, 1, 2, 3, 4]  # COUNT, SUM(v) halves, MIN, MAX: exact
+    assert np.array_equal(xa[:, ints], xb[:, ints])
+    da, db = xa[:, 5, 0].view(np.float64), xb[:, 5, 0].view(np.float64)
+    np.testing.assert_allclose(da, db, rtol=DOUBLE_RTOL, atol=1e-300)
+
+
+def test_results_alone_equal_results_in_the_mix():
+    tables = S.make_tables(8, 10_000, 2_000_000, seed=5)
+    for t in tables:
+        t.to_device()
+    queries = S.make_queries(tables, 160, rate=2000.0, seed=6)
+    prepared, arrays = S.prepare(tables, queries)
+    ops.jit_set_mode(abi.JIT_SYNC)
+    try:
+        for mode in ("plain", "batched"):
+            st = S.run(tables, prepared, arrays, mode)
+            assert st.completed == len(queries)
+            for p in prepared:
+                keys, ex = S.run_alone(p, arrays, mode == "batched")
+                r = st.results[p.qr.qid]
+                same(keys, ex, r.keys, r.exact)
+            print(f"\n[serving] {mode}: {st.qps:.0f} QPS, p50 {st.p50_ms:.2f} ms, p99 {st.p99_ms:.2f} ms, "
+                  f"overflow reruns {st.overflow_reruns}")
+    finally:
+        ops.jit_set_mode(-1)
+        for t in tables:
+            t.free_device()

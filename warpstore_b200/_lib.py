@@ -77,6 +77,9 @@ SIGNATURES = {
     "ws_sort_perm": (C.c_int, [P, P, C.c_int, C.c_int64, C.POINTER(P)]),
     "ws_map_rank": (C.c_int, [P, P, C.c_int64]),
     "ws_encode_column": (C.c_int, [P, C.c_int, C.c_int64, C.c_int, C.POINTER(P), I64P, C.POINTER(C.c_int)]),
+    "ws_hll_sketch": (C.c_int, [C.POINTER(abi.ExprEnv), C.c_int, C.POINTER(abi.AggPlan), C.c_int, P, P, P, C.c_int,
+                                C.c_int64, P, I64P, I64P]),
+    "ws_mlp_infer": (C.c_int, [P, C.c_int, C.c_int, C.c_int, P, P, P, P, P, C.c_float, P]),
     "ws_jit_set_mode": (C.c_int, [C.c_int]),
     "ws_jit_mode": (C.c_int, []),
     "ws_jit_set_default_mode": (C.c_int, [C.c_int]),

@@ -509,11 +509,14 @@ def distinct_phase2(plan: abi.AggPlan, p1: abi.AggPlan, keys_ptr: int, accs_ptr:
     return env2, nk + 1 + na, p2
 
 
-def distinct_aggregate_run(batches: list, e, aq, dprog, rows_in: int, impl: str = "ours", timer=None):
+def distinct_aggregate_run(batches: list, e, aq, dprog, rows_in: int, impl: str = "ours", timer=None,
+                           sizing: str = "plain"):
     """GROUP BY keys with COUNT(DISTINCT x) as the engine runs it: phase 1 hash GROUP BY (keys, x)
     with capacity pow2 >= min(rows, 2^22) and the overflow retry, compaction on the device, phase 2
     GROUP BY keys over the distinct pairs (src/engine_select.cpp:1397-1492).  Returns (keys, accs in
-    the engine format with the distinct count as the last slot, phase-1 runs, distinct pairs)."""
+    the engine format with the distinct count as the last slot, phase-1 runs, distinct pairs).
+    sizing "learned" (ours only): the phase-1 table is sized from the estimator's prediction of the
+    pair count instead (estimator.py), the plain overflow retry remaining the fallback."""
     import contextlib
 
     from . import ops
@@ -528,6 +531,9 @@ def distinct_aggregate_run(batches: list, e, aq, dprog, rows_in: int, impl: str 
         try:
             jit1 = ops.jit_get(e.env, e.ncols, p1, abi.JF_GROUPED, "aggregate (distinct pairs)")
             with timer("phase 1 (keys, x)"):
+                if sizing == "learned":
+                    from . import estimator
+                    cap1 = estimator.learned_capacity(estimator.estimate_groups(e.env, e.ncols, p1, batches))
                 while True:
                     runs += 1
                     a1 = ops.GpuAggregator(p1, cap1)
