@@ -181,6 +181,49 @@ int ws_hll_sketch(const ws_expr_env* env, int ncols, const ws_agg_plan* plan, in
 int ws_mlp_infer(const float* x, int rows, int features, int hidden, const uint16_t* w1_bf16, const float* b1,
                  const uint16_t* w2_bf16, const float* b2, const uint16_t* w3_bf16, float b3, float* y);
 
+/* ---- request loop (no counterpart in the reference, whose connections each run their query
+ * synchronously): prepared GROUP BY queries served by `slots` host threads with a CUDA stream each,
+ * in arrival order, admitted while the footprints of the queries in flight fit hbm_budget. */
+typedef struct ws_serve_query {
+  /* in */
+  const ws_expr_env* env;
+  int ncols;
+  const ws_agg_plan* plan;
+  const ws_jit_program* jit;        /* compiled plan, or null (interpreter) */
+  int nb;
+  const int64_t* bn;
+  const uint32_t* const* bdel;
+  const ws_col_view* bcols;
+  int64_t cap_plain;                /* hash table capacity of the plain sizing rule */
+  double key_range;                 /* product of the keys' value ranges (0: unknown) */
+  double arrival_s;                 /* seconds from the start of ws_serve */
+  int64_t footprint;                /* device bytes the query may hold while it runs */
+  int64_t max_groups;               /* capacity of the result arrays below (0: results not kept) */
+  double* keys;                     /* [max_groups][nkeys], as ws_agg_fetch (may be null) */
+  double* accs;                     /* [max_groups][naggs] (may be null) */
+  int64_t* exact;                   /* [max_groups][naggs][2] (may be null) */
+  /* out */
+  double start_s, finish_s;         /* admitted, done (seconds from the start) */
+  int runs;                         /* aggregation runs (1 + overflow reruns) */
+  int64_t cap_used, groups;
+} ws_serve_query;
+/* Learned sizing (est may be null for the plain rule): the estimator's MLP (9 features, `hidden`
+ * units, BF16 weight bits), its input normalisation and the capacity margin (2^(p90 log2 error)). */
+typedef struct ws_estimator_weights {
+  int hidden;
+  const uint16_t* w1;
+  const float* b1;
+  const uint16_t* w2;
+  const float* b2;
+  const uint16_t* w3;
+  float b3;
+  const float* mean;
+  const float* std;
+  double margin;
+} ws_estimator_weights;
+int ws_serve(ws_serve_query* queries, int n, int slots, int64_t hbm_budget, const ws_estimator_weights* est,
+             double* wall_s);
+
 /* ---- ORDER BY (src/gpu.h:197-199) */
 /* gpuSortPerm: stable permutation sorting rows 0..m-1 by keys[0] (most significant) .. keys[nkeys-1],
  * each ascending or descending (desc[k] != 0); NULL (NaN) sorts as -inf (first ascending, last

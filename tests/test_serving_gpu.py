@@ -31,15 +31,21 @@ def test_results_alone_equal_results_in_the_mix():
     prepared, arrays = S.prepare(tables, queries)
     ops.jit_set_mode(abi.JIT_SYNC)
     try:
-        for mode in ("plain", "batched"):
-            st = S.run(tables, prepared, arrays, mode)
-            assert st.completed == len(queries)
-            for p in prepared:
-                keys, ex = S.run_alone(p, arrays, mode == "batched")
-                r = st.results[p.qr.qid]
-                same(keys, ex, r.keys, r.exact)
-            print(f"\n[serving] {mode}: {st.qps:.0f} QPS, p50 {st.p50_ms:.2f} ms, p99 {st.p99_ms:.2f} ms, "
-                  f"overflow reruns {st.overflow_reruns}")
+        alone = {p.qr.qid: S.run_alone(p, arrays, False) for p in prepared}  # each query by itself
+        rows = {q: a[0].shape[0] for q, a in alone.items()}
+        S.run_native(tables, prepared, arrays, "batched", result_rows=rows)  # warm: pools, estimator weights
+        for loop in ("python", "native"):
+            for mode in ("plain", "batched"):
+                if loop == "python":
+                    st = S.run(tables, prepared, arrays, mode)
+                else:
+                    st = S.run_native(tables, prepared, arrays, mode, result_rows=rows)
+                assert st.completed == len(queries)
+                for p in prepared:
+                    r = st.results[p.qr.qid]
+                    same(*alone[p.qr.qid], r.keys, r.exact)
+                print(f"\n[serving] {loop} loop, {mode}: {st.qps:.0f} QPS, p50 {st.p50_ms:.2f} ms, "
+                      f"p99 {st.p99_ms:.2f} ms, overflow reruns {st.overflow_reruns}")
     finally:
         ops.jit_set_mode(-1)
         for t in tables:

@@ -80,6 +80,7 @@ SIGNATURES = {
     "ws_hll_sketch": (C.c_int, [C.POINTER(abi.ExprEnv), C.c_int, C.POINTER(abi.AggPlan), C.c_int, P, P, P, C.c_int,
                                 C.c_int64, P, I64P, I64P]),
     "ws_mlp_infer": (C.c_int, [P, C.c_int, C.c_int, C.c_int, P, P, P, P, P, C.c_float, P]),
+    "ws_serve": (C.c_int, [P, C.c_int, C.c_int, C.c_int64, P, C.POINTER(C.c_double)]),
     "ws_jit_set_mode": (C.c_int, [C.c_int]),
     "ws_jit_mode": (C.c_int, []),
     "ws_jit_set_default_mode": (C.c_int, [C.c_int]),

@@ -86,3 +86,20 @@ def layout() -> list[int]:
             AggPlan.aggBits.offset, AggPlan.aggPart.offset, AggPlan.aggNull.offset, AggPlan.densePriv.offset,
             AggPlan.keyInt.offset, AggPlan.genv.offset, o(DenseSpec), DenseSpec.kmin.offset, DenseSpec.range.offset,
             DenseSpec.stride.offset, DenseSpec.slotOff.offset, DenseSpec.kind.offset]
+
+
+class ServeQuery(C.Structure):
+    """ws_serve_query (include/ws_b200.h)."""
+    _fields_ = [("env", C.c_void_p), ("ncols", C.c_int), ("plan", C.c_void_p), ("jit", C.c_void_p), ("nb", C.c_int),
+                ("bn", C.c_void_p), ("bdel", C.c_void_p), ("bcols", C.c_void_p), ("cap_plain", C.c_int64),
+                ("key_range", C.c_double), ("arrival_s", C.c_double), ("footprint", C.c_int64),
+                ("max_groups", C.c_int64), ("keys", C.c_void_p), ("accs", C.c_void_p), ("exact", C.c_void_p),
+                ("start_s", C.c_double), ("finish_s", C.c_double), ("runs", C.c_int), ("cap_used", C.c_int64),
+                ("groups", C.c_int64)]
+
+
+class EstimatorWeights(C.Structure):
+    """ws_estimator_weights (include/ws_b200.h)."""
+    _fields_ = [("hidden", C.c_int), ("w1", C.c_void_p), ("b1", C.c_void_p), ("w2", C.c_void_p), ("b2", C.c_void_p),
+                ("w3", C.c_void_p), ("b3", C.c_float), ("mean", C.c_void_p), ("std", C.c_void_p),
+                ("margin", C.c_double)]

@@ -254,3 +254,57 @@ def run_alone(p: Prepared, arrays: list, learned: bool):
     """The query by itself on this thread (the reference result of the mix checks)."""
     keys, ex, _, _ = execute(p, arrays[p.qr.table], learned)
     return keys, ex
+
+
+def run_native(tables: list, prepared: list, arrays: list, mode: str = "batched", slots: int | None = None,
+               hbm_budget: int = 8 << 30, keep_results: bool = True, result_rows: dict | None = None) -> Stats:
+    """The same serving loop in the library (ws_serve): C++ worker threads with a CUDA stream each,
+    no Python on the per-query path; the prepared queries' arrival times are honoured.  Results go to
+    host arrays allocated (and touched) before the loop: result_rows[qid] rows each when given, else
+    the key ranges' bound."""
+    import ctypes as C
+
+    from . import estimator, ops
+    learned = mode == "batched"
+    nslots = slots or (16 if learned else 4)
+    qs = (abi.ServeQuery * len(prepared))()
+    keep = []
+    for i, p in enumerate(prepared):
+        t = tables[p.qr.table]
+        nb, bn, bdel, arr, _ = arrays[p.qr.table]
+        q = qs[i]
+        q.env, q.ncols, q.plan, q.jit = C.addressof(p.env), p.ncols, C.addressof(p.plan), p.prog
+        q.nb, q.bn, q.bdel, q.bcols = nb, C.addressof(bn), C.addressof(bdel), C.addressof(arr)
+        q.cap_plain, q.key_range, q.arrival_s, q.footprint = p.cap, float(p.bound), p.qr.arrival, footprint(t, p.qr)
+        if keep_results:
+            g = result_rows[p.qr.qid] if result_rows else min(p.bound, t.n)
+            nk, na = p.plan.nkeys, p.plan.naggs
+            k = np.empty((g, nk), np.float64)
+            x = np.empty((g, na, 2), np.int64)
+            k.fill(0)  # page the arrays in before the timed loop
+            x.fill(0)
+            keep.append((k, x))
+            q.max_groups, q.keys, q.exact = g, k.ctypes.data, x.ctypes.data
+        else:
+            keep.append(None)
+    w = None
+    if learned:
+        m = estimator.model()
+        hold = [np.ascontiguousarray(a) for a in (m.w1, m.b1, m.w2, m.b2, m.w3, m.mean, m.std)]
+        keep.append(hold)
+        w = abi.EstimatorWeights(estimator.HIDDEN, hold[0].ctypes.data, hold[1].ctypes.data, hold[2].ctypes.data,
+                                 hold[3].ctypes.data, hold[4].ctypes.data, float(m.b3), hold[5].ctypes.data,
+                                 hold[6].ctypes.data, 2.0 ** float(m.meta.get("val_p90_log2_err", 0.0)))
+    wall = C.c_double()
+    ops.check(ops.lib().ws_serve(qs, len(prepared), nslots, hbm_budget, C.byref(w) if w else None, C.byref(wall)))
+    lat = np.array([(q.finish_s - q.arrival_s) * 1e3 for q in qs])
+    span = max(q.finish_s for q in qs) - min(q.arrival_s for q in qs)
+    results = {}
+    for i, p in enumerate(prepared):
+        q = qs[i]
+        k, x = keep[i] if keep[i] is not None else (None, None)
+        results[p.qr.qid] = Result(p.qr.qid, k[:q.groups] if k is not None else None,
+                                   x[:q.groups] if x is not None else None, q.arrival_s, q.start_s, q.finish_s, q.runs,
+                                   q.cap_used)
+    return Stats(mode, len(prepared) / span, float(np.percentile(lat, 50)), float(np.percentile(lat, 99)),
+                 len(prepared), sum(q.runs - 1 for q in qs), results)
