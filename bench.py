@@ -111,14 +111,21 @@ def dist_setup(n_gpus: int):
     return ws, rank, local
 
 
-def reduce_max(x: float, ws: int) -> float:
+def reduce_max(x: float, ws: int, device: str = "cuda") -> float:
+    """Max over ranks (the step time of the slowest replica)."""
     if ws <= 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def whole_job_rate(rows_per_rank: int, ws: int, ms_step_max: float) -> float:
+    """G rows/s of all replicas: every rank scans rows_per_rank per step; the job's step lasts as long
+    as the slowest rank's."""
+    return rows_per_rank * ws / (ms_step_max / 1e3) / 1e9
 
 
 def barrier(ws: int):
@@ -243,7 +250,7 @@ def run_ours(args, ws, rank, local):
     kernel_ms = float(np.mean([a.elapsed_time(b) for a, b in ev]))
     ms_step = reduce_max(total_ms / args.steps, ws)
     rows_all = table.n * ws
-    value = rows_all / (ms_step / 1e3) / 1e9
+    value = whole_job_rate(table.n, ws, ms_step)
 
     # end to end from pinned host buffers through the C ABI
     e2e_steps = max(1, min(args.steps, 5))
