@@ -53,6 +53,10 @@ int ws_d2h(void* dst, const void* src, size_t bytes);
 int ws_d2d(void* dst, const void* src, size_t bytes);
 int ws_gpu_sync(void);
 int ws_gpu_trim_pool(void);
+/* Pinned host memory that kernels can write (cudaHostAlloc, mapped): the destination of
+ * ws_agg_fetch_async.  No counterpart in the reference, whose pinned staging is internal. */
+int ws_host_alloc(size_t bytes, void** out);
+int ws_host_free(void* p);
 
 /* ---- aggregation (src/gpu.h:84-130, class GpuAggregator).
  * Batches (segments, write buffers or a joined relation) are collected with ws_agg_add_batch and
@@ -84,6 +88,19 @@ int ws_agg_group_count(ws_aggregator* agg, int64_t* out);
  * the exact int128 integer SUM, (value, 0) for COUNT / integer MIN / MAX, (bits, 0) for doubles.
  * max_groups < groups: WS_ERR_SIZE with *ngroups set. */
 int ws_agg_fetch(ws_aggregator* agg, int64_t max_groups, double* keys, double* accs, int64_t* exact, int64_t* ngroups);
+/* The same groups without a host round trip (no counterpart in the reference; the serving loop's
+ * form): queues compaction and a kernel that writes keys [g][nkeys] and exact [g][naggs][2] (the
+ * formats above) straight into host memory, and *status, then returns.  keys, exact and status must
+ * be pinned host memory (ws_host_alloc, or registered with CUDA); they are valid once the calling
+ * thread's stream has been synchronised (ws_gpu_sync).  status->overflow: the hash table filled up
+ * (ws_agg_overflowed; nothing written, rerun bigger); status->error: WS_ERR_RANGE / WS_ERR_INTERNAL
+ * where ws_agg_fetch would raise them (nothing written); status->groups > max_groups: nothing written. */
+typedef struct ws_fetch_status {
+  int64_t groups;
+  int32_t overflow;
+  int32_t error;
+} ws_fetch_status;
+int ws_agg_fetch_async(ws_aggregator* agg, int64_t max_groups, double* keys, int64_t* exact, ws_fetch_status* status);
 /* Without GROUP BY: which slots hold exact int64 bits (GpuAggregator::sumBitsSlots) and the high 64 bits
  * of the exact integer sums (GpuAggregator::sumHigh; valid after ws_agg_fetch). */
 int ws_agg_sum_bits_slots(const ws_aggregator* agg, uint8_t* out);
@@ -183,7 +200,10 @@ int ws_mlp_infer(const float* x, int rows, int features, int hidden, const uint1
 
 /* ---- request loop (no counterpart in the reference, whose connections each run their query
  * synchronously): prepared GROUP BY queries served by `slots` host threads with a CUDA stream each,
- * in arrival order, admitted while the footprints of the queries in flight fit hbm_budget. */
+ * in arrival order, admitted while the footprints of the queries in flight fit hbm_budget.  A query
+ * whose result arrays (keys, exact; no accs) are pinned host memory (ws_host_alloc) is run in the
+ * one-sync form (ws_agg_fetch_async: the thread waits once per run); other queries follow the engine's
+ * sequence of ws_agg_overflowed / ws_agg_fetch. */
 typedef struct ws_serve_query {
   /* in */
   const ws_expr_env* env;

@@ -35,6 +35,8 @@ SIGNATURES = {
     "ws_d2d": (C.c_int, [P, P, C.c_size_t]),
     "ws_gpu_sync": (C.c_int, []),
     "ws_gpu_trim_pool": (C.c_int, []),
+    "ws_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(P)]),
+    "ws_host_free": (C.c_int, [P]),
     "ws_agg_create": (C.c_int, [C.POINTER(abi.AggPlan), C.c_int64, C.POINTER(abi.DenseSpec), C.POINTER(P)]),
     "ws_agg_destroy": (None, [P]),
     "ws_agg_add_batch": (C.c_int, [P, C.POINTER(abi.ExprEnv), C.c_int, C.c_int64, P]),
@@ -49,6 +51,7 @@ SIGNATURES = {
     "ws_agg_overflowed": (C.c_int, [P, C.POINTER(C.c_int)]),
     "ws_agg_group_count": (C.c_int, [P, I64P]),
     "ws_agg_fetch": (C.c_int, [P, C.c_int64, P, P, P, I64P]),
+    "ws_agg_fetch_async": (C.c_int, [P, C.c_int64, P, P, P]),
     "ws_agg_sum_bits_slots": (C.c_int, [P, P]),
     "ws_agg_sum_high": (C.c_int, [P, P]),
     "ws_agg_compact": (C.c_int, [P, C.POINTER(P), C.POINTER(P), I64P]),

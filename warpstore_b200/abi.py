@@ -98,6 +98,11 @@ class ServeQuery(C.Structure):
                 ("groups", C.c_int64)]
 
 
+class FetchStatus(C.Structure):
+    """ws_fetch_status (include/ws_b200.h)."""
+    _fields_ = [("groups", C.c_int64), ("overflow", C.c_int32), ("error", C.c_int32)]
+
+
 class EstimatorWeights(C.Structure):
     """ws_estimator_weights (include/ws_b200.h)."""
     _fields_ = [("hidden", C.c_int), ("w1", C.c_void_p), ("b1", C.c_void_p), ("w2", C.c_void_p), ("b2", C.c_void_p),

@@ -96,6 +96,7 @@ struct OccSpec {
 };
 __device__ __forceinline__ bool occupied(const u64* rows, int64_t i, const OccSpec& s) {
   const u64* r = rows + i * s.rw;
+  if (s.mode == 0) return true;  // no GROUP BY: the one result row
   if (s.mode == 1) return r[s.cnt0] != 0;
   if (i == s.cap) return r[0] != 0;
   return r[0] != kEmpty;
@@ -151,34 +152,87 @@ struct EmitSpec {
   const double* tkeys;
   int64_t cap;
 };
+// Keys (engine format) and exact words of result row i: key k at kout[k * kstride], slot a at
+// xout[2a], xout[2a + 1].
+__device__ __forceinline__ void emitRow(const u64* rows, int64_t i, const EmitSpec& s, double* kout, int64_t kstride,
+                                        long long* xout) {
+  const u64* r = rows + i * s.rw;
+  for (int k = 0; k < s.nk; ++k) {
+    double kv;
+    if (s.mode == 1) {
+      const long long v = s.kmin[k] + (i / s.stride[k]) % s.range[k];
+      kv = s.keyInt[k] ? __longlong_as_double(v) : (double)v;
+    } else if (s.nk == 1 && i != s.cap) {
+      kv = __longlong_as_double((long long)r[0]);
+    } else {
+      kv = s.tkeys[i * s.nk + k];
+    }
+    kout[k * kstride] = kv;
+  }
+  for (int a = 0; a < s.na; ++a) {
+    const int src = s.kind[a] == SK_NONE ? s.partner[a] : a;
+    const int o = s.woff[src];
+    long long w0 = (long long)r[o], w1 = 0;
+    const uint8_t k = s.kind[src];
+    if (k == SK_ISUM) w1 = (long long)r[o + 1];
+    else if (k == SK_DMIN || k == SK_DMAX) w0 = __double_as_longlong(dunord(w0));
+    xout[2 * a] = w0;
+    xout[2 * a + 1] = w1;
+  }
+}
+
 __global__ void kEmit(const u64* rows, const int64_t* idx, int64_t m, EmitSpec s, double* keys, int64_t* exact,
                       int colMajor) {
   for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < m; j += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = idx ? idx[j] : j;
-    const u64* r = rows + i * s.rw;
-    for (int k = 0; k < s.nk; ++k) {
-      double kv;
-      if (s.mode == 1) {
-        const long long v = s.kmin[k] + (i / s.stride[k]) % s.range[k];
-        kv = s.keyInt[k] ? __longlong_as_double(v) : (double)v;
-      } else if (s.nk == 1 && i != s.cap) {
-        kv = __longlong_as_double((long long)r[0]);
-      } else {
-        kv = s.tkeys[i * s.nk + k];
-      }
-      keys[colMajor ? k * m + j : j * s.nk + k] = kv;
-    }
-    for (int a = 0; a < s.na; ++a) {
-      const int src = s.kind[a] == SK_NONE ? s.partner[a] : a;
-      const int o = s.woff[src];
-      long long w0 = (long long)r[o], w1 = 0;
-      const uint8_t k = s.kind[src];
-      if (k == SK_ISUM) w1 = (long long)r[o + 1];
-      else if (k == SK_DMIN || k == SK_DMAX) w0 = __double_as_longlong(dunord(w0));
-      exact[(j * s.na + a) * 2] = w0;
-      exact[(j * s.na + a) * 2 + 1] = w1;
-    }
+    emitRow(rows, i, s, colMajor ? keys + j : keys + j * s.nk, colMajor ? m : 1, (long long*)exact + j * s.na * 2);
   }
+}
+
+// Fetch straight into host memory (pinned and mapped): the groups of chunk b of kOccChunk result rows
+// go to rows offs[b].. in ascending row order, one sub-tile of blockDim result rows at a time, each
+// sub-tile's rows staged in shared memory ([blockDim][nk + 2 na] words) and stored as contiguous words
+// (whole PCIe writes rather than one 8-byte write per word of a row).  Nothing is written when the run
+// raised a flag (hash overflow, dense key out of range, staged-copy timeout) or the groups exceed
+// maxGroups: the caller reads the status and reruns or grows its buffers.
+__global__ void kOccEmitHost(const u64* rows, int64_t nrows, OccSpec o, EmitSpec s, const int64_t* offs, int64_t nchunks,
+                             const int* err, int64_t maxGroups, double* keys, long long* exact) {
+  extern __shared__ long long stg[];
+  __shared__ int wbase[32];
+  if (err[0] || err[2] || (o.mode == 2 && err[1]) || offs[nchunks] > maxGroups) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int xw = 2 * s.na, rw = s.nk + xw;
+  const int64_t c0 = (int64_t)blockIdx.x * kOccChunk, cend = min(c0 + kOccChunk, nrows);
+  int64_t run = offs[blockIdx.x];
+  for (int64_t b = c0; b < cend; b += blockDim.x) {
+    const int64_t i = b + threadIdx.x;
+    const bool occ = i < cend && occupied(rows, i, o);
+    const unsigned m = __ballot_sync(0xffffffffu, occ);
+    if (lane == 0) wbase[warp] = __popc(m);
+    __syncthreads();
+    int before = 0, total = 0;
+    for (int w = 0; w < nw; ++w) {
+      if (w < warp) before += wbase[w];
+      total += wbase[w];
+    }
+    if (occ) {
+      long long* r = stg + (int64_t)(before + __popc(m & ((1u << lane) - 1))) * rw;
+      emitRow(rows, i, s, (double*)r, 1, r + s.nk);
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < total * s.nk; t += blockDim.x)
+      keys[run * s.nk + t] = __longlong_as_double(stg[(t / s.nk) * rw + t % s.nk]);
+    for (int t = threadIdx.x; t < total * xw; t += blockDim.x) exact[run * xw + t] = stg[(t / xw) * rw + s.nk + t % xw];
+    run += total;
+    __syncthreads();
+  }
+}
+
+// Status of an asynchronous fetch, in host memory (pinned and mapped).
+__global__ void kFetchStatus(const int64_t* total, const int* err, int hashMode, ws_fetch_status* st) {
+  st->groups = *total;
+  st->overflow = hashMode && err[1] ? 1 : 0;
+  st->error = err[0] ? WS_ERR_RANGE : err[2] ? WS_ERR_INTERNAL : 0;
 }
 
 // Exact words -> the engine's double slot format, on the device (for compact()).
@@ -748,6 +802,56 @@ int ws_agg_fetch(ws_aggregator* A, int64_t max_groups, double* keys, double* acc
     }
     A->hi = A->cachedHi;
     A->fetched = true;
+  });
+}
+
+int ws_agg_fetch_async(ws_aggregator* A, int64_t max_groups, double* keys, int64_t* exact, ws_fetch_status* status) {
+  return guardedCall([&] {
+    const int nk = A->plan.nkeys, na = A->plan.naggs;
+    auto mapped = [](void* h, const char* what) -> void* {
+      if (!h) throw Error(std::string("fetch_async: ") + what + " is null", WS_ERR_ARG);
+      cudaPointerAttributes at{};
+      if (cudaPointerGetAttributes(&at, h) != cudaSuccess || at.type != cudaMemoryTypeHost || !at.devicePointer) {
+        cudaGetLastError();
+        throw Error(std::string("fetch_async: ") + what + " is not pinned host memory", WS_ERR_ARG);
+      }
+      return at.devicePointer;
+    };
+    auto* st = (ws_fetch_status*)mapped(status, "status");
+    double* dk = nk ? (double*)mapped(keys, "keys") : nullptr;
+    auto* dx = (long long*)mapped(exact, "exact");
+    const int64_t nr = A->nrows();
+    OccSpec o{A->lay.rw, nk == 0 ? 0 : A->isDense ? 1 : 2, A->lay.woff[0], A->cap};
+    const int64_t nchunks = (nr + kOccChunk - 1) / kOccChunk;
+    DBuf<int64_t> counts(nchunks + 1);
+    WS_LAUNCH(kOccCount, (unsigned)nchunks, 256, 0, A->rows.p, nr, o, counts.p);
+    WS_LAUNCH(kScanExclusive, 1, 1024, 0, counts.p, nchunks);
+    WS_LAUNCH(kFetchStatus, 1, 1, 0, counts.p + nchunks, A->err(), o.mode == 2 ? 1 : 0, st);
+    // sub-tile rows: staging of at most 32 KB, a multiple of 32 rows
+    const int rowBytes = 8 * (nk + 2 * na);
+    const int threads = std::max(32, std::min(256, (32768 / rowBytes) & ~31));
+    WS_LAUNCH(kOccEmitHost, (unsigned)nchunks, threads, (size_t)threads * rowBytes, A->rows.p, nr, o, emitSpec(*A),
+              counts.p, nchunks, A->err(), max_groups, dk, dx);
+    A->cachedGroups = -1;
+    A->fetched = true;
+  });
+}
+
+int ws_host_alloc(size_t bytes, void** out) {
+  return guardedCall([&] {
+    *out = nullptr;
+    ws_gpu_init();
+    if (cudaHostAlloc(out, std::max<size_t>(bytes, 1), cudaHostAllocMapped) != cudaSuccess) {
+      cudaGetLastError();
+      *out = nullptr;
+      throw Error("pinned host allocation of " + std::to_string(bytes) + " bytes failed", WS_ERR_OOM);
+    }
+  });
+}
+
+int ws_host_free(void* p) {
+  return guardedCall([&] {
+    if (p) WS_CK(cudaFreeHost(p));
   });
 }
 

@@ -72,8 +72,21 @@ void checkRc(int rc) {
   if (rc) throw ws::Error(ws_last_error(), rc);
 }
 
-// One query on the calling thread's stream.
-void serveOne(ws_serve_query& q, const ws_estimator_weights* w) {
+bool pinnedHost(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeHost && at.devicePointer;
+}
+
+// One query on the calling thread's stream.  Results into pinned host arrays (keys / exact, no accs)
+// take the one-sync form: run, compaction and the kernel that writes the groups into host memory are
+// queued back to back, and the thread waits once; otherwise the engine's sequence (overflow check,
+// group count, compaction, copies), which waits at each step.
+void serveOne(ws_serve_query& q, const ws_estimator_weights* w, ws_fetch_status* st) {
   int64_t cap = q.cap_plain;
   if (w && cap > (1 << 16)) {
     std::vector<uint32_t> regs(1u << 12);
@@ -95,6 +108,22 @@ void serveOne(ws_serve_query& q, const ws_estimator_weights* w) {
     checkRc(ws_agg_create(q.plan, cap, nullptr, &a));
     int rc = ws_agg_add_batches(a, q.ncols, q.nb, q.bn, q.bdel, q.bcols);
     if (!rc) rc = ws_agg_run(a, q.env, q.jit);
+    if (st) {
+      if (!rc) rc = ws_agg_fetch_async(a, q.max_groups, q.keys, q.exact, st);
+      if (!rc) rc = ws_gpu_sync();
+      ws_agg_destroy(a);
+      checkRc(rc);
+      if (st->error) throw ws::Error("serve: the aggregation raised an error flag", st->error);
+      if (st->overflow) {
+        cap = grow(cap, st->groups);
+        continue;
+      }
+      if (st->groups > q.max_groups)
+        throw ws::Error("output buffer too small for " + std::to_string(st->groups) + " groups", WS_ERR_SIZE);
+      q.groups = st->groups;
+      q.cap_used = cap;
+      return;
+    }
     int ovf = 0;
     if (!rc) rc = ws_agg_overflowed(a, &ovf);
     if (!rc && ovf) {
@@ -139,6 +168,12 @@ int ws_serve(ws_serve_query* queries, int n, int slots, int64_t hbm_budget, cons
         return;
       }
       ws_set_stream(s);
+      ws_fetch_status* st = nullptr;  // this worker's fetch status (pinned, for the one-sync form)
+      if (cudaHostAlloc((void**)&st, sizeof(ws_fetch_status), cudaHostAllocMapped) != cudaSuccess) {
+        cudaGetLastError();
+        st = nullptr;
+        failed = 1;
+      }
       for (;;) {
         const int i = next++;
         if (i >= n || failed) break;
@@ -152,7 +187,9 @@ int ws_serve(ws_serve_query* queries, int n, int slots, int64_t hbm_budget, cons
         }
         q.start_s = nowS() - t0;
         try {
-          serveOne(q, est);
+          const bool oneSync = (q.keys || !q.plan->nkeys) && q.exact && !q.accs && pinnedHost(q.exact) &&
+                               (!q.keys || pinnedHost(q.keys));
+          serveOne(q, est, oneSync ? st : nullptr);
         } catch (const ws::Error& e) {
           std::lock_guard<std::mutex> l(mu);
           if (!failed++) firstError = e.what(), firstCode = e.code;
@@ -167,6 +204,7 @@ int ws_serve(ws_serve_query* queries, int n, int slots, int64_t hbm_budget, cons
       ws_set_stream(nullptr);
       cudaStreamSynchronize(s);
       cudaStreamDestroy(s);
+      if (st) cudaFreeHost(st);
     };
     std::vector<std::thread> th;
     for (int k = 0; k < slots; ++k) th.emplace_back(worker);

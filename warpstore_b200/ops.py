@@ -119,6 +119,36 @@ def codegen_compile_check(env: abi.ExprEnv, ncols: int, plan: abi.AggPlan, fn: i
 
 
 # ------------------------------------------------------------------ aggregation
+FETCH_STATUS = np.dtype([("groups", "<i8"), ("overflow", "<i4"), ("error", "<i4")])
+
+
+class HostBuffer:
+    """Pinned host memory that kernels can write (ws_host_alloc), viewed as a numpy array."""
+
+    def __init__(self, shape, dtype):
+        dtype = np.dtype(dtype)
+        shape = tuple(int(x) for x in np.atleast_1d(shape))
+        count = int(np.prod(shape))
+        nbytes = max(count * dtype.itemsize, 1)
+        p = P()
+        check(lib().ws_host_alloc(nbytes, C.byref(p)))
+        self.ptr = p.value
+        raw = np.ctypeslib.as_array((C.c_uint8 * nbytes).from_address(self.ptr))
+        self.array = raw[:count * dtype.itemsize].view(dtype).reshape(shape)
+
+    def close(self):
+        if self.ptr:
+            self.array = None
+            lib().ws_host_free(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class GpuAggregator:
     """GPU aggregation state of one query (src/gpu.h:84-130)."""
 
@@ -193,6 +223,12 @@ class GpuAggregator:
         check(lib().ws_agg_fetch(self.h, n, keys.ctypes.data if nk else None, accs.ctypes.data,
                                  ex.ctypes.data if exact else None, C.byref(g)))
         return keys, accs, ex
+
+    def fetch_async(self, max_groups: int, keys: "HostBuffer | None", exact: "HostBuffer", status: "HostBuffer"):
+        """Queues the groups' copy straight into pinned host buffers (ws_agg_fetch_async); they are valid
+        after sync().  status: a HostBuffer of FETCH_STATUS (groups, overflow, error)."""
+        check(lib().ws_agg_fetch_async(self.h, int(max_groups), keys.ptr if keys is not None else None, exact.ptr,
+                                       status.ptr))
 
     def sum_bits_slots(self) -> np.ndarray:
         out = np.zeros(self.plan.naggs, dtype=np.uint8)

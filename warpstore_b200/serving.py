@@ -257,15 +257,19 @@ def run_alone(p: Prepared, arrays: list, learned: bool):
 
 
 def run_native(tables: list, prepared: list, arrays: list, mode: str = "batched", slots: int | None = None,
-               hbm_budget: int = 8 << 30, keep_results: bool = True, result_rows: dict | None = None) -> Stats:
+               hbm_budget: int = 8 << 30, keep_results: bool = True, result_rows: dict | None = None,
+               pinned: bool | None = None) -> Stats:
     """The same serving loop in the library (ws_serve): C++ worker threads with a CUDA stream each,
     no Python on the per-query path; the prepared queries' arrival times are honoured.  Results go to
     host arrays allocated (and touched) before the loop: result_rows[qid] rows each when given, else
-    the key ranges' bound."""
+    the key ranges' bound.  pinned (default: the batched form): the result arrays are pinned host
+    memory, so each query runs in the one-sync form (the GPU writes its groups into them); plain:
+    ordinary host arrays, the engine's fetch sequence."""
     import ctypes as C
 
     from . import estimator, ops
     learned = mode == "batched"
+    pinned = learned if pinned is None else pinned
     nslots = slots or (16 if learned else 4)
     qs = (abi.ServeQuery * len(prepared))()
     keep = []
@@ -279,11 +283,16 @@ def run_native(tables: list, prepared: list, arrays: list, mode: str = "batched"
         if keep_results:
             g = result_rows[p.qr.qid] if result_rows else min(p.bound, t.n)
             nk, na = p.plan.nkeys, p.plan.naggs
-            k = np.empty((g, nk), np.float64)
-            x = np.empty((g, na, 2), np.int64)
+            if pinned:
+                hk, hx = ops.HostBuffer((max(g, 1), nk), np.float64), ops.HostBuffer((max(g, 1), na, 2), np.int64)
+                keep.append((hk.array, hx.array, hk, hx))
+                k, x = hk.array, hx.array
+            else:
+                k = np.empty((g, nk), np.float64)
+                x = np.empty((g, na, 2), np.int64)
+                keep.append((k, x))
             k.fill(0)  # page the arrays in before the timed loop
             x.fill(0)
-            keep.append((k, x))
             q.max_groups, q.keys, q.exact = g, k.ctypes.data, x.ctypes.data
         else:
             keep.append(None)
@@ -302,9 +311,9 @@ def run_native(tables: list, prepared: list, arrays: list, mode: str = "batched"
     results = {}
     for i, p in enumerate(prepared):
         q = qs[i]
-        k, x = keep[i] if keep[i] is not None else (None, None)
-        results[p.qr.qid] = Result(p.qr.qid, k[:q.groups] if k is not None else None,
-                                   x[:q.groups] if x is not None else None, q.arrival_s, q.start_s, q.finish_s, q.runs,
-                                   q.cap_used)
+        k, x = keep[i][:2] if keep[i] is not None else (None, None)
+        results[p.qr.qid] = Result(p.qr.qid, k[:q.groups].copy() if k is not None else None,
+                                   x[:q.groups].copy() if x is not None else None, q.arrival_s, q.start_s, q.finish_s,
+                                   q.runs, q.cap_used)
     return Stats(mode, len(prepared) / span, float(np.percentile(lat, 50)), float(np.percentile(lat, 99)),
                  len(prepared), sum(q.runs - 1 for q in qs), results)
