@@ -89,18 +89,21 @@ int ws_agg_group_count(ws_aggregator* agg, int64_t* out);
  * max_groups < groups: WS_ERR_SIZE with *ngroups set. */
 int ws_agg_fetch(ws_aggregator* agg, int64_t max_groups, double* keys, double* accs, int64_t* exact, int64_t* ngroups);
 /* The same groups without a host round trip (no counterpart in the reference; the serving loop's
- * form): queues compaction and a kernel that writes keys [g][nkeys] and exact [g][naggs][2] (the
- * formats above) straight into host memory, and *status, then returns.  keys, exact and status must
- * be pinned host memory (ws_host_alloc, or registered with CUDA); they are valid once the calling
- * thread's stream has been synchronised (ws_gpu_sync).  status->overflow: the hash table filled up
- * (ws_agg_overflowed; nothing written, rerun bigger); status->error: WS_ERR_RANGE / WS_ERR_INTERNAL
- * where ws_agg_fetch would raise them (nothing written); status->groups > max_groups: nothing written. */
+ * form): queues compaction and a kernel that writes groups [first_group, first_group + max_groups) (in
+ * ws_agg_fetch's order) as keys [.][nkeys] and exact [.][naggs][2] (the formats above) straight into
+ * host memory, and *status, then returns.  keys, exact and status must be pinned host memory
+ * (ws_host_alloc, or registered with CUDA); they are valid once the calling thread's stream has been
+ * synchronised (ws_gpu_sync).  status->groups: all groups of the run (a caller with a smaller buffer
+ * fetches the rest range by range; the compaction is done once per run); status->overflow: the hash
+ * table filled up (ws_agg_overflowed; nothing written, rerun bigger); status->error: WS_ERR_RANGE /
+ * WS_ERR_INTERNAL where ws_agg_fetch would raise them (nothing written). */
 typedef struct ws_fetch_status {
   int64_t groups;
   int32_t overflow;
   int32_t error;
 } ws_fetch_status;
-int ws_agg_fetch_async(ws_aggregator* agg, int64_t max_groups, double* keys, int64_t* exact, ws_fetch_status* status);
+int ws_agg_fetch_async(ws_aggregator* agg, int64_t first_group, int64_t max_groups, double* keys, int64_t* exact,
+                       ws_fetch_status* status);
 /* Without GROUP BY: which slots hold exact int64 bits (GpuAggregator::sumBitsSlots) and the high 64 bits
  * of the exact integer sums (GpuAggregator::sumHigh; valid after ws_agg_fetch). */
 int ws_agg_sum_bits_slots(const ws_aggregator* agg, uint8_t* out);
@@ -200,10 +203,14 @@ int ws_mlp_infer(const float* x, int rows, int features, int hidden, const uint1
 
 /* ---- request loop (no counterpart in the reference, whose connections each run their query
  * synchronously): prepared GROUP BY queries served by `slots` host threads with a CUDA stream each,
- * in arrival order, admitted while the footprints of the queries in flight fit hbm_budget.  A query
- * whose result arrays (keys, exact; no accs) are pinned host memory (ws_host_alloc) is run in the
- * one-sync form (ws_agg_fetch_async: the thread waits once per run); other queries follow the engine's
- * sequence of ws_agg_overflowed / ws_agg_fetch. */
+ * in arrival order, admitted while the footprints of the queries in flight fit hbm_budget.
+ * Results go to the query's arrays when it has them, else (arena_bytes > 0) to the worker's own
+ * buffer, where each delivery is folded into the query's digest when `checksum` is set (the buffer
+ * is reused by the worker's next query, as a server's send buffer is), else they stay on the device.
+ * one_sync: queries run in the one-sync form (ws_agg_fetch_async into pinned memory: the thread waits
+ * once per run, or once per arena-sized range of a larger result) when their arrays (keys, exact; no
+ * accs) are pinned host memory (ws_host_alloc), or into the arena (pinned); otherwise queries follow
+ * the engine's sequence of ws_agg_overflowed / ws_agg_fetch (into pageable arrays or arena). */
 typedef struct ws_serve_query {
   /* in */
   const ws_expr_env* env;
@@ -218,7 +225,7 @@ typedef struct ws_serve_query {
   double key_range;                 /* product of the keys' value ranges (0: unknown) */
   double arrival_s;                 /* seconds from the start of ws_serve */
   int64_t footprint;                /* device bytes the query may hold while it runs */
-  int64_t max_groups;               /* capacity of the result arrays below (0: results not kept) */
+  int64_t max_groups;               /* capacity of the result arrays below */
   double* keys;                     /* [max_groups][nkeys], as ws_agg_fetch (may be null) */
   double* accs;                     /* [max_groups][naggs] (may be null) */
   int64_t* exact;                   /* [max_groups][naggs][2] (may be null) */
@@ -226,6 +233,9 @@ typedef struct ws_serve_query {
   double start_s, finish_s;         /* admitted, done (seconds from the start) */
   int runs;                         /* aggregation runs (1 + overflow reruns) */
   int64_t cap_used, groups;
+  uint64_t checksum;                /* with `checksum`: sum over the groups of a hash of their key bits and
+                                       exact words (DOUBLE SUM slots excluded) -- order-independent */
+  double fsum;                      /* with `checksum`: the sum of the DOUBLE SUM slots over the groups */
 } ws_serve_query;
 /* Learned sizing (est may be null for the plain rule): the estimator's MLP (9 features, `hidden`
  * units, BF16 weight bits), its input normalisation and the capacity margin (2^(p90 log2 error)). */
@@ -241,8 +251,15 @@ typedef struct ws_estimator_weights {
   const float* std;
   double margin;
 } ws_estimator_weights;
-int ws_serve(ws_serve_query* queries, int n, int slots, int64_t hbm_budget, const ws_estimator_weights* est,
-             double* wall_s);
+typedef struct ws_serve_options {
+  int slots;                        /* worker threads (queries in flight), 1..256 */
+  int64_t hbm_budget;               /* admission: device bytes of the queries in flight */
+  const ws_estimator_weights* est;  /* learned sizing of large hash tables; null: the plain rule */
+  int one_sync;                     /* the one-sync form (see above) */
+  int64_t arena_bytes;              /* per worker, for queries without result arrays (0: none) */
+  int checksum;                     /* digest every delivered group (checksum, fsum) */
+} ws_serve_options;
+int ws_serve(ws_serve_query* queries, int n, const ws_serve_options* opt, double* wall_s);
 
 /* ---- ORDER BY (src/gpu.h:197-199) */
 /* gpuSortPerm: stable permutation sorting rows 0..m-1 by keys[0] (most significant) .. keys[nkeys-1],

@@ -1,7 +1,7 @@
 """The one-sync fetch (ws_agg_fetch_async): the groups the GPU writes straight into pinned host memory
 are the ones ws_agg_fetch returns, word for word and in the same order (dense, hash, multi-key and
-no-key plans, with and without the compiled plan); an overflowed hash run and a too-small buffer
-write nothing and say so in the status; ordinary host memory is refused."""
+no-key plans, with and without the compiled plan), whole or range by range; an overflowed hash run
+writes nothing and says so in the status; ordinary host memory is refused."""
 import ctypes as C
 
 import numpy as np
@@ -16,19 +16,19 @@ from .test_agg_gpu import gpu_aggregate
 pytestmark = pytest.mark.gpu
 
 
-def fetch_async(agg, max_groups):
+def fetch_async(agg, max_groups, first=0):
     nk, na = agg.plan.nkeys, agg.plan.naggs
     hk = ops.HostBuffer((max(max_groups, 1), max(nk, 1)), np.float64)
     hx = ops.HostBuffer((max(max_groups, 1), na, 2), np.int64)
     st = ops.HostBuffer(1, ops.FETCH_STATUS)
     hk.array.fill(0)
     hx.array.fill(0)
-    agg.fetch_async(max_groups, hk if nk else None, hx, st)
+    agg.fetch_async(max_groups, hk if nk else None, hx, st, first)
     ops.sync()
     s = st.array[0]
     g = int(s["groups"])
-    out = (g, int(s["overflow"]), int(s["error"]), hk.array[:min(g, max_groups), :nk].copy(),
-           hx.array[:min(g, max_groups)].copy(), hx.array.copy())
+    m = max(0, min(g - first, max_groups))
+    out = (g, int(s["overflow"]), int(s["error"]), hk.array[:m, :nk].copy(), hx.array[:m].copy(), hx.array.copy())
     for b in (hk, hx, st):
         b.close()
     return out
@@ -74,7 +74,7 @@ def test_multi_key_many_groups_equal_fetch():
     agg.close()
 
 
-def test_overflow_and_small_buffer_write_nothing():
+def test_overflow_writes_nothing_and_ranges_assemble():
     n = 400_000
     rng = np.random.default_rng(3)
     t = W.Table(n, seg_rows=1 << 17)
@@ -88,14 +88,22 @@ def test_overflow_and_small_buffer_write_nothing():
     assert ovf == 1 and err == 0 and not whole.any()
     agg.close()
     agg = gpu_aggregate(t, e, aq.plan, None, 1 << 17)
-    keys, _, _ = agg.fetch()
-    g, ovf, err, _, _, whole = fetch_async(agg, keys.shape[0] - 1)
-    assert (g, ovf, err) == (keys.shape[0], 0, 0) and not whole.any()
+    keys, _, ex = agg.fetch()
+    # range by range (ragged last range, a range past the end): the same groups in the same order
+    parts_k, parts_x, first = [], [], 0
+    while first <= keys.shape[0]:
+        g, ovf, err, k2, x2, _ = fetch_async(agg, 4999, first)
+        assert (g, ovf, err) == (keys.shape[0], 0, 0)
+        parts_k.append(k2)
+        parts_x.append(x2)
+        first += 4999
+    assert np.array_equal(np.concatenate(parts_k).view(np.int64), keys.view(np.int64))
+    assert np.array_equal(np.concatenate(parts_x), ex)
     # ordinary (pageable) host memory is refused
     x = np.zeros((keys.shape[0], aq.plan.naggs, 2), np.int64)
     k = np.zeros((keys.shape[0], 1))
     st = ops.HostBuffer(1, ops.FETCH_STATUS)
-    rc = ops.lib().ws_agg_fetch_async(agg.h, keys.shape[0], k.ctypes.data, x.ctypes.data, st.ptr)
+    rc = ops.lib().ws_agg_fetch_async(agg.h, 0, keys.shape[0], k.ctypes.data, x.ctypes.data, st.ptr)
     assert rc == 1210
     st.close()
     agg.close()

@@ -1,6 +1,7 @@
 """The request loop: every query's result in the mix (overlapping on the device with others) equals
-its result alone — integer slots exactly, DOUBLE sums within 1e-12 relative — in both serving forms;
-QPS and p50 / p99 of the two forms are printed."""
+its result alone — integer slots exactly, DOUBLE sums within 1e-12 relative — in both serving forms,
+into result arrays and through per-worker buffers (digests); QPS and p50 / p99 of the forms are
+printed."""
 import numpy as np
 import pytest
 
@@ -46,6 +47,19 @@ def test_results_alone_equal_results_in_the_mix():
                     same(*alone[p.qr.qid], r.keys, r.exact)
                 print(f"\n[serving] {loop} loop, {mode}: {st.qps:.0f} QPS, p50 {st.p50_ms:.2f} ms, "
                       f"p99 {st.p99_ms:.2f} ms, overflow reruns {st.overflow_reruns}")
+        # results delivered to per-worker buffers (pageable / pinned, range by range through a buffer
+        # smaller than the largest result) and digested as they arrive: the digests of the results alone
+        want = {p.qr.qid: S.digest(p.plan, *alone[p.qr.qid]) for p in prepared}
+        big = max(rows.values())
+        for mode in ("plain", "batched"):
+            st = S.run_native(tables, prepared, arrays, mode, keep_results=False, arena_bytes=big * 40, checksum=True)
+            for p in prepared:
+                r = st.results[p.qr.qid]
+                c, f = want[p.qr.qid]
+                assert r.groups == rows[p.qr.qid] and r.checksum == c
+                assert abs(r.fsum - f) <= 1e-9 * max(abs(f), 1e-300)
+            print(f"\n[serving] native loop, {mode}, results to per-worker buffers: {st.qps:.0f} QPS, "
+                  f"p50 {st.p50_ms:.2f} ms, p99 {st.p99_ms:.2f} ms")
     finally:
         ops.jit_set_mode(-1)
         for t in tables:

@@ -51,7 +51,7 @@ SIGNATURES = {
     "ws_agg_overflowed": (C.c_int, [P, C.POINTER(C.c_int)]),
     "ws_agg_group_count": (C.c_int, [P, I64P]),
     "ws_agg_fetch": (C.c_int, [P, C.c_int64, P, P, P, I64P]),
-    "ws_agg_fetch_async": (C.c_int, [P, C.c_int64, P, P, P]),
+    "ws_agg_fetch_async": (C.c_int, [P, C.c_int64, C.c_int64, P, P, P]),
     "ws_agg_sum_bits_slots": (C.c_int, [P, P]),
     "ws_agg_sum_high": (C.c_int, [P, P]),
     "ws_agg_compact": (C.c_int, [P, C.POINTER(P), C.POINTER(P), I64P]),
@@ -83,7 +83,7 @@ SIGNATURES = {
     "ws_hll_sketch": (C.c_int, [C.POINTER(abi.ExprEnv), C.c_int, C.POINTER(abi.AggPlan), C.c_int, P, P, P, C.c_int,
                                 C.c_int64, P, I64P, I64P]),
     "ws_mlp_infer": (C.c_int, [P, C.c_int, C.c_int, C.c_int, P, P, P, P, P, C.c_float, P]),
-    "ws_serve": (C.c_int, [P, C.c_int, C.c_int, C.c_int64, P, C.POINTER(C.c_double)]),
+    "ws_serve": (C.c_int, [P, C.c_int, P, C.POINTER(C.c_double)]),
     "ws_jit_set_mode": (C.c_int, [C.c_int]),
     "ws_jit_mode": (C.c_int, []),
     "ws_jit_set_default_mode": (C.c_int, [C.c_int]),

@@ -95,7 +95,13 @@ class ServeQuery(C.Structure):
                 ("key_range", C.c_double), ("arrival_s", C.c_double), ("footprint", C.c_int64),
                 ("max_groups", C.c_int64), ("keys", C.c_void_p), ("accs", C.c_void_p), ("exact", C.c_void_p),
                 ("start_s", C.c_double), ("finish_s", C.c_double), ("runs", C.c_int), ("cap_used", C.c_int64),
-                ("groups", C.c_int64)]
+                ("groups", C.c_int64), ("checksum", C.c_uint64), ("fsum", C.c_double)]
+
+
+class ServeOptions(C.Structure):
+    """ws_serve_options (include/ws_b200.h)."""
+    _fields_ = [("slots", C.c_int), ("hbm_budget", C.c_int64), ("est", C.c_void_p), ("one_sync", C.c_int),
+                ("arena_bytes", C.c_int64), ("checksum", C.c_int)]
 
 
 class FetchStatus(C.Structure):

@@ -189,17 +189,19 @@ __global__ void kEmit(const u64* rows, const int64_t* idx, int64_t m, EmitSpec s
   }
 }
 
-// Fetch straight into host memory (pinned and mapped): the groups of chunk b of kOccChunk result rows
-// go to rows offs[b].. in ascending row order, one sub-tile of blockDim result rows at a time, each
-// sub-tile's rows staged in shared memory ([blockDim][nk + 2 na] words) and stored as contiguous words
-// (whole PCIe writes rather than one 8-byte write per word of a row).  Nothing is written when the run
-// raised a flag (hash overflow, dense key out of range, staged-copy timeout) or the groups exceed
-// maxGroups: the caller reads the status and reruns or grows its buffers.
+// Fetch straight into host memory (pinned and mapped): group p (ascending result-row order; the groups
+// of chunk b of kOccChunk result rows are offs[b]..) goes to output row p - first when first <= p <
+// first + limit.  One sub-tile of blockDim result rows at a time, its rows staged in shared memory
+// ([blockDim][nk + 2 na] words) and stored as contiguous words (whole PCIe writes rather than one
+// 8-byte write per word of a row).  Nothing is written when the run raised a flag (hash overflow, dense
+// key out of range, staged-copy timeout): the caller reads the status and reruns.
 __global__ void kOccEmitHost(const u64* rows, int64_t nrows, OccSpec o, EmitSpec s, const int64_t* offs, int64_t nchunks,
-                             const int* err, int64_t maxGroups, double* keys, long long* exact) {
+                             const int* err, int64_t first, int64_t limit, double* keys, long long* exact) {
   extern __shared__ long long stg[];
   __shared__ int wbase[32];
-  if (err[0] || err[2] || (o.mode == 2 && err[1]) || offs[nchunks] > maxGroups) return;
+  if (err[0] || err[2] || (o.mode == 2 && err[1])) return;
+  if (offs[blockIdx.x + 1] <= first || offs[blockIdx.x] >= first + limit) return;  // none of this chunk's groups
+  const int64_t last = first + limit;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int xw = 2 * s.na, rw = s.nk + xw;
   const int64_t c0 = (int64_t)blockIdx.x * kOccChunk, cend = min(c0 + kOccChunk, nrows);
@@ -220,9 +222,13 @@ __global__ void kOccEmitHost(const u64* rows, int64_t nrows, OccSpec o, EmitSpec
       emitRow(rows, i, s, (double*)r, 1, r + s.nk);
     }
     __syncthreads();
-    for (int t = threadIdx.x; t < total * s.nk; t += blockDim.x)
-      keys[run * s.nk + t] = __longlong_as_double(stg[(t / s.nk) * rw + t % s.nk]);
-    for (int t = threadIdx.x; t < total * xw; t += blockDim.x) exact[run * xw + t] = stg[(t / xw) * rw + s.nk + t % xw];
+    // this sub-tile's groups [run, run + total) clipped to [first, last), at output row p - first
+    const int lo = (int)min((int64_t)total, max((int64_t)0, first - run));
+    const int hi = (int)max((int64_t)lo, min((int64_t)total, last - run));
+    for (int t = lo * s.nk + threadIdx.x; t < hi * s.nk; t += blockDim.x)
+      keys[(run - first) * s.nk + t] = __longlong_as_double(stg[(t / s.nk) * rw + t % s.nk]);
+    for (int t = lo * xw + threadIdx.x; t < hi * xw; t += blockDim.x)
+      exact[(run - first) * xw + t] = stg[(t / xw) * rw + s.nk + t % xw];
     run += total;
     __syncthreads();
   }
@@ -443,6 +449,9 @@ struct ws_aggregator {
   DBuf<double> cachedKeys, cachedAccs;
   DBuf<int64_t> cachedExact;
   std::vector<int64_t> cachedHi;
+  // groups before each chunk of kOccChunk result rows (ws_agg_fetch_async), until the next run
+  DBuf<int64_t> fetchOffs;
+  bool fetchOffsValid = false;
 
   u64* count() { return (u64*)ctl.p; }
   int* err() { return (int*)(ctl.p + 8); }
@@ -504,6 +513,7 @@ static void aggRun(ws_aggregator& A, const ws_expr_env& env, const ws_jit_progra
   A.fetched = false;
   A.lastGroups = -1;
   A.cachedGroups = -1;
+  A.fetchOffsValid = false;
   const bool useJit = jit && jit->state.load() == 1 && planCovers(env, nb, A.ncols, A.bcols.data());
   if (!useJit && (A.plan.naggs > WS_INTERP_AGGS || A.plan.nkeys > WS_INTERP_KEYS))
     throw Error("this aggregation needs a compiled plan (more than 16 aggregates or 4 GROUP BY keys); codegen failed or is off", WS_ERR_PLAN);
@@ -805,7 +815,8 @@ int ws_agg_fetch(ws_aggregator* A, int64_t max_groups, double* keys, double* acc
   });
 }
 
-int ws_agg_fetch_async(ws_aggregator* A, int64_t max_groups, double* keys, int64_t* exact, ws_fetch_status* status) {
+int ws_agg_fetch_async(ws_aggregator* A, int64_t first_group, int64_t max_groups, double* keys, int64_t* exact,
+                       ws_fetch_status* status) {
   return guardedCall([&] {
     const int nk = A->plan.nkeys, na = A->plan.naggs;
     auto mapped = [](void* h, const char* what) -> void* {
@@ -820,18 +831,24 @@ int ws_agg_fetch_async(ws_aggregator* A, int64_t max_groups, double* keys, int64
     auto* st = (ws_fetch_status*)mapped(status, "status");
     double* dk = nk ? (double*)mapped(keys, "keys") : nullptr;
     auto* dx = (long long*)mapped(exact, "exact");
+    if (first_group < 0 || max_groups < 0) throw Error("fetch_async: negative group range", WS_ERR_ARG);
     const int64_t nr = A->nrows();
     OccSpec o{A->lay.rw, nk == 0 ? 0 : A->isDense ? 1 : 2, A->lay.woff[0], A->cap};
     const int64_t nchunks = (nr + kOccChunk - 1) / kOccChunk;
-    DBuf<int64_t> counts(nchunks + 1);
-    WS_LAUNCH(kOccCount, (unsigned)nchunks, 256, 0, A->rows.p, nr, o, counts.p);
-    WS_LAUNCH(kScanExclusive, 1, 1024, 0, counts.p, nchunks);
-    WS_LAUNCH(kFetchStatus, 1, 1, 0, counts.p + nchunks, A->err(), o.mode == 2 ? 1 : 0, st);
+    if (!A->fetchOffsValid) {  // group offsets per chunk, kept for the later ranges of the same run
+      A->fetchOffs = DBuf<int64_t>(nchunks + 1);
+      WS_LAUNCH(kOccCount, (unsigned)nchunks, 256, 0, A->rows.p, nr, o, A->fetchOffs.p);
+      WS_LAUNCH(kScanExclusive, 1, 1024, 0, A->fetchOffs.p, nchunks);
+      A->fetchOffsValid = true;
+    }
+    const int64_t* counts = A->fetchOffs.p;
+    WS_LAUNCH(kFetchStatus, 1, 1, 0, counts + nchunks, A->err(), o.mode == 2 ? 1 : 0, st);
+    if (max_groups == 0) return;
     // sub-tile rows: staging of at most 32 KB, a multiple of 32 rows
     const int rowBytes = 8 * (nk + 2 * na);
     const int threads = std::max(32, std::min(256, (32768 / rowBytes) & ~31));
     WS_LAUNCH(kOccEmitHost, (unsigned)nchunks, threads, (size_t)threads * rowBytes, A->rows.p, nr, o, emitSpec(*A),
-              counts.p, nchunks, A->err(), max_groups, dk, dx);
+              counts, nchunks, A->err(), first_group, max_groups, dk, dx);
     A->cachedGroups = -1;
     A->fetched = true;
   });

@@ -82,11 +82,58 @@ bool pinnedHost(const void* p) {
   return at.type == cudaMemoryTypeHost && at.devicePointer;
 }
 
-// One query on the calling thread's stream.  Results into pinned host arrays (keys / exact, no accs)
-// take the one-sync form: run, compaction and the kernel that writes the groups into host memory are
-// queued back to back, and the thread waits once; otherwise the engine's sequence (overflow check,
-// group count, compaction, copies), which waits at each step.
-void serveOne(ws_serve_query& q, const ws_estimator_weights* w, ws_fetch_status* st) {
+uint64_t mix64h(uint64_t z) {  // splitmix64 finalizer
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// Order-independent digest of delivered groups: the sum over groups of a hash of the group's key bits
+// and exact words, DOUBLE SUM slots left out (their last bits depend on the order of the additions);
+// those are added up separately.
+void digest(const ws_agg_plan& plan, const double* keys, const int64_t* exact, int64_t rows, ws_serve_query& q) {
+  const int nk = plan.nkeys, na = plan.naggs;
+  for (int64_t r = 0; r < rows; ++r) {
+    uint64_t h = 0x9E3779B97F4A7C15ull;
+    for (int k = 0; k < nk; ++k) {
+      uint64_t b;
+      std::memcpy(&b, keys + r * nk + k, 8);
+      h = mix64h(h ^ b);
+    }
+    const int64_t* x = exact + r * na * 2;
+    for (int a = 0; a < na; ++a) {
+      if (plan.ops[a] == WS_AGG_SUM && !plan.aggInt[a]) {
+        double d;
+        std::memcpy(&d, x + 2 * a, 8);
+        q.fsum += d;
+        continue;
+      }
+      h = mix64h(h ^ (uint64_t)x[2 * a]);
+      h = mix64h(h ^ (uint64_t)x[2 * a + 1]);
+    }
+    q.checksum += h;
+  }
+}
+
+// A worker thread's result buffers for queries without result arrays (arena mode): pinned, delivered
+// range by range, in the one-sync form; pageable, grown to the largest result, otherwise.
+struct Arena {
+  uint8_t* pinned = nullptr;
+  int64_t bytes = 0;
+  std::vector<uint8_t> host;
+};
+
+void growTo(std::vector<uint8_t>& v, size_t bytes) {
+  if (v.size() < bytes) v.resize(bytes);
+}
+
+// One query on the calling thread's stream.
+//  one-sync form (st != null): run, compaction and the kernel that writes the groups into pinned host
+//    memory are queued back to back and the thread waits once per run (per range for results larger
+//    than the arena);
+//  otherwise the engine's sequence: overflow check, group count, compaction, copies, each a wait.
+void serveOne(ws_serve_query& q, const ws_serve_options& o, ws_fetch_status* st, Arena& ar) {
+  const ws_estimator_weights* w = o.est;
   int64_t cap = q.cap_plain;
   if (w && cap > (1 << 16)) {
     std::vector<uint32_t> regs(1u << 12);
@@ -101,7 +148,12 @@ void serveOne(ws_serve_query& q, const ws_estimator_weights* w, ws_fetch_status*
     const double pred = std::exp2((double)x[8] + (double)y) - 1;
     cap = std::min(cap, pow2AtLeast(2 * pred * w->margin, 1024));
   }
+  const int nk = q.plan->nkeys, na = q.plan->naggs;
+  const int64_t rowBytes = 8 * (nk + 2 * na);
+  const bool arena = !q.keys && !q.accs && !q.exact && o.arena_bytes > 0;
   q.runs = 0;
+  q.checksum = 0;
+  q.fsum = 0;
   for (;;) {
     ++q.runs;
     ws_aggregator* a = nullptr;
@@ -109,18 +161,34 @@ void serveOne(ws_serve_query& q, const ws_estimator_weights* w, ws_fetch_status*
     int rc = ws_agg_add_batches(a, q.ncols, q.nb, q.bn, q.bdel, q.bcols);
     if (!rc) rc = ws_agg_run(a, q.env, q.jit);
     if (st) {
-      if (!rc) rc = ws_agg_fetch_async(a, q.max_groups, q.keys, q.exact, st);
-      if (!rc) rc = ws_gpu_sync();
+      // destination: the caller's arrays, or the arena range by range
+      const int64_t per = arena ? std::max<int64_t>(1, ar.bytes / rowBytes) : q.max_groups;
+      double* dk = arena ? (double*)ar.pinned : q.keys;
+      int64_t* dx = arena ? (int64_t*)(ar.pinned + per * 8 * nk) : q.exact;
+      int64_t first = 0, groups = 0;
+      for (;;) {
+        if (!rc) rc = ws_agg_fetch_async(a, first, per, dk, dx, st);
+        if (!rc) rc = ws_gpu_sync();
+        if (rc) break;
+        if (st->error || st->overflow) break;
+        groups = st->groups;
+        const int64_t got = std::max<int64_t>(0, std::min(per, groups - first));
+        if (o.checksum) digest(*q.plan, dk, dx, got, q);
+        first += per;
+        if (!arena || first >= groups) break;
+      }
       ws_agg_destroy(a);
       checkRc(rc);
       if (st->error) throw ws::Error("serve: the aggregation raised an error flag", st->error);
       if (st->overflow) {
         cap = grow(cap, st->groups);
+        q.checksum = 0;
+        q.fsum = 0;
         continue;
       }
-      if (st->groups > q.max_groups)
-        throw ws::Error("output buffer too small for " + std::to_string(st->groups) + " groups", WS_ERR_SIZE);
-      q.groups = st->groups;
+      if (!arena && groups > q.max_groups)
+        throw ws::Error("output buffer too small for " + std::to_string(groups) + " groups", WS_ERR_SIZE);
+      q.groups = groups;
       q.cap_used = cap;
       return;
     }
@@ -134,9 +202,22 @@ void serveOne(ws_serve_query& q, const ws_estimator_weights* w, ws_fetch_status*
       cap = grow(cap, g);
       continue;
     }
-    int64_t g = 0;  // without result arrays the groups stay on the device (compacted, not downloaded)
-    const bool keep = q.keys || q.accs || q.exact;
-    if (!rc) rc = ws_agg_fetch(a, keep ? q.max_groups : INT64_MAX, q.keys, q.accs, q.exact, &g);
+    int64_t g = 0;
+    if (arena) {  // the engine's fetch into this worker's host buffer: size query, then the copies
+      if (!rc) rc = ws_agg_fetch(a, 0, nullptr, nullptr, nullptr, &g);
+      if (rc == WS_ERR_SIZE) rc = 0;
+      if (!rc) {
+        growTo(ar.host, (size_t)(g * rowBytes));
+        double* hk = (double*)ar.host.data();
+        int64_t* hx = (int64_t*)(ar.host.data() + g * 8 * nk);
+        rc = ws_agg_fetch(a, g, nk ? hk : nullptr, nullptr, hx, &g);
+        if (!rc && o.checksum) digest(*q.plan, hk, hx, g, q);
+      }
+    } else {  // without result arrays or an arena the groups stay on the device (compacted, not downloaded)
+      const bool keep = q.keys || q.accs || q.exact;
+      if (!rc) rc = ws_agg_fetch(a, keep ? q.max_groups : INT64_MAX, q.keys, q.accs, q.exact, &g);
+      if (!rc && keep && o.checksum && q.exact && (q.keys || !nk)) digest(*q.plan, q.keys, q.exact, g, q);
+    }
     ws_agg_destroy(a);
     checkRc(rc);
     q.groups = g;
@@ -149,10 +230,11 @@ void serveOne(ws_serve_query& q, const ws_estimator_weights* w, ws_fetch_status*
 
 extern "C" {
 
-int ws_serve(ws_serve_query* queries, int n, int slots, int64_t hbm_budget, const ws_estimator_weights* est,
-             double* wall_s) {
+int ws_serve(ws_serve_query* queries, int n, const ws_serve_options* opt, double* wall_s) {
   return ws::guardedCall([&] {
-    if (slots < 1 || slots > 256) throw ws::Error("serve: 1 to 256 slots", WS_ERR_ARG);
+    if (!opt) throw ws::Error("serve: options are null", WS_ERR_ARG);
+    const ws_serve_options o = *opt;
+    if (o.slots < 1 || o.slots > 256) throw ws::Error("serve: 1 to 256 slots", WS_ERR_ARG);
     ws_gpu_init();
     std::mutex mu;
     std::condition_variable cv;
@@ -160,20 +242,32 @@ int ws_serve(ws_serve_query* queries, int n, int slots, int64_t hbm_budget, cons
     std::atomic<int> next{0}, failed{0};
     std::string firstError;
     int firstCode = 0;
-    const double t0 = nowS();
-    auto worker = [&] {
-      cudaStream_t s = nullptr;
-      if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
-        failed = 1;
-        return;
-      }
-      ws_set_stream(s);
-      ws_fetch_status* st = nullptr;  // this worker's fetch status (pinned, for the one-sync form)
-      if (cudaHostAlloc((void**)&st, sizeof(ws_fetch_status), cudaHostAllocMapped) != cudaSuccess) {
+    auto fail = [&](const std::string& m, int code) {
+      std::lock_guard<std::mutex> l(mu);
+      if (!failed++) firstError = m, firstCode = code;
+    };
+    // per worker: a stream, the fetch status and the arena (allocated before the clock starts)
+    std::vector<cudaStream_t> streams(o.slots, nullptr);
+    std::vector<ws_fetch_status*> stat(o.slots, nullptr);
+    std::vector<Arena> arenas(o.slots);
+    for (int k = 0; k < o.slots && !failed; ++k) {
+      if (cudaStreamCreateWithFlags(&streams[k], cudaStreamNonBlocking) != cudaSuccess ||
+          (o.one_sync && cudaHostAlloc((void**)&stat[k], sizeof(ws_fetch_status), cudaHostAllocMapped) != cudaSuccess) ||
+          (o.one_sync && o.arena_bytes > 0 &&
+           cudaHostAlloc((void**)&arenas[k].pinned, (size_t)o.arena_bytes, cudaHostAllocMapped) != cudaSuccess)) {
         cudaGetLastError();
-        st = nullptr;
-        failed = 1;
+        fail("serve: could not create a worker's stream or pinned buffers", WS_ERR_OOM);
+        break;
       }
+      arenas[k].bytes = o.one_sync ? o.arena_bytes : 0;
+      if (!o.one_sync && o.arena_bytes > 0) {  // touched now, so that the loop does not fault the pages in
+        arenas[k].host.resize((size_t)o.arena_bytes);
+        std::memset(arenas[k].host.data(), 0, arenas[k].host.size());
+      }
+    }
+    const double t0 = nowS();
+    auto worker = [&](int k) {
+      ws_set_stream(streams[k]);
       for (;;) {
         const int i = next++;
         if (i >= n || failed) break;
@@ -182,17 +276,18 @@ int ws_serve(ws_serve_query* queries, int n, int slots, int64_t hbm_budget, cons
         if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(wait));
         {
           std::unique_lock<std::mutex> l(mu);  // admission by HBM footprint
-          cv.wait(l, [&] { return inFlight == 0 || inFlight + q.footprint <= hbm_budget; });
+          cv.wait(l, [&] { return inFlight == 0 || inFlight + q.footprint <= o.hbm_budget; });
           inFlight += q.footprint;
         }
         q.start_s = nowS() - t0;
         try {
-          const bool oneSync = (q.keys || !q.plan->nkeys) && q.exact && !q.accs && pinnedHost(q.exact) &&
-                               (!q.keys || pinnedHost(q.keys));
-          serveOne(q, est, oneSync ? st : nullptr);
+          const bool arrays = q.keys || q.accs || q.exact;
+          const bool oneSync = o.one_sync && (arrays ? (q.keys || !q.plan->nkeys) && q.exact && !q.accs &&
+                                                           pinnedHost(q.exact) && (!q.keys || pinnedHost(q.keys))
+                                                     : o.arena_bytes > 0);
+          serveOne(q, o, oneSync ? stat[k] : nullptr, arenas[k]);
         } catch (const ws::Error& e) {
-          std::lock_guard<std::mutex> l(mu);
-          if (!failed++) firstError = e.what(), firstCode = e.code;
+          fail(e.what(), e.code);
         }
         q.finish_s = nowS() - t0;
         {
@@ -202,16 +297,21 @@ int ws_serve(ws_serve_query* queries, int n, int slots, int64_t hbm_budget, cons
         cv.notify_all();
       }
       ws_set_stream(nullptr);
-      cudaStreamSynchronize(s);
-      cudaStreamDestroy(s);
-      if (st) cudaFreeHost(st);
     };
     std::vector<std::thread> th;
-    for (int k = 0; k < slots; ++k) th.emplace_back(worker);
+    if (!failed)
+      for (int k = 0; k < o.slots; ++k) th.emplace_back(worker, k);
     for (auto& t : th) t.join();
     if (wall_s) *wall_s = nowS() - t0;
-    if (failed) throw ws::Error(firstError.empty() ? "serve: a worker could not start" : firstError,
-                                firstCode ? firstCode : WS_ERR_INTERNAL);
+    for (int k = 0; k < o.slots; ++k) {
+      if (streams[k]) {
+        cudaStreamSynchronize(streams[k]);
+        cudaStreamDestroy(streams[k]);
+      }
+      if (stat[k]) cudaFreeHost(stat[k]);
+      if (arenas[k].pinned) cudaFreeHost(arenas[k].pinned);
+    }
+    if (failed) throw ws::Error(firstError, firstCode ? firstCode : WS_ERR_INTERNAL);
   });
 }
 

@@ -224,11 +224,13 @@ class GpuAggregator:
                                  ex.ctypes.data if exact else None, C.byref(g)))
         return keys, accs, ex
 
-    def fetch_async(self, max_groups: int, keys: "HostBuffer | None", exact: "HostBuffer", status: "HostBuffer"):
-        """Queues the groups' copy straight into pinned host buffers (ws_agg_fetch_async); they are valid
-        after sync().  status: a HostBuffer of FETCH_STATUS (groups, overflow, error)."""
-        check(lib().ws_agg_fetch_async(self.h, int(max_groups), keys.ptr if keys is not None else None, exact.ptr,
-                                       status.ptr))
+    def fetch_async(self, max_groups: int, keys: "HostBuffer | None", exact: "HostBuffer", status: "HostBuffer",
+                    first: int = 0):
+        """Queues the copy of groups [first, first + max_groups) straight into pinned host buffers
+        (ws_agg_fetch_async); they are valid after sync().  status: a HostBuffer of FETCH_STATUS
+        (all groups of the run, overflow, error)."""
+        check(lib().ws_agg_fetch_async(self.h, int(first), int(max_groups), keys.ptr if keys is not None else None,
+                                       exact.ptr, status.ptr))
 
     def sum_bits_slots(self) -> np.ndarray:
         out = np.zeros(self.plan.naggs, dtype=np.uint8)

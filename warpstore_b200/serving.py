@@ -104,6 +104,9 @@ class Result:
     finish: float = 0.0
     runs: int = 1
     cap: int = 0
+    checksum: int = 0      # digest of the delivered groups (ws_serve with checksum)
+    fsum: float = 0.0
+    groups: int = 0
 
 
 @dataclass
@@ -250,6 +253,26 @@ def run(tables: list, prepared: list, arrays: list, mode: str = "batched", slots
                  sum(r.runs - 1 for r in done), {r.qid: r for r in done})
 
 
+def digest(plan, keys: np.ndarray, exact: np.ndarray) -> tuple:
+    """(checksum, DOUBLE SUM total) of a query's groups, ws_serve's digest: the sum (mod 2^64) over the
+    groups of mix64 chained over the key bits and the exact words, DOUBLE SUM slots added up apart."""
+    from .estimator import mix64
+    g = exact.shape[0]
+    h = np.full(g, 0x9E3779B97F4A7C15, np.uint64)
+    kb = np.ascontiguousarray(keys).view(np.uint64).reshape(g, plan.nkeys) if plan.nkeys else None
+    for k in range(plan.nkeys):
+        h = mix64(h ^ kb[:, k])
+    fs = 0.0
+    ex = np.ascontiguousarray(exact).view(np.uint64)
+    for a in range(plan.naggs):
+        if plan.ops[a] == abi.AGG_SUM and not plan.aggInt[a]:
+            fs += float(ex[:, a, 0].view(np.float64).sum())
+            continue
+        h = mix64(h ^ ex[:, a, 0])
+        h = mix64(h ^ ex[:, a, 1])
+    return int(h.sum(dtype=np.uint64)), fs
+
+
 def run_alone(p: Prepared, arrays: list, learned: bool):
     """The query by itself on this thread (the reference result of the mix checks)."""
     keys, ex, _, _ = execute(p, arrays[p.qr.table], learned)
@@ -258,13 +281,17 @@ def run_alone(p: Prepared, arrays: list, learned: bool):
 
 def run_native(tables: list, prepared: list, arrays: list, mode: str = "batched", slots: int | None = None,
                hbm_budget: int = 8 << 30, keep_results: bool = True, result_rows: dict | None = None,
-               pinned: bool | None = None) -> Stats:
+               pinned: bool | None = None, arena_bytes: int = 0, checksum: bool = False) -> Stats:
     """The same serving loop in the library (ws_serve): C++ worker threads with a CUDA stream each,
-    no Python on the per-query path; the prepared queries' arrival times are honoured.  Results go to
-    host arrays allocated (and touched) before the loop: result_rows[qid] rows each when given, else
-    the key ranges' bound.  pinned (default: the batched form): the result arrays are pinned host
-    memory, so each query runs in the one-sync form (the GPU writes its groups into them); plain:
-    ordinary host arrays, the engine's fetch sequence."""
+    no Python on the per-query path; the prepared queries' arrival times are honoured.
+
+    keep_results: results go to host arrays allocated (and touched) before the loop, result_rows[qid]
+    rows each when given, else the key ranges' bound.  Otherwise, with arena_bytes, every worker
+    receives its queries' groups in a buffer of its own (reused query after query, as a server's send
+    buffer; checksum: each query's groups are digested as they arrive), else they stay on the device.
+    pinned (default: the batched form) selects the one-sync form: result arrays / arenas are pinned
+    host memory and the GPU writes the groups into them; plain: pageable memory and the engine's fetch
+    sequence."""
     import ctypes as C
 
     from . import estimator, ops
@@ -305,7 +332,9 @@ def run_native(tables: list, prepared: list, arrays: list, mode: str = "batched"
                                  hold[3].ctypes.data, hold[4].ctypes.data, float(m.b3), hold[5].ctypes.data,
                                  hold[6].ctypes.data, 2.0 ** float(m.meta.get("val_p90_log2_err", 0.0)))
     wall = C.c_double()
-    ops.check(ops.lib().ws_serve(qs, len(prepared), nslots, hbm_budget, C.byref(w) if w else None, C.byref(wall)))
+    opt = abi.ServeOptions(nslots, hbm_budget, C.addressof(w) if w else None, int(bool(pinned)),
+                           0 if keep_results else int(arena_bytes), int(bool(checksum)))
+    ops.check(ops.lib().ws_serve(qs, len(prepared), C.byref(opt), C.byref(wall)))
     lat = np.array([(q.finish_s - q.arrival_s) * 1e3 for q in qs])
     span = max(q.finish_s for q in qs) - min(q.arrival_s for q in qs)
     results = {}
@@ -314,6 +343,73 @@ def run_native(tables: list, prepared: list, arrays: list, mode: str = "batched"
         k, x = keep[i][:2] if keep[i] is not None else (None, None)
         results[p.qr.qid] = Result(p.qr.qid, k[:q.groups].copy() if k is not None else None,
                                    x[:q.groups].copy() if x is not None else None, q.arrival_s, q.start_s, q.finish_s,
-                                   q.runs, q.cap_used)
+                                   q.runs, q.cap_used, int(q.checksum), float(q.fsum), int(q.groups))
     return Stats(mode, len(prepared) / span, float(np.percentile(lat, 50)), float(np.percentile(lat, 99)),
                  len(prepared), sum(q.runs - 1 for q in qs), results)
+
+
+def main():
+    """Serving measurement: both forms over the same tables and arrivals, each query's groups delivered
+    to a per-worker buffer and digested, the digests of the two forms compared query by query (DOUBLE
+    SUM totals within 1e-9 relative, the rest exact).  One JSON line per form and repeat.
+
+        python -m warpstore_b200.serving [--tables 64] [--max-rows 5e7] [--queries 10000] [--rate 2000]
+    """
+    import argparse
+    import json
+
+    import torch
+
+    from . import ops
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--tables", type=int, default=64)
+    ap.add_argument("--min-rows", type=float, default=1e4)
+    ap.add_argument("--max-rows", type=float, default=5e7)
+    ap.add_argument("--queries", type=int, default=10_000)
+    ap.add_argument("--rate", type=float, default=2000.0)
+    ap.add_argument("--repeats", type=int, default=2)
+    ap.add_argument("--arena-mb", type=int, default=256, help="per-worker result buffer")
+    ap.add_argument("--hbm-gb", type=float, default=8.0, help="admission budget")
+    a = ap.parse_args()
+    t0 = time.perf_counter()
+    tables = make_tables(a.tables, int(a.min_rows), int(a.max_rows), seed=5)
+    for t in tables:
+        t.to_device()
+    queries = make_queries(tables, a.queries, rate=a.rate, seed=6)
+    prepared, arrays = prepare(tables, queries)
+    rows = sum(t.n for t in tables)
+    setup_s = time.perf_counter() - t0
+    ops.jit_set_mode(abi.JIT_SYNC)
+    kw = dict(keep_results=False, arena_bytes=a.arena_mb << 20, checksum=True, hbm_budget=int(a.hbm_gb * 2 ** 30))
+    try:
+        run_native(tables, prepared[:200], arrays, "batched", **kw)  # warm: pools, pinned buffers, weights
+        run_native(tables, prepared[:200], arrays, "plain", **kw)
+        ref = None
+        for rep in range(a.repeats):
+            for mode in ("plain", "batched"):
+                torch.cuda.synchronize()
+                st = run_native(tables, prepared, arrays, mode, **kw)
+                dig = {qid: (r.checksum, r.fsum, r.cap) for qid, r in st.results.items()}
+                same = None
+                if ref is not None:
+                    same = all(dig[q][0] == ref[q][0] and abs(dig[q][1] - ref[q][1]) <= 1e-9 * max(abs(ref[q][1]), 1e-300)
+                               for q in ref)
+                else:
+                    ref = dig
+                print(json.dumps({"form": mode, "repeat": rep, "qps": round(st.qps, 1), "p50_ms": round(st.p50_ms, 3),
+                                  "p99_ms": round(st.p99_ms, 3), "completed": st.completed,
+                                  "overflow_reruns": st.overflow_reruns,
+                                  "groups": int(sum(r.groups for r in st.results.values())),
+                                  "digests_equal_first_run": same,
+                                  "config": {"tables": a.tables, "rows": rows, "queries": a.queries,
+                                             "rate_per_s": a.rate, "arena_mb": a.arena_mb,
+                                             "slots": 16 if mode == "batched" else 4, "setup_s": round(setup_s, 1)}}),
+                      flush=True)
+    finally:
+        ops.jit_set_mode(-1)
+        for t in tables:
+            t.free_device()
+
+
+if __name__ == "__main__":
+    main()
