@@ -201,6 +201,23 @@ int ws_hll_sketch(const ws_expr_env* env, int ncols, const ws_agg_plan* plan, in
 int ws_mlp_infer(const float* x, int rows, int features, int hidden, const uint16_t* w1_bf16, const float* b1,
                  const uint16_t* w2_bf16, const float* b2, const uint16_t* w3_bf16, float b3, float* y);
 
+/* ---- launch-shape autotuner (no counterpart in the reference, whose launch shapes are fixed,
+ * src/gpu.cu:393-653).  Per (scan kernel, plan, size class = log2 of the scan's tiles): the CTAs per
+ * SM of the persistent grid and, for the hash scan, the per-CTA shared table's budget.  WS_TUNE_ON: a
+ * key seen for the first time is tuned inside ws_agg_run on the query's own batches (each candidate
+ * timed on the calling stream after resetting the result rows; the fastest is kept and the final run
+ * uses it, so results never depend on tuning); WS_TUNE_USE (default): recorded choices are used,
+ * others get the default shape; WS_TUNE_OFF: default shapes.  The table is kept in memory and in the
+ * plan-cache directory (ws_jit_set_cache_dir).  Only fresh aggregators (no earlier window) tune. */
+#define WS_TUNE_USE 0
+#define WS_TUNE_ON 1
+#define WS_TUNE_OFF 2
+int ws_tune_set_mode(int mode);
+/* The table as text, one line per key: `key ctas_per_sm smem_kb microseconds`. */
+int ws_tune_table(char* buf, size_t size, size_t* needed);
+int ws_tune_load(const char* text);   /* adds / replaces entries from such text */
+int ws_tune_clear(void);
+
 /* ---- request loop (no counterpart in the reference, whose connections each run their query
  * synchronously): prepared GROUP BY queries served by `slots` host threads with a CUDA stream each,
  * in arrival order, admitted while the footprints of the queries in flight fit hbm_budget.
@@ -287,7 +304,7 @@ typedef struct ws_jit_query_info {
 int ws_jit_set_mode(int mode);          /* this thread: WS_JIT_OFF / ON / SYNC */
 int ws_jit_mode(void);
 int ws_jit_set_default_mode(int mode);
-int ws_jit_set_cache_dir(const char* dir);
+int ws_jit_set_cache_dir(const char* dir);  /* also holds the autotuner's table (wsb200_tune.txt) */
 /* The compiled plan for `fn` over the plan's expressions (nullptr in *out: run interpreted). */
 int ws_jit_get(const ws_expr_env* env, int ncols, const ws_agg_plan* plan, int fn, const char* kind,
                const ws_jit_program** out);

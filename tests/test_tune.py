@@ -1,0 +1,30 @@
+"""The launch-shape autotuner's table (no GPU): text round trip, later entries replace earlier ones,
+malformed lines and modes are refused."""
+import ctypes as C
+
+from warpstore_b200 import ops
+
+
+def table() -> str:
+    need = C.c_size_t()
+    ops.lib().ws_tune_table(None, 0, C.byref(need))
+    buf = C.create_string_buffer(need.value)
+    assert ops.lib().ws_tune_table(buf, need.value, C.byref(need)) == 0
+    return buf.value.decode()
+
+
+def test_table_round_trip():
+    lib = ops.lib()
+    assert lib.ws_tune_clear() == 0
+    assert table() == ""
+    text = "hash:q0123456789abcdef:t10 0 32 812.5\ndense_priv:qfedcba9876543210:t16 1 0 850.0\n"
+    assert lib.ws_tune_load(text.encode()) == 0
+    assert sorted(table().splitlines()) == sorted(text.splitlines())
+    assert lib.ws_tune_load(b"hash:q0123456789abcdef:t10 2 0 700.0\n") == 0   # replaces the entry
+    assert "hash:q0123456789abcdef:t10 2 0 700.0" in table().splitlines()
+    assert len(table().splitlines()) == 2
+    assert lib.ws_tune_load(b"not a line\n") == 1210
+    assert lib.ws_tune_load(b"hash:x:t1 999 0 1.0\n") == 1210                 # CTAs per SM out of range
+    assert lib.ws_tune_set_mode(7) == 1210
+    assert lib.ws_tune_set_mode(0) == 0
+    assert lib.ws_tune_clear() == 0

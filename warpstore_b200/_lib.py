@@ -84,6 +84,10 @@ SIGNATURES = {
                                 C.c_int64, P, I64P, I64P]),
     "ws_mlp_infer": (C.c_int, [P, C.c_int, C.c_int, C.c_int, P, P, P, P, P, C.c_float, P]),
     "ws_serve": (C.c_int, [P, C.c_int, P, C.POINTER(C.c_double)]),
+    "ws_tune_set_mode": (C.c_int, [C.c_int]),
+    "ws_tune_table": (C.c_int, [C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "ws_tune_load": (C.c_int, [C.c_char_p]),
+    "ws_tune_clear": (C.c_int, []),
     "ws_jit_set_mode": (C.c_int, [C.c_int]),
     "ws_jit_mode": (C.c_int, []),
     "ws_jit_set_default_mode": (C.c_int, [C.c_int]),

@@ -606,12 +606,14 @@ int ws_jit_set_cache_dir(const char* dir) {
     std::lock_guard<std::mutex> g(gMu);
     if (!dir || !*dir) {
       gDiskDir.clear();
+      tuneSetDir("");
       return;
     }
     std::error_code ec;
     std::filesystem::create_directories(dir, ec);
     gDiskDir = ec ? "" : dir;
     if (ec) throw Error(std::string("plan cache directory unusable: ") + ec.message(), WS_ERR_ARG);
+    tuneSetDir(gDiskDir);  // launch shapes tuned earlier for these plans
   });
 }
 

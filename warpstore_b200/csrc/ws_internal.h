@@ -58,6 +58,18 @@ void d2hSync(void* h, const void* d, size_t b);
 void d2hLarge(void* h, const void* d, size_t b);
 void sync();
 void countLaunch(int n = 1);     // kernels launched by this library (ws_kernel_launches)
+// Launch-shape autotuner (ws_tune.cpp): a scan's CTAs per SM (0: as many as fit) and, for the hash
+// scan, the per-CTA table's shared-memory budget in KB (0: the default).
+struct TuneChoice {
+  int ctasPerSm = 0;
+  int smemKB = 0;
+  bool found = false;
+};
+int tuneMode();  // WS_TUNE_USE / WS_TUNE_ON / WS_TUNE_OFF
+std::string tuneKey(const char* kernel, const ws_jit_program* jit, const ws_agg_plan& plan, int64_t ntiles);
+bool tuneLookup(const std::string& key, TuneChoice& c);
+void tuneStore(const std::string& key, const TuneChoice& c, double us);
+void tuneSetDir(const std::string& dir);  // "" : memory only
 void setStream(cudaStream_t s);
 // Runs f, translating exceptions into the calling thread's last error; returns the error code.
 int guardedCall(const std::function<void()>& f);

@@ -488,17 +488,26 @@ static RowTemplate rowTemplate(const SlotLayout& lay) {
   return t;
 }
 
+// Result rows to their identities (hash rows empty) and the control words (count, flags, ticket) to 0.
+static void aggResetRows(ws_aggregator& A) {
+  const int64_t nr = A.nrows();
+  const int64_t emptyRows = A.plan.nkeys && !A.isDense ? A.cap : 0;
+  WS_LAUNCH(kFillRows, gridFor(nr), 256, 0, A.rows.p, nr, A.lay.rw, rowTemplate(A.lay), emptyRows);
+  WS_CK(cudaMemsetAsync(A.ctl.p, 0, 32, stream()));
+}
+
 static void aggInitRows(ws_aggregator& A) {
   const int64_t nr = A.nrows();
   A.rows = DBuf<u64>(nr * A.lay.rw);
-  const int64_t emptyRows = A.plan.nkeys && !A.isDense ? A.cap : 0;
-  WS_LAUNCH(kFillRows, gridFor(nr), 256, 0, A.rows.p, nr, A.lay.rw, rowTemplate(A.lay), emptyRows);
   if (A.plan.nkeys && !A.isDense) {
     A.tkeys = DBuf<double>((A.cap + 1) * std::max(A.plan.nkeys, 1));
   }
   A.ctl = DBuf<uint8_t>(32);
-  WS_CK(cudaMemsetAsync(A.ctl.p, 0, 32, stream()));
+  aggResetRows(A);
 }
+
+static TuneChoice tuneScan(ws_aggregator& A, const std::string& key, const std::vector<TuneChoice>& cands,
+                           const std::function<void(const TuneChoice&)>& launch);
 
 static size_t hashSmemSlots(const ws_aggregator& A, size_t budget) {
   const size_t per = (size_t)A.lay.rw * 8 + (A.plan.nkeys > 1 ? (size_t)A.plan.nkeys * 8 : 0);
@@ -539,19 +548,34 @@ static void aggRun(ws_aggregator& A, const ws_expr_env& env, const ws_jit_progra
   }();
   const int S = stageBytes > 0 ? (int)std::min<int64_t>(maxStages, (200 * 1024) / stageBytes) : 0;
   const size_t stageSmem = S >= 2 ? (size_t)S * stageBytes : 0;
+  // The scan's launch shape as a function of a tuning choice: kernel, shared memory, block size and
+  // the launch fields the shape changes.  Per-CTA partial rows (`part`: no-key and private-row scans)
+  // are sized by the grid.
+  struct Shape {
+    CUfunction f = nullptr;
+    size_t smem = 0;
+    int threads = kThreads;
+  };
+  std::function<Shape(const TuneChoice&)> shapeOf;
+  const char* name = "";
+  int64_t partRows = 0;  // rows of `part` per CTA (0: none)
+  std::vector<TuneChoice> cands(1);  // candidates for the autotuner; [0] = the default shape
+  auto ctas = [](int c) {
+    TuneChoice t;
+    t.ctasPerSm = c;
+    return t;
+  };
   if (A.plan.nkeys == 0) {
     CUfunction f = ks.fn[K_NOKEYS];
     if (!f) throw Error("compiled plan has no aggregation kernel", WS_ERR_INTERNAL);
     L.stages = S >= 2 ? S : 0;
     const int threads = L.stages ? kStagedThreads : kThreads;
-    const unsigned grid = persistentGrid(f, stageSmem, d.ntiles, threads);
-    DBuf<u64> part((int64_t)grid * A.lay.rw);
-    L.part = part.p;
-    WS_CK(cudaMemsetAsync(A.ticket(), 0, 4, stream()));
-    launchScan(f, grid, stageSmem, L, threads);
-    return;
-  }
-  if (A.isDense) {
+    shapeOf = [=](const TuneChoice&) { return Shape{f, stageSmem, threads}; };
+    name = "nokeys";
+    partRows = 1;
+    cands.push_back(ctas(2));
+    cands.push_back(ctas(1));
+  } else if (A.isDense) {
     for (int k = 0; k < A.plan.nkeys; ++k) {
       L.kmin[k] = A.dense.kmin[k];
       L.range[k] = A.dense.range[k];
@@ -563,6 +587,7 @@ static void aggRun(ws_aggregator& A, const ws_expr_env& env, const ws_jit_progra
     // private rows [G][frw][kThreads] + int128 spill counters [G][NA][2] (NA: the evaluator's slot bound)
     const int naEv = ks.interp ? WS_INTERP_AGGS : A.plan.naggs;
     const size_t privBytes = (size_t)G * A.lay.frw * kThreads * 8 + (size_t)G * naEv * 16;
+    const size_t sharedSmem = (size_t)G * A.lay.rw * 8;
     if (G * A.lay.frw <= 48 && ks.fn[K_DENSE_PRIV]) {
       const size_t budget = 220 * 1024;
       int S2 = stageBytes > 0 ? (int)std::min<int64_t>(maxStages, (int64_t)(budget - privBytes) / stageBytes) : 0;
@@ -571,38 +596,116 @@ static void aggRun(ws_aggregator& A, const ws_expr_env& env, const ws_jit_progra
       L.stages = S2;
       const int threads = S2 ? kStagedThreads : kThreads;
       const size_t smem = (size_t)S2 * stageBytes + privBytes;
-      const unsigned grid = persistentGrid(f, smem, d.ntiles, threads);
-      DBuf<u64> part((int64_t)grid * G * A.lay.rw);
-      L.part = part.p;
-      WS_CK(cudaMemsetAsync(A.ticket(), 0, 4, stream()));
-      launchScan(f, grid, smem, L, threads);
-      return;
-    }
-    const size_t smem = (size_t)G * A.lay.rw * 8;
-    if (smem <= 96 * 1024 && ks.fn[K_DENSE_SHARED]) {
+      shapeOf = [=](const TuneChoice&) { return Shape{f, smem, threads}; };
+      name = "dense_priv";
+      partRows = G;
+      cands.push_back(ctas(1));
+    } else if (sharedSmem <= 96 * 1024 && ks.fn[K_DENSE_SHARED]) {
       CUfunction f = ks.fn[K_DENSE_SHARED];
-      launchScan(f, persistentGrid(f, smem, d.ntiles), smem, L);
+      shapeOf = [=](const TuneChoice&) { return Shape{f, sharedSmem, kThreads}; };
+      name = "dense_shared";
+      cands.push_back(ctas(2));
+      cands.push_back(ctas(1));
     } else {
       CUfunction f = ks.fn[K_DENSE_GLOBAL];
       if (!f) throw Error("compiled plan has no dense kernel", WS_ERR_INTERNAL);
-      launchScan(f, persistentGrid(f, 0, d.ntiles), 0, L);
+      shapeOf = [=](const TuneChoice&) { return Shape{f, 0, kThreads}; };
+      name = "dense_global";
+      cands.push_back(ctas(4));
+      cands.push_back(ctas(2));
     }
-    return;
+  } else {
+    CUfunction f = ks.fn[K_HASH];
+    if (!f) throw Error("compiled plan has no hash aggregation kernel", WS_ERR_INTERNAL);
+    L.table = A.rows.p;
+    L.tkeys = A.tkeys.p;
+    L.mask = (u64)(A.cap - 1);
+    L.count = A.count();
+    L.probeLimit = (int)std::min<int64_t>(A.cap, 1 << 16);
+    const size_t per = (size_t)A.lay.rw * 8 + (A.plan.nkeys > 1 ? (size_t)A.plan.nkeys * 8 : 0);
+    // spill buffer: up to a tile's rows, within 40 KB
+    L.spillRows = (int)std::min<size_t>(kTile, (40 * 1024) / per);
+    Launch* lp = &L;
+    ws_aggregator* ap = &A;
+    shapeOf = [=](const TuneChoice& c) {
+      // per-CTA table: up to 4096 slots within the budget (default 64 KB)
+      const size_t slots = hashSmemSlots(*ap, (size_t)(c.smemKB > 0 ? c.smemKB : 64) * 1024);
+      lp->smemSlots = (int)slots;
+      return Shape{f, (slots + (size_t)lp->spillRows) * per, kThreads};
+    };
+    name = "hash";
+    for (int kb : {32, 128}) {
+      TuneChoice t;
+      t.smemKB = kb;
+      cands.push_back(t);
+    }
+    cands.push_back(ctas(2));
   }
-  CUfunction f = ks.fn[K_HASH];
-  if (!f) throw Error("compiled plan has no hash aggregation kernel", WS_ERR_INTERNAL);
-  L.table = A.rows.p;
-  L.tkeys = A.tkeys.p;
-  L.mask = (u64)(A.cap - 1);
-  L.count = A.count();
-  L.probeLimit = (int)std::min<int64_t>(A.cap, 1 << 16);
-  const size_t slots = hashSmemSlots(A, 64 * 1024);
-  L.smemSlots = (int)slots;
-  const size_t per = (size_t)A.lay.rw * 8 + (A.plan.nkeys > 1 ? (size_t)A.plan.nkeys * 8 : 0);
-  // spill buffer: up to a tile's rows, within 40 KB
-  L.spillRows = (int)std::min<size_t>(kTile, (40 * 1024) / per);
-  const size_t smem = (slots + (size_t)L.spillRows) * per;
-  launchScan(f, persistentGrid(f, smem, d.ntiles), smem, L);
+  DBuf<u64> part;
+  int64_t partCap = 0;
+  auto launchOnce = [&](const TuneChoice& c) {
+    const Shape sh = shapeOf(c);
+    unsigned grid = persistentGrid(sh.f, sh.smem, d.ntiles, sh.threads);
+    if (c.ctasPerSm > 0) grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(grid, (int64_t)c.ctasPerSm * smCount()));
+    if (partRows) {
+      if ((int64_t)grid * partRows > partCap) {
+        partCap = (int64_t)grid * partRows;
+        part = DBuf<u64>(partCap * A.lay.rw);
+      }
+      L.part = part.p;
+      WS_CK(cudaMemsetAsync(A.ticket(), 0, 4, stream()));
+    }
+    launchScan(sh.f, grid, sh.smem, L, sh.threads);
+  };
+  const std::string key = tuneKey(name, useJit ? jit : nullptr, A.plan, d.ntiles);
+  TuneChoice choice;
+  if (!tuneLookup(key, choice) && tuneMode() == WS_TUNE_ON && A.windows == 0 && A.rowsDone == 0)
+    choice = tuneScan(A, key, cands, launchOnce);
+  launchOnce(choice);
+}
+
+// Times each candidate launch shape of a scan on the aggregation's own batches (best of two runs,
+// CUDA events on the calling stream, the result rows reset before each run) and records the fastest;
+// the rows are reset again for the caller's final run.  A run that raised a flag (overflow, key out of
+// range) records nothing: the final run raises it again and the caller decides.
+static TuneChoice tuneScan(ws_aggregator& A, const std::string& key, const std::vector<TuneChoice>& cands,
+                           const std::function<void(const TuneChoice&)>& launch) {
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  WS_CK(cudaEventCreate(&e0));
+  WS_CK(cudaEventCreate(&e1));
+  TuneChoice best;
+  double bestMs = 1e300;
+  bool flagged = false;
+  try {
+    for (const TuneChoice& c : cands) {
+      double ms = 1e300;
+      for (int rep = 0; rep < 2; ++rep) {
+        aggResetRows(A);
+        WS_CK(cudaEventRecord(e0, stream()));
+        launch(c);
+        WS_CK(cudaEventRecord(e1, stream()));
+        WS_CK(cudaEventSynchronize(e1));
+        float t = 0;
+        WS_CK(cudaEventElapsedTime(&t, e0, e1));
+        ms = std::min(ms, (double)t);
+      }
+      int e[3] = {0, 0, 0};
+      d2hSync(e, A.err(), 12);
+      flagged |= e[0] || e[1] || e[2];
+      if (ms < bestMs) bestMs = ms, best = c;
+    }
+  } catch (...) {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  aggResetRows(A);
+  if (flagged) return TuneChoice{};
+  tuneStore(key, best, bestMs * 1000);
+  best.found = true;
+  return best;
 }
 
 // Occupied row indices of the result rows (ascending), on the device; returns the count.

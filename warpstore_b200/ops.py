@@ -75,6 +75,32 @@ def sync():
     check(lib().ws_gpu_sync())
 
 
+TUNE_USE, TUNE_ON, TUNE_OFF = 0, 1, 2
+
+
+def tune_set_mode(mode: int):
+    """Launch-shape autotuner: TUNE_ON tunes unseen (kernel, plan, size class) keys inside ws_agg_run;
+    TUNE_USE applies recorded choices; TUNE_OFF uses the default shapes."""
+    check(lib().ws_tune_set_mode(int(mode)))
+
+
+def tune_table() -> dict:
+    """{key: (ctas per SM, shared KB, microseconds)} of the autotuner's table."""
+    need = C.c_size_t()
+    lib().ws_tune_table(None, 0, C.byref(need))
+    buf = C.create_string_buffer(need.value)
+    check(lib().ws_tune_table(buf, need.value, C.byref(need)))
+    out = {}
+    for line in buf.value.decode().splitlines():
+        k, c, m, us = line.split()
+        out[k] = (int(c), int(m), float(us))
+    return out
+
+
+def tune_clear():
+    check(lib().ws_tune_clear())
+
+
 def kernel_launches() -> int:
     return int(lib().ws_kernel_launches())
 
