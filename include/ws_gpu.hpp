@@ -157,6 +157,11 @@ class GpuAggregator {
     ws_agg_sum_high(h_, hi_.data());
     return g;
   }
+  // Addition (no counterpart in gpu.h): groups [first, first + max) straight into pinned host memory
+  // (keys [.][nkeys], exact [.][naggs][2]); status valid after the stream is synchronised.
+  void fetchAsync(int64_t first, int64_t max, double* keys, int64_t* exact, ws_fetch_status* status) {
+    wsCheck(ws_agg_fetch_async(h_, first, max, keys, exact, status));
+  }
   std::vector<uint8_t> sumBitsSlots() const {
     std::vector<uint8_t> f(naggs_);
     ws_agg_sum_bits_slots(h_, f.data());
