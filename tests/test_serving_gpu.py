@@ -64,3 +64,30 @@ def test_results_alone_equal_results_in_the_mix():
         ops.jit_set_mode(-1)
         for t in tables:
             t.free_device()
+
+
+def test_a_failing_query_ends_the_loop_with_its_error():
+    """A query whose operator call fails (a column count the library refuses) ends ws_serve with that
+    query's error code once the workers in flight have finished; nothing hangs and the library stays
+    usable for the next call."""
+    tables = S.make_tables(2, 10_000, 200_000, seed=7)
+    for t in tables:
+        t.to_device()
+    queries = S.make_queries(tables, 24, rate=5000.0, seed=8)
+    prepared, arrays = S.prepare(tables, queries)
+    ops.jit_set_mode(abi.JIT_SYNC)
+    try:
+        bad = prepared[5]
+        saved = bad.ncols
+        bad.ncols = abi.MAX_COLS + 1  # refused by every entry point before any memory is read
+        for mode in ("plain", "batched"):
+            with pytest.raises(ops.WsError) as ei:
+                S.run_native(tables, prepared, arrays, mode, keep_results=False)
+            assert ei.value.code == 1210
+        bad.ncols = saved
+        st = S.run_native(tables, prepared, arrays, "batched", keep_results=False)
+        assert st.completed == len(queries)
+    finally:
+        ops.jit_set_mode(-1)
+        for t in tables:
+            t.free_device()

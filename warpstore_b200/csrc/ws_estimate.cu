@@ -124,6 +124,7 @@ int ws_hll_sketch(const ws_expr_env* env, int ncols, const ws_agg_plan* plan, in
                   const uint32_t* const* bdel, const ws_col_view* bcols, int p, int64_t sample_rows, uint32_t* regs_out,
                   int64_t* sampled, int64_t* passing) {
   return guardedCall([&] {
+    if (ncols < 0 || ncols > WS_MAX_COLS || nb < 0) throw Error("sketch: bad column or batch count", WS_ERR_ARG);
     if (p < 4 || p > kHllMaxP) throw Error("sketch: precision must be 4..12", WS_ERR_ARG);
     if (plan->nkeys < 1 || plan->nkeys > WS_INTERP_KEYS) throw Error("sketch: 1 to 4 GROUP BY keys", WS_ERR_ARG);
     std::unique_ptr<TProgs> tp(new TProgs);

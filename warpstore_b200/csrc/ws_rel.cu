@@ -264,6 +264,7 @@ double kNullF64() {  // the engine's NULL double: the canonical quiet NaN
 }
 
 EvalSpec evalSpec(const ws_expr_env& env, int ncols, ws_prog prog, DBuf<uint8_t>& progBuf) {
+  if (ncols < 0 || ncols > WS_MAX_COLS) throw Error("bad column count", WS_ERR_ARG);
   ws_agg_plan plan;
   memset(&plan, 0, sizeof plan);
   plan.hasWhere = 1;
@@ -296,6 +297,7 @@ EvalSpec evalSpec(const ws_expr_env& env, int ncols, ws_prog prog, DBuf<uint8_t>
 }
 
 const ws_col_view* uploadCols(const ws_expr_env& env, int ncols, DBuf<uint8_t>& buf) {
+  if (ncols < 0 || ncols > WS_MAX_COLS) throw Error("bad column count", WS_ERR_ARG);
   const size_t bytes = sizeof(ws_col_view) * (size_t)std::max(ncols, 1);
   buf = DBuf<uint8_t>((int64_t)bytes);
   uint8_t* st = pinnedStage(bytes);

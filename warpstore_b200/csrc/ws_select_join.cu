@@ -467,6 +467,7 @@ static SelDesc uploadSel(int nb, int ncols, const int64_t* bn, const uint32_t* c
 static int64_t selectRun(const ws_expr_env& env, bool hasWhere, ws_prog where, int nb, const int64_t* bn,
                          const uint32_t* const* bdel, const ws_col_view* bcols, int ncols, int32_t** out,
                          int64_t* perBatch, const ws_jit_program* jit) {
+  if (ncols < 0 || ncols > WS_MAX_COLS || nb < 0) throw Error("select: bad column or batch count", WS_ERR_ARG);
   for (int b = 0; b < nb; ++b)
     if (perBatch) perBatch[b] = 0;
   int64_t total = 0;
