@@ -104,6 +104,24 @@ typedef struct ws_fetch_status {
 } ws_fetch_status;
 int ws_agg_fetch_async(ws_aggregator* agg, int64_t first_group, int64_t max_groups, double* keys, int64_t* exact,
                        ws_fetch_status* status);
+/* ---- prepared queries (no counterpart in the reference, which launches every query afresh).  The
+ * aggregation of `plan` over the batches, built once: result rows, batch descriptor, and one CUDA graph
+ * of the whole query (rows reset, the scan, compaction, the groups and a ws_fetch_status written into
+ * pinned host memory owned by the executor, up to max_groups groups).  ws_exec_run queues the graph on
+ * the calling thread's stream with env's constants, sets and maps (its expressions must be those of
+ * the env given at creation: WS_ERR_ARG otherwise); after the stream is synchronised ws_exec_results
+ * gives the groups (ws_agg_fetch's formats), valid until the next run.  status->overflow: the hash
+ * table filled up (create a bigger one); status->groups > max_groups: only max_groups were written.
+ * Needs a compiled plan covering the batches (WS_ERR_PLAN otherwise).  One run at a time per executor;
+ * destroy it from the thread whose stream ran it. */
+typedef struct ws_executor ws_executor;
+int ws_exec_create(const ws_agg_plan* plan, int64_t capacity, const ws_dense_spec* dense, const ws_expr_env* env,
+                   int ncols, int nb, const int64_t* bn, const uint32_t* const* bdel, const ws_col_view* bcols,
+                   const ws_jit_program* jit, int64_t max_groups, ws_executor** out);
+int ws_exec_run(ws_executor* ex, const ws_expr_env* env);
+int ws_exec_results(ws_executor* ex, const double** keys, const int64_t** exact, const ws_fetch_status** status);
+void ws_exec_destroy(ws_executor* ex);
+
 /* Without GROUP BY: which slots hold exact int64 bits (GpuAggregator::sumBitsSlots) and the high 64 bits
  * of the exact integer sums (GpuAggregator::sumHigh; valid after ws_agg_fetch). */
 int ws_agg_sum_bits_slots(const ws_aggregator* agg, uint8_t* out);

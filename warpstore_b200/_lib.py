@@ -52,6 +52,10 @@ SIGNATURES = {
     "ws_agg_group_count": (C.c_int, [P, I64P]),
     "ws_agg_fetch": (C.c_int, [P, C.c_int64, P, P, P, I64P]),
     "ws_agg_fetch_async": (C.c_int, [P, C.c_int64, C.c_int64, P, P, P]),
+    "ws_exec_create": (C.c_int, [P, C.c_int64, P, P, C.c_int, C.c_int, P, P, P, P, C.c_int64, C.POINTER(P)]),
+    "ws_exec_run": (C.c_int, [P, P]),
+    "ws_exec_results": (C.c_int, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P)]),
+    "ws_exec_destroy": (None, [P]),
     "ws_agg_sum_bits_slots": (C.c_int, [P, P]),
     "ws_agg_sum_high": (C.c_int, [P, P]),
     "ws_agg_compact": (C.c_int, [P, C.POINTER(P), C.POINTER(P), I64P]),

@@ -44,6 +44,7 @@ struct DriverApi {
   CUresult (*funcSetAttribute)(CUfunction, CUfunction_attribute, int);
   CUresult (*occupancy)(int*, CUfunction, int, size_t);
   CUresult (*getErrorString)(CUresult, const char**);
+  CUresult (*graphExecKernelNodeSetParams)(CUgraphExec, CUgraphNode, const CUDA_KERNEL_NODE_PARAMS*);
 };
 const DriverApi& drv();
 void ensureInit();

@@ -516,7 +516,23 @@ static size_t hashSmemSlots(const ws_aggregator& A, size_t budget) {
   return s * per > budget ? 0 : s;
 }
 
-static void aggRun(ws_aggregator& A, const ws_expr_env& env, const ws_jit_program* jit) {
+// A scan prepared for launching elsewhere (a captured graph): kernel, shape, launch descriptor and the
+// device buffers the descriptor points to.
+struct PreparedScan {
+  bool ready = false;     // false: the batches hold no tiles (nothing to launch)
+  bool compiled = false;  // the plan's generated kernels (not the interpreter)
+  CUfunction f = nullptr;
+  unsigned grid = 0;
+  size_t smem = 0;
+  int threads = kThreads;
+  Launch L{};
+  BatchDesc desc;
+  DBuf<u64> part;
+};
+
+// The aggregation scan over the collected batches; with `prep`, everything up to the launch (descriptor
+// upload, kernel and shape choice, tuning) is done and the launch is handed to the caller instead.
+static void aggRun(ws_aggregator& A, const ws_expr_env& env, const ws_jit_program* jit, PreparedScan* prep = nullptr) {
   const int nb = (int)A.bn.size();
   if (nb == 0) return;
   A.fetched = false;
@@ -661,6 +677,26 @@ static void aggRun(ws_aggregator& A, const ws_expr_env& env, const ws_jit_progra
   TuneChoice choice;
   if (!tuneLookup(key, choice) && tuneMode() == WS_TUNE_ON && A.windows == 0 && A.rowsDone == 0)
     choice = tuneScan(A, key, cands, launchOnce);
+  if (prep) {
+    const Shape sh = shapeOf(choice);
+    unsigned grid = persistentGrid(sh.f, sh.smem, d.ntiles, sh.threads);
+    if (choice.ctasPerSm > 0)
+      grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(grid, (int64_t)choice.ctasPerSm * smCount()));
+    if (partRows) {
+      part = DBuf<u64>((int64_t)grid * partRows * A.lay.rw);
+      L.part = part.p;
+    }
+    prep->compiled = useJit;
+    prep->f = sh.f;
+    prep->grid = grid;
+    prep->smem = sh.smem;
+    prep->threads = sh.threads;
+    prep->L = L;
+    prep->desc = std::move(d);
+    prep->part = std::move(part);
+    prep->ready = true;
+    return;
+  }
   launchOnce(choice);
 }
 
@@ -956,6 +992,173 @@ int ws_agg_fetch_async(ws_aggregator* A, int64_t first_group, int64_t max_groups
     A->fetched = true;
   });
 }
+
+}  // extern "C"
+
+// A prepared query (ws_exec_*): the aggregation's result rows, its batch descriptor and one CUDA graph
+// of the whole query — result rows reset, the scan, compaction, the groups and the status written into
+// pinned host memory — captured once; each run updates the scan node's launch descriptor (the plan's
+// constants) and launches the graph.
+struct ws_executor {
+  ws_aggregator* A = nullptr;
+  ws::PreparedScan ps;
+  uint64_t code = 0;  // digest of the expressions the graph was built for
+  int64_t maxGroups = 0;
+  double* keys = nullptr;
+  int64_t* exact = nullptr;
+  ws_fetch_status* st = nullptr;
+  ws::DBuf<int64_t> offs;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaGraphNode_t scanNode = nullptr;
+  int kernels = 0;  // kernel nodes per run
+  ~ws_executor() {
+    cudaStreamSynchronize(ws::stream());  // a run queued on this thread's stream may still be in flight
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (keys) cudaFreeHost(keys);
+    if (exact) cudaFreeHost(exact);
+    if (st) cudaFreeHost(st);
+    if (A) ws_agg_destroy(A);
+  }
+};
+
+namespace {
+uint64_t codeDigest(const ws_expr_env& env) {
+  uint64_t h = 0xcbf29ce484222325ull;
+  const unsigned char* b = (const unsigned char*)env.code;
+  for (size_t i = 0; i < sizeof env.code; ++i) h = (h ^ b[i]) * 0x100000001b3ull;
+  return h;
+}
+}  // namespace
+
+extern "C" {
+
+int ws_exec_create(const ws_agg_plan* plan, int64_t capacity, const ws_dense_spec* dense, const ws_expr_env* env,
+                   int ncols, int nb, const int64_t* bn, const uint32_t* const* bdel, const ws_col_view* bcols,
+                   const ws_jit_program* jit, int64_t max_groups, ws_executor** out) {
+  return guardedCall([&] {
+    *out = nullptr;
+    if (max_groups < 1) throw Error("exec: max_groups must be positive", WS_ERR_ARG);
+    if (!jit || jit->state.load() != 1) throw Error("exec: a prepared query needs a compiled plan", WS_ERR_PLAN);
+    std::unique_ptr<ws_executor> X(new ws_executor);
+    if (int rc = ws_agg_create(plan, capacity, dense, &X->A)) throw Error(ws_last_error(), rc);
+    if (int rc = ws_agg_add_batches(X->A, ncols, nb, bn, bdel, bcols)) throw Error(ws_last_error(), rc);
+    ws_aggregator& A = *X->A;
+    aggRun(A, *env, jit, &X->ps);
+    if (X->ps.ready && !X->ps.compiled)
+      throw Error("exec: the compiled plan does not cover these batches (encodings)", WS_ERR_PLAN);
+    X->code = codeDigest(*env);
+    X->maxGroups = max_groups;
+    const int nk = A.plan.nkeys, na = A.plan.naggs;
+    auto pinned = [](size_t bytes, void** p) {
+      if (cudaHostAlloc(p, std::max<size_t>(bytes, 8), cudaHostAllocMapped) != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        throw Error("exec: pinned result buffers", WS_ERR_OOM);
+      }
+    };
+    pinned(sizeof(double) * max_groups * std::max(nk, 1), (void**)&X->keys);
+    pinned(sizeof(int64_t) * max_groups * na * 2, (void**)&X->exact);
+    pinned(sizeof(ws_fetch_status), (void**)&X->st);
+    double* dk = nullptr;
+    long long* dx = nullptr;
+    ws_fetch_status* dst = nullptr;
+    WS_CK(cudaHostGetDevicePointer((void**)&dk, X->keys, 0));
+    WS_CK(cudaHostGetDevicePointer((void**)&dx, X->exact, 0));
+    WS_CK(cudaHostGetDevicePointer((void**)&dst, X->st, 0));
+    const int64_t nr = A.nrows();
+    const OccSpec o{A.lay.rw, nk == 0 ? 0 : A.isDense ? 1 : 2, A.lay.woff[0], A.cap};
+    const int64_t nchunks = (nr + kOccChunk - 1) / kOccChunk;
+    X->offs = DBuf<int64_t>(nchunks + 1);
+    const int rowBytes = 8 * (nk + 2 * na);
+    const int threads = std::max(32, std::min(256, (32768 / rowBytes) & ~31));
+    const EmitSpec es = emitSpec(A);
+    sync();  // the preparation's copies and allocations are done before the capture starts
+    // capture on a private stream (nothing else of this thread's work joins the graph)
+    cudaStream_t cs = nullptr;
+    WS_CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaStream_t prev = stream();
+    auto restore = [&] { ws_set_stream(prev == cudaStreamPerThread ? nullptr : (void*)prev); };
+    ws_set_stream(cs);
+    bool capturing = false;
+    try {
+      WS_CK(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+      capturing = true;
+      aggResetRows(A);
+      X->kernels = 1;
+      if (X->ps.ready) {
+        const PreparedScan& p = X->ps;
+        if (p.smem > 0)
+          WS_CKD(drv().funcSetAttribute(p.f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)p.smem));
+        void* args[] = {(void*)&X->ps.L};
+        WS_CKD(drv().launchKernel(p.f, p.grid, 1, 1, (unsigned)p.threads, 1, 1, (unsigned)p.smem, (CUstream)cs, args,
+                                  nullptr));
+        countLaunch();
+        cudaStreamCaptureStatus cst;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t ndeps = 0;
+        WS_CK(cudaStreamGetCaptureInfo(cs, &cst, nullptr, nullptr, &deps, &ndeps));
+        if (ndeps != 1) throw Error("exec: could not find the scan in the captured graph", WS_ERR_INTERNAL);
+        X->scanNode = deps[0];
+        ++X->kernels;
+      }
+      WS_LAUNCH(kOccCount, (unsigned)nchunks, 256, 0, A.rows.p, nr, o, X->offs.p);
+      WS_LAUNCH(kScanExclusive, 1, 1024, 0, X->offs.p, nchunks);
+      WS_LAUNCH(kFetchStatus, 1, 1, 0, X->offs.p + nchunks, A.err(), o.mode == 2 ? 1 : 0, dst);
+      WS_LAUNCH(kOccEmitHost, (unsigned)nchunks, threads, (size_t)threads * rowBytes, A.rows.p, nr, o, es, X->offs.p,
+                nchunks, A.err(), (int64_t)0, max_groups, dk, dx);
+      X->kernels += 4;
+      capturing = false;
+      WS_CK(cudaStreamEndCapture(cs, &X->graph));
+      WS_CK(cudaGraphInstantiate(&X->exec, X->graph, 0));
+    } catch (...) {
+      if (capturing) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(cs, &g);
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+      }
+      restore();
+      cudaStreamDestroy(cs);
+      throw;
+    }
+    countLaunch(-X->kernels);  // captured, not launched
+    restore();
+    WS_CK(cudaStreamDestroy(cs));
+    *out = X.release();
+  });
+}
+
+int ws_exec_run(ws_executor* X, const ws_expr_env* env) {
+  return guardedCall([&] {
+    if (codeDigest(*env) != X->code) throw Error("exec: the expressions differ from the prepared query's", WS_ERR_ARG);
+    if (X->scanNode) {
+      X->ps.L.env = envK(*env);
+      void* args[] = {(void*)&X->ps.L};
+      CUDA_KERNEL_NODE_PARAMS kp{};
+      kp.func = X->ps.f;
+      kp.gridDimX = X->ps.grid;
+      kp.gridDimY = kp.gridDimZ = 1;
+      kp.blockDimX = (unsigned)X->ps.threads;
+      kp.blockDimY = kp.blockDimZ = 1;
+      kp.sharedMemBytes = (unsigned)X->ps.smem;
+      kp.kernelParams = args;
+      WS_CKD(drv().graphExecKernelNodeSetParams((CUgraphExec)X->exec, (CUgraphNode)X->scanNode, &kp));
+    }
+    WS_CK(cudaGraphLaunch(X->exec, stream()));
+    countLaunch(X->kernels);
+  });
+}
+
+int ws_exec_results(ws_executor* X, const double** keys, const int64_t** exact, const ws_fetch_status** status) {
+  if (keys) *keys = X->keys;
+  if (exact) *exact = X->exact;
+  if (status) *status = X->st;
+  return WS_OK;
+}
+
+void ws_exec_destroy(ws_executor* X) { delete X; }
 
 int ws_host_alloc(size_t bytes, void** out) {
   return guardedCall([&] {

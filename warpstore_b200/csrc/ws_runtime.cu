@@ -76,6 +76,7 @@ const DriverApi& drv() {
     get("cuFuncSetAttribute", (void**)&a.funcSetAttribute);
     get("cuOccupancyMaxActiveBlocksPerMultiprocessor", (void**)&a.occupancy);
     get("cuGetErrorString", (void**)&a.getErrorString);
+    get("cuGraphExecKernelNodeSetParams", (void**)&a.graphExecKernelNodeSetParams);
     return a;
   }();
   return api;

@@ -175,6 +175,49 @@ class HostBuffer:
             pass
 
 
+class Executor:
+    """A prepared query (ws_exec_*): the aggregation of `plan` over device batches (the arrays of
+    estimator.batch_arrays) built once with a CUDA graph of the whole query; run(env) queues it with
+    env's constants, results() reads the groups after sync()."""
+
+    def __init__(self, plan: abi.AggPlan, capacity: int, dense, env: abi.ExprEnv, ncols: int, arrays: tuple,
+                 jit: int, max_groups: int):
+        self.plan = plan
+        self.h = None
+        nb, bn, bdel, arr = arrays[:4]
+        h = P()
+        check(lib().ws_exec_create(C.byref(plan), int(capacity), C.byref(dense) if dense is not None else None,
+                                   C.byref(env), ncols, nb, bn, bdel, arr, jit, int(max_groups), C.byref(h)))
+        self.h = h.value
+        self.max_groups = int(max_groups)
+
+    def run(self, env: abi.ExprEnv):
+        check(lib().ws_exec_run(self.h, C.byref(env)))
+
+    def results(self):
+        """(keys [g, nk] float64, exact [g, na, 2] int64, status) copies of the last run's groups."""
+        k, x, s = P(), P(), P()
+        check(lib().ws_exec_results(self.h, C.byref(k), C.byref(x), C.byref(s)))
+        st = np.ctypeslib.as_array((C.c_uint8 * FETCH_STATUS.itemsize).from_address(s.value)).view(FETCH_STATUS)[0]
+        g = min(int(st["groups"]), self.max_groups)
+        nk, na = self.plan.nkeys, self.plan.naggs
+        keys = np.ctypeslib.as_array((C.c_double * max(g * max(nk, 1), 1)).from_address(k.value))
+        keys = keys[:g * nk].reshape(g, nk).copy()
+        ex = np.ctypeslib.as_array((C.c_int64 * max(g * na * 2, 1)).from_address(x.value))[:g * na * 2]
+        return keys, ex.reshape(g, na, 2).copy(), {n: int(st[n]) for n in FETCH_STATUS.names}
+
+    def close(self):
+        if self.h:
+            lib().ws_exec_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class GpuAggregator:
     """GPU aggregation state of one query (src/gpu.h:84-130)."""
 
@@ -413,7 +456,7 @@ def map_rank(keys_ptr: int, rank_ptr: int, m: int):
     check(lib().ws_map_rank(keys_ptr, rank_ptr, m))
 
 
-__all__ = ["DeviceBuffer", "GpuAggregator", "WsError", "agg_nokeys_noalloc", "bits_to_double", "codegen_compile_check",
+__all__ = ["DeviceBuffer", "Executor", "GpuAggregator", "WsError", "agg_nokeys_noalloc", "bits_to_double", "codegen_compile_check",
            "codegen_source", "cross_join", "device_to_array", "encode_column", "eval_at", "eval_at_int", "gather", "gather_bytes",
            "gather_enc", "gather_multi", "gather_null", "gpu_init", "hash_join", "hash_join_outer", "hash_join_parts",
            "jit_get", "jit_info", "jit_set_cache_dir", "jit_set_default_mode", "jit_set_mode", "kernel_launches",
