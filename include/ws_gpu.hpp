@@ -189,6 +189,30 @@ class GpuAggregator {
   std::vector<int64_t> hi_;
 };
 
+// Addition (no counterpart in gpu.h): a query prepared once as a CUDA graph and rerun with new
+// constants (ws_exec_*).  Results live in the executor's pinned memory until the next run.
+class PreparedQuery {
+ public:
+  PreparedQuery(const AggPlan& plan, int64_t capacity, const DenseSpec* dense, const ExprEnv& env, int ncols,
+                const std::vector<int64_t>& bn, const std::vector<const uint32_t*>& bdel,
+                const std::vector<ColView>& bcols, const JitProgram* jit, int64_t maxGroups) {
+    wsCheck(ws_exec_create((const ws_agg_plan*)&plan, capacity, (const ws_dense_spec*)dense,
+                           (const ws_expr_env*)&env, ncols, (int)bn.size(), bn.data(), bdel.data(),
+                           (const ws_col_view*)bcols.data(), jit, maxGroups, &h_));
+  }
+  ~PreparedQuery() { ws_exec_destroy(h_); }
+  PreparedQuery(const PreparedQuery&) = delete;
+  PreparedQuery& operator=(const PreparedQuery&) = delete;
+  void run(const ExprEnv& env) { wsCheck(ws_exec_run(h_, (const ws_expr_env*)&env)); }
+  // after gpuSync(): keys [g][nkeys], exact [g][naggs][2], status (groups, overflow, error)
+  void results(const double** keys, const int64_t** exact, const ws_fetch_status** status) {
+    wsCheck(ws_exec_results(h_, keys, exact, status));
+  }
+
+ private:
+  ws_executor* h_ = nullptr;
+};
+
 // ---- selection / gathers (src/gpu.h:132-143, :170-172)
 inline int64_t gpuSelect(const ExprEnv& env, bool hasWhere, Prog where, int64_t n, const uint32_t* del, int32_t* outIdx,
                          const JitProgram* jit = nullptr) {
