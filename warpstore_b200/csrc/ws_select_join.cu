@@ -123,6 +123,14 @@ __device__ __forceinline__ bool joinKeyStream(const ws_col_view& c, int64_t r, l
   return d == d;
 }
 
+// Both slots of a 32-byte sector in one 256-bit load (one L1 request per lane instead of two; the
+// probe's random table reads are bound by L1 requests).  `p` is 32-byte aligned (an even slot).
+__device__ __forceinline__ void ldSector(const JSlot* p, ulonglong2& a, ulonglong2& b) {
+  asm("ld.global.nc.v4.u64 {%0,%1,%2,%3}, [%4];"
+               : "=l"(a.x), "=l"(a.y), "=l"(b.x), "=l"(b.y)
+               : "l"(p));
+}
+
 struct JPass {
   int bits;  // log2 of the pass count
   int pass;
@@ -359,8 +367,8 @@ __global__ void __launch_bounds__(kJThreads) kJoinProbe(ws_col_view key, int64_t
       if (nq > 0) {
         const unsigned s0 = qs[0];
         const unsigned even = s0 & ~1u;
-        const ulonglong2 a = __ldg((const ulonglong2*)(t + even));
-        const ulonglong2 b = __ldg((const ulonglong2*)(t + even + 1));
+        ulonglong2 a, b;
+        ldSector(t + even, a, b);
         pr = qr[0];
         done = false;
         // slot `even` counts only when the walk starts there; slot even + 1 always
