@@ -126,9 +126,7 @@ __device__ __forceinline__ bool joinKeyStream(const ws_col_view& c, int64_t r, l
 // Both slots of a 32-byte sector in one 256-bit load (one L1 request per lane instead of two; the
 // probe's random table reads are bound by L1 requests).  `p` is 32-byte aligned (an even slot).
 __device__ __forceinline__ void ldSector(const JSlot* p, ulonglong2& a, ulonglong2& b) {
-  asm("ld.global.nc.v4.u64 {%0,%1,%2,%3}, [%4];"
-               : "=l"(a.x), "=l"(a.y), "=l"(b.x), "=l"(b.y)
-               : "l"(p));
+  asm("ld.global.nc.v4.u64 {%0,%1,%2,%3}, [%4];" : "=l"(a.x), "=l"(a.y), "=l"(b.x), "=l"(b.y) : "l"(p));
 }
 
 struct JPass {
