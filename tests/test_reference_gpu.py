@@ -124,6 +124,43 @@ def test_join_vs_reference():
     print(f"\n[timing] hash join build {nb} probe {np_}: reference {rms:.3f} ms, ours {oms:.3f} ms")
 
 
+@pytest.mark.parametrize("nb,np_", [(7_500_000, 60_000_000), (7_500_000, 8_000_000)], ids=["60m", "8m"])
+def test_sparse_key_join_vs_reference(nb, np_):
+    """Build keys spread over all of int64 (the hash path, no dense range): pairs keyed alike, the
+    reference's pair count; CUDA-event times of both (second run)."""
+    import torch
+    rng = np.random.default_rng(3)
+    mul = np.uint64(0x9E3779B97F4A7C15)
+    bk = (rng.permutation(15_000_000)[:nb].astype(np.uint64) * mul).view(np.int64)
+    pk = (rng.integers(0, 15_000_000, np_).astype(np.uint64) * mul).view(np.int64)
+    db, dp = ops.DeviceBuffer.from_array(bk), ops.DeviceBuffer.from_array(pk)
+    bv, pv = abi.ColView(db.ptr, abi.T_I64, 0, 0, 0), abi.ColView(dp.ptr, abi.T_I64, 0, 0, 0)
+    times = {}
+    for rep in range(2):
+        torch.cuda.synchronize()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record()
+        rb, rp, rm, _ = ref.hash_join_dev(bv, nb, pv, np_)
+        s1.record()
+        s1.synchronize()
+        times["reference"] = s0.elapsed_time(s1)
+        ref.free(rb)
+        ref.free(rp)
+        s0.record()
+        ob, op, m = ops.hash_join(bv, nb, pv, np_)
+        s1.record()
+        s1.synchronize()
+        times["ours"] = s0.elapsed_time(s1)
+        gb, gp = ops.device_to_array(ob, np.int32, m), ops.device_to_array(op, np.int32, m)
+        ops.tmp_free(ob)
+        ops.tmp_free(op)
+    assert m == rm and m > 0
+    assert np.array_equal(bk[gb], pk[gp])            # every pair's keys are equal
+    assert np.unique(gp).size == m                   # unique build keys: one pair per matching probe row
+    print(f"\n[timing] sparse-key hash join build {nb} probe {np_}: reference {times['reference']:.3f} ms, "
+          f"ours {times['ours']:.3f} ms")
+
+
 def test_select_vs_reference():
     t = W.pricing_summary(3 * W.SEG_ROWS + 12345, seed=4)
     e = W.env_for(t)
