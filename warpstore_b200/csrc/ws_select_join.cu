@@ -412,10 +412,27 @@ int64_t joinTableBudget() {
   return b;
 }
 
+
 int64_t pow2AtLeast(int64_t x) {
   int64_t c = 2;
   while (c < x) c <<= 1;
   return c;
+}
+
+// Hash join table slots for `keys` build keys and `probes` probe rows: the next power of two of 4 x
+// keys (load <= 1/4, shorter clusters: 7.5M x 60M measured 2.48 against 2.66 ms) when the probe side
+// has at least 8 rows per key and the table stays within 2 GiB, else of 2 x keys (a smaller probe side
+// does not repay clearing the larger table: 7.5M x 8M measured 0.90 against 0.85 ms);
+// WARPSTORE_B200_JOIN_SLOTS_PER_KEY = 2..16 fixes the factor.
+int64_t joinTableSlots(int64_t keys, int64_t probes) {
+  static const int64_t fixed = [] {
+    const char* e = getenv("WARPSTORE_B200_JOIN_SLOTS_PER_KEY");
+    const long long v = e ? atoll(e) : 0;
+    return v >= 2 && v <= 16 ? (int64_t)v : (int64_t)0;
+  }();
+  if (fixed) return pow2AtLeast(fixed * keys);
+  const int64_t c = pow2AtLeast(4 * keys);
+  return probes >= 8 * keys && c * (int64_t)sizeof(JSlot) <= ((int64_t)2 << 30) ? c : pow2AtLeast(2 * keys);
 }
 
 }  // namespace
@@ -680,7 +697,9 @@ static void joinImpl(ws_col_view build_key, const int64_t* boff, int pb, ws_col_
     std::vector<int> bits(pb, 0);
     for (int q = 0; q < pb; ++q) {
       const int64_t nq = boff[q + 1] - boff[q];
-      while (bits[q] < 6 && pow2AtLeast(2 * ((nq >> bits[q]) + 1)) * (int64_t)sizeof(JSlot) > joinTableBudget()) ++bits[q];
+      const int64_t npq = pb == 1 ? np : poff[q + 1] - poff[q];  // probe rows joined with build partition q
+      while (bits[q] < 6 && joinTableSlots((nq >> bits[q]) + 1, npq >> bits[q]) * (int64_t)sizeof(JSlot) > joinTableBudget())
+        ++bits[q];
     }
     // Build-key statistics (non-NULL count, min, max, keys per hash pass) of every partition.
     DBuf<unsigned long long> stats((int64_t)pb * kJStatWords);
@@ -711,7 +730,7 @@ static void joinImpl(ws_col_view build_key, const int64_t* boff, int pb, ws_col_
         continue;
       }
       for (int p = 0; p < (1 << bits[q]); ++p) {
-        const int64_t c = pow2AtLeast(2 * (bits[q] ? (int64_t)st[3 + p] : keys));
+        const int64_t c = joinTableSlots(bits[q] ? (int64_t)st[3 + p] : keys, (pb == 1 ? np : poff[q + 1] - poff[q]) >> bits[q]);
         cap[q].push_back(c);
         tableSlots = std::max(tableSlots, c);
       }
