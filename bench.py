@@ -39,7 +39,7 @@ PEAK_FALLBACK_GBS = 6650.0
 # DRAM bytes (read + write) per row of the workload's scan kernel, from one ncu capture of a smaller
 # case of the same kernel (8,388,608 and 25,000,000 rows), scaled to a launch by its rows: the traffic
 # grows in proportion to the rows scanned
-NCU_DRAM_BYTES_PER_ROW = {"pricing_summary_60m": 38.52, "high_cardinality_100m": 22.94}
+NCU_DRAM_BYTES_PER_ROW = {"pricing_summary_60m": 38.52, "high_cardinality_100m": 22.94, "pricing_nokeys_60m": 28.55}
 
 
 def measured_peak():
@@ -164,6 +164,18 @@ def make_workload(name: str, rank: int, rows: int | None = None):
             "columns": "ship_date i32, quantity/price/discount/tax i64, flag1/flag2 u8-encoded",
             "groups": 6, "aggregation": "dense",
             "l2": f"inputs {t.n * W.PRICING_BYTES_PER_ROW / 1e9:.2f} GB > 126 MB L2 (no flush needed)"}
+    if name == "pricing_nokeys_60m":  # the same table, filter + aggregates without GROUP BY
+        from warpstore_b200 import query as q
+        t = W.pricing_summary(rows or W.PRICING_ROWS, seed=2 + rank)
+        e = W.env_for(t)
+        aggs = [q.Agg("COUNT"), q.Agg("SUM", q.col(2) * (q.ilit(100) - q.col(3)), "BIGINT", False),
+                q.Agg("MIN", q.col(2), "BIGINT", True), q.Agg("MAX", q.col(1), "BIGINT", True)]
+        aq = q.AggQuery(e, q.col(0).le(2467), [], aggs)
+        return t, e, aq, None, 4 + 8 * 3, 1, {
+            "workload": "pricing_nokeys_60m", "rows": t.n, "segments": t.nseg, "segment_rows": t.seg_rows,
+            "columns": "ship_date i32, price/discount/quantity i64 (28 B/row read)", "groups": 1,
+            "aggregation": "no keys: COUNT, exact SUM(price*(100-discount)), MIN(price), MAX(quantity)",
+            "l2": f"inputs {t.n * 28 / 1e9:.2f} GB > 126 MB L2 (no flush needed)"}
     if name == "high_cardinality_100m":
         n = rows or W.HC_ROWS
         t = W.high_cardinality(n, W.HC_RANKS if n == W.HC_ROWS else max(n // 10, 1000), W.HC_DICT, seed=4 + rank)
@@ -394,7 +406,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="pricing_summary_60m",
-                    choices=["pricing_summary_60m", "filter_groupby_1m", "high_cardinality_100m"])
+                    choices=["pricing_summary_60m", "pricing_nokeys_60m", "filter_groupby_1m", "high_cardinality_100m"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--traffic", type=float, default=None, help="ncu dram bytes per launch, when known")
