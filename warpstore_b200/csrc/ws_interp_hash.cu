@@ -1,0 +1,12 @@
+// Interpreter instantiations (prefix wsi) of the hash GROUP BY scan.  The scan kernels are
+// split over several translation units so that they compile in parallel.
+#include "ws_internal.h"
+#include "ws_interp.cuh"
+
+WS_K_HASH(ws::InterpEv, wsi)
+
+namespace ws {
+void interpSyms_hash(const void** s) {
+  s[K_HASH] = (const void*)wsi_hash;
+}
+}  // namespace ws

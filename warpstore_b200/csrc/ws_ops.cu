@@ -4,19 +4,23 @@
 #include <cstring>
 
 #include "ws_internal.h"
-#include "ws_interp.cuh"
-
-// Interpreter instantiations of every scan kernel (prefix wsi).
-WS_DEFINE_SCAN_KERNELS(ws::InterpEv, wsi)
 
 namespace ws {
+
+// Interpreter instantiations of every scan kernel (prefix wsi), one translation unit per group.
+void interpSyms_agg(const void** s);
+void interpSyms_priv(const void** s);
+void interpSyms_hash(const void** s);
+void interpSyms_select(const void** s);
 
 const KernelSet& interpKernels() {
   static KernelSet ks = [] {
     KernelSet k;
-    const void* syms[K_COUNT_] = {(const void*)wsi_nokeys, (const void*)wsi_dense_shared, (const void*)wsi_dense_global,
-                                  (const void*)wsi_hash, (const void*)wsi_select_count, (const void*)wsi_select_write,
-                                  (const void*)wsi_dense_priv, (const void*)wsi_dense_priv_staged};
+    const void* syms[K_COUNT_] = {};
+    interpSyms_agg(syms);
+    interpSyms_priv(syms);
+    interpSyms_hash(syms);
+    interpSyms_select(syms);
     for (int i = 0; i < K_COUNT_; ++i) {
       cudaFunction_t f;
       WS_CK(cudaGetFuncBySymbol(&f, syms[i]));
