@@ -153,6 +153,49 @@ def cpu_oracle_rate(table, env, plan, budget_s: float, max_segments: int = 8):
     return done / el, rows, os.cpu_count() or 1
 
 
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def make_checker(name: str, table, env, aq, rank: int):
+    """(check(keys, exact, groups) -> None or what differs, description, every_step): the oracle's
+    groups of the whole workload, computed once before timing, against which results are compared
+    outside the timed events.  Few groups: every timed step; the high-cardinality workload (4M groups,
+    seconds to compare): the last timed step."""
+    from oracle import oracle
+    if name == "high_cardinality_100m":
+        from warpstore_b200 import workloads as W
+        key, payload = table.cols[0].data, table.cols[1].data
+        cut = W.high_cardinality_cut(4 + rank)  # the workload's predicate constant (make_workload)
+        wk, wc, ws_ = oracle.groupby_count_sum_np(key, payload, cut)
+        a_sum = aq.aggs[1]
+
+        def check(keys, exact, g):
+            if g != wk.size:
+                return f"{g} groups, the numpy restatement has {wk.size}"
+            k = np.ascontiguousarray(keys[:g, 0]).view(np.int64)
+            o = np.argsort(k)
+            if not np.array_equal(k[o], wk):
+                return "group keys differ"
+            ex = exact[:g][o]
+            if not np.array_equal(ex[:, 0, 0], wc):
+                return "COUNT differs"
+            lo, hi = ex[:, a_sum.slot, 0], ex[:, a_sum.slot, 1]
+            if not (np.array_equal(lo, ws_) and np.array_equal(hi, ws_ >> 63)):
+                return "SUM differs (exact words)"
+            return None
+        return check, "numpy restatement (sort + exact int64 sums), last timed step", False
+    okeys, owords, _ = oracle.aggregate(env.env, aq.plan, table.batches(False), env.ncols)
+    return (lambda keys, exact, g: oracle.compare_groups(aq.plan, okeys, owords, keys, exact, g),
+            "oracle (C++ restatement, int128 words), every timed step", True)
+
+
 # ------------------------------------------------------------------ workloads
 def make_workload(name: str, rank: int, rows: int | None = None):
     from warpstore_b200 import workloads as W
@@ -203,6 +246,9 @@ def run_ours(args, ws, rank, local):
     ops.lib().ws_set_stream(stream.cuda_stream)
     ops.gpu_init()
     table, env, aq, ds, bpr, cap, cfg = make_workload(args.workload, rank, args.rows)
+    # the exact groups of the whole workload, computed on the host before timing: every result is
+    # compared with them outside the timed events (a mismatch ends the run with an error)
+    check, verified, check_every = make_checker(args.workload, table, env, aq, rank)
     table.to_device()
     ops.jit_set_cache_dir(os.path.join(tempfile.gettempdir(), "warpstore_b200_plans"))
     ops.jit_set_mode(abi.JIT_SYNC)
@@ -237,8 +283,8 @@ def run_ours(args, ws, rank, local):
         done.record(stream)
         return agg, slot
 
-    def finish_step(q):
-        """Waits for a queued query and checks its groups (flags, count)."""
+    def finish_step(q, verify=check_every):
+        """Waits for a queued query and checks its status word and (verify) its groups."""
         agg, slot = q
         hk, hx, st, done = slots[slot]
         done.synchronize()
@@ -246,6 +292,10 @@ def run_ours(args, ws, rank, local):
         if s["error"] or s["overflow"] or s["groups"] > max_groups or s["groups"] < 1:
             raise SystemExit(f"query failed: status {s}")
         agg.close()
+        if verify:
+            err = check(hk.array if nk else None, hx.array, int(s["groups"]))
+            if err:
+                raise SystemExit(f"result differs from the {verified.split(',')[0]}: {err}")
         return int(s["groups"])
 
     def step(i=None):
@@ -280,7 +330,7 @@ def run_ours(args, ws, rank, local):
         if prev is not None:
             finish_step(prev)
         prev = cur
-    finish_step(prev)
+    finish_step(prev, verify=True)  # the last step is verified in every mode
     s1.record(stream)
     s1.synchronize()
     launches = ops.kernel_launches() - launches0
@@ -323,6 +373,10 @@ def run_ours(args, ws, rank, local):
             raise SystemExit(f"query failed: status {st.array[0]}")
         d2h = g * 8 * (nk + 2 * na) + ops.FETCH_STATUS.itemsize
         agg.close()
+        if check_every:
+            err = check(hk.array if nk else None, hx.array, g)
+            if err:
+                raise SystemExit(f"end-to-end result differs from the {verified.split(',')[0]}: {err}")
 
     e2e_step()
     stream.synchronize()
@@ -346,7 +400,7 @@ def run_ours(args, ws, rank, local):
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         rate, rows, cores = cpu_oracle_rate(table, env, aq.plan, args.cpu_seconds)
-        cpu = {"value": rate / 1e9, "unit": "G rows/s", "cores": cores, "kind": "port",
+        cpu = {"value": rate / 1e9, "unit": "G rows/s", "cores": cores, "cpu": cpu_model(), "kind": "port",
                "sample": f"{rows} rows (first segments of the same table), repeated for ~{args.cpu_seconds:.0f} s"}
     if rank == 0:
         line = {
@@ -359,7 +413,7 @@ def run_ours(args, ws, rank, local):
                          "kernel_ms": round(kernel_ms, 4), "algorithmic_bytes": algo_bytes},
             "e2e": {"value": round(e2e_value, 4), "unit": "G rows/s", "h2d_bytes_per_step": table.nbytes(),
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_ms, 3)},
-            "gpu_launches": int(launches), "clocks": clk, "cpu_baseline": cpu,
+            "gpu_launches": int(launches), "clocks": clk, "cpu_baseline": cpu, "verified": verified,
         }
         print(json.dumps(line), flush=True)
     table.free_device()
@@ -368,7 +422,10 @@ def run_ours(args, ws, rank, local):
 def run_reference(args, ws, rank, local):
     if rank != 0:
         return
+    from oracle import oracle
+    from warpstore_b200 import query as q
     from warpstore_b200 import workloads as W
+    q.TYPER = oracle.prog_is_int  # plans typed by the oracle: this arm loads none of the library's code
     name = args.workload
     if name == "pricing_summary_60m":
         # the per-step sample: 8 segments (8.4M rows) of the same table
@@ -379,7 +436,6 @@ def run_reference(args, ws, rank, local):
         t = W.filter_groupby_1m(1 << 20, seed=0)
         e, aq = W.filter_groupby_1m_query(t)
         cfg = {"workload": "filter_groupby_1m", "rows": t.n, "sample_rows": t.n}
-    from oracle import oracle
     batches = t.batches(False)
     for _ in range(args.warmup):
         oracle.aggregate(e.env, aq.plan, batches, e.ncols)
@@ -393,7 +449,7 @@ def run_reference(args, ws, rank, local):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(el / args.steps * 1e3, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
             "data": "synthetic (seeded numpy)", "config": cfg, "impl": "reference",
-            "cpu_baseline": {"value": round(rate, 4), "unit": "G rows/s", "cores": cores, "kind": "port",
+            "cpu_baseline": {"value": round(rate, 4), "unit": "G rows/s", "cores": cores, "cpu": cpu_model(), "kind": "port",
                              "sample": f"{t.n} rows per step"},
             "e2e": {"value": round(rate, 4), "unit": "G rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)

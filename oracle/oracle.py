@@ -27,6 +27,7 @@ def lib() -> C.CDLL:
                                           C.c_int, C.POINTER(P)]
         l.ws_oracle_aggregate_distinct.argtypes = [C.POINTER(abi.ExprEnv), C.POINTER(abi.AggPlan), abi.Prog, C.c_int,
                                                    C.c_int, P, P, P, C.c_int, C.c_int, C.POINTER(P)]
+        l.ws_oracle_prog_is_int.argtypes = [C.POINTER(abi.ExprEnv), abi.Prog]
         l.ws_oracle_ngroups.restype = C.c_int64
         l.ws_oracle_ngroups.argtypes = [P]
         l.ws_oracle_nkeys.argtypes = [P]
@@ -51,6 +52,14 @@ def lib() -> C.CDLL:
                                      C.POINTER(C.c_int), C.POINTER(C.c_int)]
         _lib = l
     return _lib
+
+
+def prog_is_int(env: abi.ExprEnv, prog: abi.Prog) -> bool:
+    """The oracle's static type of an expression (int64 or double)."""
+    r = lib().ws_oracle_prog_is_int(C.byref(env), prog)
+    if r < 0:
+        raise ValueError("malformed expression")
+    return bool(r)
 
 
 def _batches(batches: list):
@@ -170,3 +179,56 @@ def eval_at(env: abi.ExprEnv, cols: list, prog: abi.Prog, idx, m: int, as_int: b
     ov = C.c_int()
     lib().ws_oracle_eval_at(C.byref(env), arr, prog, ix, m, int(as_int), out.ctypes.data, C.byref(ov))
     return out[:m], bool(ov.value)
+
+
+def compare_groups(plan: abi.AggPlan, okeys: np.ndarray, owords: np.ndarray, keys, exact: np.ndarray, g: int):
+    """None when a GPU result equals the oracle's groups, else what differs.  keys [g][nkeys] float64 and
+    exact [g][naggs][2] int64 are ws_agg_fetch's formats (integer keys as int64 bits); okeys / owords
+    come from aggregate().  Integer slots and COUNT compare exactly (int128 words); DOUBLE slots within
+    1e-12 relative."""
+    if g != okeys.shape[0]:
+        return f"{g} groups, the oracle has {okeys.shape[0]}"
+    nk, na = plan.nkeys, plan.naggs
+    if nk:
+        gk = np.ascontiguousarray(keys[:g, :nk]).view(np.int64)
+        o1, o2 = np.lexsort(gk.T[::-1]), np.lexsort(okeys.T[::-1])
+        if not np.array_equal(gk[o1], okeys[o2]):
+            return "group keys differ"
+    else:
+        o1 = o2 = np.arange(g)
+    for a in range(na):
+        mine, want = exact[:g][o1][:, a], owords[o2][:, a]
+        if plan.aggInt[a] or plan.ops[a] == abi.AGG_COUNT:
+            if not np.array_equal(mine, want):
+                return f"slot {a} differs (exact words)"
+            continue
+        x, y = np.ascontiguousarray(mine[:, 0]).view(np.float64), np.ascontiguousarray(want[:, 0]).view(np.float64)
+        if plan.ops[a] == abi.AGG_SUM:
+            if not np.allclose(x, y, rtol=1e-12, atol=1e-300, equal_nan=True):
+                return f"slot {a} differs beyond 1e-12 relative"
+        elif not np.array_equal(x, y, equal_nan=True):
+            return f"slot {a} differs"
+    return None
+
+
+def groupby_count_sum_np(key: np.ndarray, payload: np.ndarray, cut: int, s: np.ndarray | None = None):
+    """WHERE payload < cut GROUP BY key: COUNT(*), SUM(payload)[, COUNT(DISTINCT s)] restated in numpy
+    (a sort instead of a hash table; exact int64 sums, which hold while every group's sum is below 2^63).
+    Returns [keys, counts, sums(, distinct counts)] sorted by key.  At 100M rows this takes seconds
+    where aggregate()'s per-thread hash maps take minutes."""
+    m = payload < cut
+    k, p = key[m], payload[m]
+    order = np.argsort(k)
+    ks = k[order]
+    starts = np.flatnonzero(np.concatenate(([True], ks[1:] != ks[:-1]))) if ks.size else np.zeros(0, np.int64)
+    cnt = np.diff(np.append(starts, ks.size)).astype(np.int64)
+    sums = np.add.reduceat(p[order], starts) if ks.size else np.zeros(0, np.int64)
+    cols = [ks[starts], cnt, sums]
+    if s is not None:
+        gid = np.repeat(np.arange(starts.size, dtype=np.int64), cnt)
+        sv = s[m][order].astype(np.int64)
+        assert sv.size == 0 or (sv.min() >= 0 and sv.max() < (1 << 23))
+        pairs = np.sort((gid << 23) | sv)
+        first = np.concatenate(([True], pairs[1:] != pairs[:-1])) if pairs.size else np.zeros(0, bool)
+        cols.append(np.bincount(pairs[first] >> 23, minlength=starts.size).astype(np.int64))
+    return cols

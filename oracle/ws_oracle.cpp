@@ -839,6 +839,16 @@ int runAggregate(const ws_expr_env* env, const ws_agg_plan* plan, const ws_prog*
 
 extern "C" {
 
+// Static type of an expression (1 = int64, 0 = double), as buildTree types it; -1 when malformed.
+int ws_oracle_prog_is_int(const ws_expr_env* env, ws_prog p) {
+  try {
+    const Tree t = buildTree(*env, p);
+    return t.nodes[t.root].isInt ? 1 : 0;
+  } catch (...) {
+    return -1;
+  }
+}
+
 double ws_oracle_eval(const ws_expr_env* env, const ws_col_view* cols, ws_prog prog, int64_t row, int64_t* ival,
                       int* is_int, int* ovf) {
   Tree t = buildTree(*env, prog);

@@ -21,6 +21,8 @@ typedef struct ws_oracle_result ws_oracle_result;
 /* Typed evaluation of one expression for one row of a batch (cols = that batch's views).
  * Returns the value as a double (NaN = NULL) and, when the expression is integer-typed, the exact
  * int64 in *ival with *is_int = 1.  *ovf is set when checked int64 arithmetic overflowed. */
+/* Static type of an expression: 1 int64, 0 double, -1 malformed. */
+int ws_oracle_prog_is_int(const ws_expr_env* env, ws_prog p);
 double ws_oracle_eval(const ws_expr_env* env, const ws_col_view* cols, ws_prog prog, int64_t row, int64_t* ival,
                       int* is_int, int* ovf);
 

@@ -43,8 +43,8 @@ def test_mlp_kernel_matches_forward_pass():
 
 def test_learned_sizing_same_result_fewer_runs(table):
     e, aq, dprog = W.high_cardinality_query(table, W.high_cardinality_cut(9), distinct=True)
-    plain = W.distinct_aggregate_run(table.batches(True), e, aq, dprog, table.n, "ours")
-    learned = W.distinct_aggregate_run(table.batches(True), e, aq, dprog, table.n, "ours", sizing="learned")
+    plain = W.distinct_aggregate_run(table.batches(True), e, aq, dprog, table.n)
+    learned = W.distinct_aggregate_run(table.batches(True), e, aq, dprog, table.n, sizing="learned")
     assert learned[3] == plain[3]
     assert learned[2] <= plain[2]
     kp, kl = np.ascontiguousarray(plain[0]).view(np.int64)[:, 0], np.ascontiguousarray(learned[0]).view(np.int64)[:, 0]

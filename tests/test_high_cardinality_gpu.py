@@ -1,7 +1,8 @@
 """High-cardinality hash GROUP BY (Zipf keys, millions of groups) and COUNT(DISTINCT) as the engine
 composes it (phase 1 GROUP BY (keys, x), compaction on the device, phase 2 GROUP BY keys): this
 library's operators against the CPU oracle (row-exact groups) and against the same pipeline on the
-reference's own operators; the full-size case prints both pipelines' times."""
+reference's own operators; at full size against an exact numpy restatement of the query and the
+reference; the full-size case prints both pipelines' times."""
 import time
 from contextlib import contextmanager
 
@@ -12,6 +13,8 @@ import torch
 from oracle import oracle, ref
 from warpstore_b200 import abi, ops
 from warpstore_b200 import workloads as W
+
+from . import ref_pipelines as RP
 
 pytestmark = pytest.mark.gpu
 
@@ -37,6 +40,12 @@ def oracle_arrays(aq, okeys, owords, distinct=False):
     return [c[order] for c in cols]
 
 
+def exact_groups_np(t, cut, distinct=False):
+    """The full-size query restated in numpy (the oracle's groupby_count_sum_np): sorted by key."""
+    key, payload, s = (t.cols[c].data for c in range(3))
+    return oracle.groupby_count_sum_np(key, payload, cut, s if distinct else None)
+
+
 def assert_same(a, b, what):
     assert len(a[0]) == len(b[0]), f"{what}: group count {len(a[0])} vs {len(b[0])}"
     for i, (x, y) in enumerate(zip(a, b)):
@@ -59,7 +68,7 @@ def test_zipf_hash_groupby_matches_oracle_and_reference(small, jit):
     try:
         prog = ops.jit_get(e.env, e.ncols, aq.plan, abi.JF_GROUPED, "hc") if jit else None
         # deliberately small first capacity: exercises the overflow retry
-        keys, accs, cap, runs = W.hash_aggregate_run(t.batches(True), e, aq, 1 << 14, "ours", prog)
+        keys, accs, cap, runs = W.hash_aggregate_run(t.batches(True), e, aq, 1 << 14, prog)
     finally:
         ops.jit_set_mode(-1)
     assert runs > 1
@@ -67,26 +76,26 @@ def test_zipf_hash_groupby_matches_oracle_and_reference(small, jit):
     ok, ow, _ = oracle.aggregate(e.env, aq.plan, t.batches(False), e.ncols)
     assert_same(got, oracle_arrays(aq, ok, ow), "ours vs oracle")
     if ref.available():
-        rk, ra, _, _ = W.hash_aggregate_run(t.batches(True), e, aq, cap, "reference")
+        rk, ra, _, _ = RP.hash_aggregate_run(t.batches(True), e, aq, cap)
         assert_same(got, engine_arrays(aq, rk, ra), "ours vs reference")
 
 
 def test_count_distinct_two_phase_matches_oracle_and_reference(small):
     t = small
     e, aq, dprog = W.high_cardinality_query(t, W.high_cardinality_cut(5), distinct=True)
-    keys, accs, runs, pairs = W.distinct_aggregate_run(t.batches(True), e, aq, dprog, t.n, "ours")
+    keys, accs, runs, pairs = W.distinct_aggregate_run(t.batches(True), e, aq, dprog, t.n)
     got = engine_arrays(aq, keys, accs, distinct=True)
     ok, ow, _ = oracle.aggregate_distinct(e.env, aq.plan, dprog, True, t.batches(False), e.ncols)
     assert_same(got, oracle_arrays(aq, ok, ow, distinct=True), "ours vs oracle")
     assert got[3].sum() == pairs
     if ref.available():
-        rk, ra, rruns, rpairs = W.distinct_aggregate_run(t.batches(True), e, aq, dprog, t.n, "reference")
+        rk, ra, rruns, rpairs = RP.distinct_aggregate_run(t.batches(True), e, aq, dprog, t.n)
         assert rpairs == pairs
         assert_same(got, engine_arrays(aq, rk, ra, distinct=True), "ours vs reference")
 
 
 @pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
-def test_high_cardinality_full_size_vs_reference():
+def test_high_cardinality_full_size_vs_exact_and_reference():
     t = W.high_cardinality()
     t.to_device()
     cut = W.high_cardinality_cut()
@@ -106,38 +115,47 @@ def test_high_cardinality_full_size_vs_reference():
         ops.jit_set_mode(abi.JIT_SYNC)
         prog = ops.jit_get(e.env, e.ncols, aq.plan, abi.JF_GROUPED, "hc")
         ops.jit_set_mode(-1)
+        runners = {"ours": lambda: W.hash_aggregate_run(t.batches(True), e, aq, cap, prog),
+                   "reference": lambda: RP.hash_aggregate_run(t.batches(True), e, aq, cap)}
         res = {}
         for impl in ("ours", "reference"):
-            W.hash_aggregate_run(t.batches(True), e, aq, cap, impl, prog if impl == "ours" else None)  # warm
+            runners[impl]()  # warm
             with timed((impl, "group by")):
-                res[impl] = W.hash_aggregate_run(t.batches(True), e, aq, cap, impl, prog if impl == "ours" else None)
-        assert_same(engine_arrays(aq, *res["ours"][:2]), engine_arrays(aq, *res["reference"][:2]), "group by")
+                res[impl] = runners[impl]()
+        got = engine_arrays(aq, *res["ours"][:2])
+        exact = exact_groups_np(t, cut, distinct=True)
+        assert_same(got, exact[:3], "group by: ours vs exact numpy")
+        assert_same(got, engine_arrays(aq, *res["reference"][:2]), "group by: ours vs reference")
         ngroups = res["ours"][0].shape[0]
 
         e2, aq2, dprog = W.high_cardinality_query(t, cut, distinct=True)
+        druns = {"ours": lambda timer=None: W.distinct_aggregate_run(t.batches(True), e2, aq2, dprog, t.n, timer),
+                 "reference": lambda timer=None: RP.distinct_aggregate_run(t.batches(True), e2, aq2, dprog, t.n, timer)}
         dres = {}
         for impl in ("ours", "reference"):  # warm: plans compiled, the memory pool grown to the largest table
-            W.distinct_aggregate_run(t.batches(True), e2, aq2, dprog, t.n, impl)
+            druns[impl]()
         for impl in ("ours", "reference"):
             @contextmanager
             def stage(name):
                 with timed((impl, name)):
                     yield
 
-            dres[impl] = W.distinct_aggregate_run(t.batches(True), e2, aq2, dprog, t.n, impl, stage)
+            dres[impl] = druns[impl](stage)
         # learned sizing of the phase-1 table (ours): same result, fewer overflow reruns
-        W.distinct_aggregate_run(t.batches(True), e2, aq2, dprog, t.n, "ours", sizing="learned")  # warm
+        W.distinct_aggregate_run(t.batches(True), e2, aq2, dprog, t.n, sizing="learned")  # warm
 
         @contextmanager
         def lstage(name):
             with timed(("learned", name)):
                 yield
 
-        dres["learned"] = W.distinct_aggregate_run(t.batches(True), e2, aq2, dprog, t.n, "ours", lstage, sizing="learned")
+        dres["learned"] = W.distinct_aggregate_run(t.batches(True), e2, aq2, dprog, t.n, lstage, sizing="learned")
         assert dres["learned"][3] == dres["ours"][3]
         assert dres["ours"][3] == dres["reference"][3]
-        assert_same(engine_arrays(aq2, *dres["ours"][:2], distinct=True),
-                    engine_arrays(aq2, *dres["reference"][:2], distinct=True), "count distinct")
+        dgot = engine_arrays(aq2, *dres["ours"][:2], distinct=True)
+        assert_same(dgot, exact, "count distinct: ours vs exact numpy")
+        assert_same(dgot, engine_arrays(aq2, *dres["learned"][:2], distinct=True), "count distinct: learned sizing")
+        assert_same(dgot, engine_arrays(aq2, *dres["reference"][:2], distinct=True), "count distinct: ours vs reference")
         print(f"\n[timing] high-cardinality GROUP BY {t.n} rows, {ngroups} groups, capacity {cap}")
         for s in ("group by", "phase 1 (keys, x)", "phase 2 (keys)"):
             r, o = times[("reference", s)], times[("ours", s)]

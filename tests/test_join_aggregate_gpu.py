@@ -12,6 +12,7 @@ from oracle import oracle, ref
 from warpstore_b200 import abi
 from warpstore_b200 import workloads as W
 
+from . import ref_pipelines as RP
 from .tests_join_util import oracle_join_aggregate
 
 pytestmark = pytest.mark.gpu
@@ -32,18 +33,18 @@ def engine_groups(aq, keys, accs):
 def test_join_aggregate_matches_oracle_and_reference():
     build, probe = W.join_tables(1_500_000, 6_000_000, seed=5)
     plans = W.join_aggregate_plans()
-    keys, accs, m = W.join_aggregate_run(build, probe, plans, "ours")
+    keys, accs, m = W.join_aggregate_run(build, probe, plans)
     got = engine_groups(plans[3], keys, accs)
     want, wm = oracle_join_aggregate(build, probe, plans)
     assert m == wm
     assert got == want
     if ref.available():
-        rk, ra, rm = W.join_aggregate_run(build, probe, plans, "reference")
+        rk, ra, rm = RP.join_aggregate_run(build, probe, plans)
         assert rm == m and engine_groups(plans[3], rk, ra) == got
 
 
 @pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
-def test_join_aggregate_full_size_vs_reference():
+def test_join_aggregate_full_size_vs_oracle_and_reference():
     build, probe = W.join_tables()
     plans = W.join_aggregate_plans()
     times = {}
@@ -60,12 +61,16 @@ def test_join_aggregate_full_size_vs_reference():
             times[(impl, name)] = 1e3 * (time.perf_counter() - t0)
         return t
 
+    runners = {"ours": W.join_aggregate_run, "reference": RP.join_aggregate_run}
     res = {}
     for impl in ("ours", "reference"):
-        W.join_aggregate_run(build, probe, plans, impl)  # warm (plans compiled, pools grown)
-        res[impl] = W.join_aggregate_run(build, probe, plans, impl, timer_for(impl))
+        runners[impl](build, probe, plans)  # warm (plans compiled, pools grown)
+        res[impl] = runners[impl](build, probe, plans, timer_for(impl))
+    got = engine_groups(plans[3], *res["ours"][:2])
+    want, wm = oracle_join_aggregate(build, probe, plans)
+    assert res["ours"][2] == wm and got == want
     assert res["ours"][2] == res["reference"][2]
-    assert engine_groups(plans[3], *res["ours"][:2]) == engine_groups(plans[3], *res["reference"][:2])
+    assert got == engine_groups(plans[3], *res["reference"][:2])
     stages = ["select", "gather build keys", "join", "gather probe columns", "aggregate"]
     print(f"\n[timing] join+aggregate build {build.n} probe {probe.n} pairs {res['ours'][2]}")
     for s in stages:

@@ -46,68 +46,71 @@ WS_DI void rowGroup(Ev& ev, unsigned live, int b, i64 r0, F&& f) {
   }
 }
 
-// First tile of batch b (tiles [t0, t1) of the launch) that this CTA owns: the CTA takes every
-// tile t with t = blockIdx.x (mod gridDim.x).
-WS_DI i64 firstOwnedTile(i64 t0) {
-  const i64 G = gridDim.x;
-  i64 r = ((i64)blockIdx.x - t0) % G;
-  if (r < 0) r += G;
-  return t0 + r;
+// The batch holding tile t of the launch (tileStart[b] <= t < tileStart[b + 1]; empty batches skipped).
+WS_DI int batchOfTile(const Launch& L, i64 t) {
+  int lo = 0, hi = L.nb - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(L.tileStart + mid) <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
 }
 
-// Visits every live row (not deleted, passing the filter) of the tiles this CTA owns, batch by batch
-// (the batch's size, bitmap and column views are read once per batch, not per tile).
-// f(i, batch, row) is called with i = the row's position (0..3) in the evaluator's 4-row group.
-// tileEnd() is called by every thread of the CTA after each of the CTA's tiles (a CTA-uniform point);
-// it returns the same value in every thread, true to end the visit there.
-template <class Ev, class F, class E>
-WS_DI void forEachRowTiles(const Launch& L, Ev& ev, F&& f, E&& tileEnd) {
-  for (int b = 0; b < L.nb; ++b) {
-    const i64 t0 = __ldg(L.tileStart + b), t1 = __ldg(L.tileStart + b + 1);
-    i64 t = firstOwnedTile(t0);
-    if (t >= t1) continue;
+// Walks the tiles this CTA owns: the contiguous range [T c / G, T (c + 1) / G) of the launch's T tiles
+// (c = blockIdx.x, G = gridDim.x), batch by batch.  A CTA crosses one or two batches, so the batch's
+// size, bitmap and column views (and an encoded column's header) are read once or twice per CTA
+// rather than once per batch of the launch.  tile(t, b, r0, n, del) is called by every thread of the
+// CTA for each tile t of batch b (r0 = the thread's first row in the batch, n = the batch's rows,
+// del = its deleted bitmap); it returns true to end the walk (the same value in every thread).
+template <class Ev, class F>
+WS_DI void forEachOwnedTile(const Launch& L, Ev& ev, F&& tile) {
+  const i64 T = L.ntiles, G = gridDim.x;
+  i64 t = T * (i64)blockIdx.x / G;
+  const i64 tEnd = T * ((i64)blockIdx.x + 1) / G;
+  if (t >= tEnd) return;
+  for (int b = batchOfTile(L, t); t < tEnd && b < L.nb; ++b) {
+    const i64 bs = __ldg(L.tileStart + b), bend = __ldg(L.tileStart + b + 1), be = bend < tEnd ? bend : tEnd;
+    if (t >= be) continue;  // an empty batch
     ev.bind(L, b);
     const i64 n = __ldg(L.n + b);
     const uint32_t* del = L.del[b];
-    for (; t < t1; t += gridDim.x) {
-      const i64 r0 = (t - t0) * kTile + threadIdx.x * 4;
-      const i64 left = n - r0;
-      if (left > 0) {
-        const int nv = left >= 4 ? 4 : (int)left;
-        ev.load(r0, ev.fastOk && nv == 4, nv);
-        unsigned live = (1u << nv) - 1;
-        if (del) live &= ~(__ldg(del + (r0 >> 5)) >> (r0 & 31)) & 0xfu;
-        rowGroup(ev, live, b, r0, f);
-      }
-      if (tileEnd()) {
-        ev.finish();
-        return;
-      }
-    }
+    for (; t < be; ++t)
+      if (tile(t, b, (t - bs) * kTile + threadIdx.x * 4, n, del)) return;
   }
+}
+
+// Loads the thread's 4 rows from r0 and visits the live ones (not deleted, passing the filter).
+template <class Ev, class F>
+WS_DI void visitRows(Ev& ev, int b, i64 r0, i64 n, const uint32_t* del, F&& f) {
+  const i64 left = n - r0;
+  if (left <= 0) return;
+  const int nv = left >= 4 ? 4 : (int)left;
+  ev.load(r0, ev.fastOk && nv == 4, nv);
+  unsigned live = (1u << nv) - 1;
+  if (del) live &= ~(__ldg(del + (r0 >> 5)) >> (r0 & 31)) & 0xfu;
+  rowGroup(ev, live, b, r0, f);
+}
+
+// Visits every live row of the tiles this CTA owns.  f(i, batch, row) is called with i = the row's
+// position (0..3) in the evaluator's 4-row group.  tileEnd() is called by every thread of the CTA
+// after each of the CTA's tiles (a CTA-uniform point); it returns the same value in every thread,
+// true to end the visit there.
+template <class Ev, class F, class E>
+WS_DI void forEachRowTiles(const Launch& L, Ev& ev, F&& f, E&& tileEnd) {
+  forEachOwnedTile(L, ev, [&](i64, int b, i64 r0, i64 n, const uint32_t* del) {
+    visitRows(ev, b, r0, n, del, f);
+    return tileEnd();
+  });
   ev.finish();
 }
 
 template <class Ev, class F>
 WS_DI void forEachRow(const Launch& L, Ev& ev, F&& f) {
-  for (int b = 0; b < L.nb; ++b) {
-    const i64 t0 = __ldg(L.tileStart + b), t1 = __ldg(L.tileStart + b + 1);
-    i64 t = firstOwnedTile(t0);
-    if (t >= t1) continue;
-    ev.bind(L, b);
-    const i64 n = __ldg(L.n + b);
-    const uint32_t* del = L.del[b];
-    for (; t < t1; t += gridDim.x) {
-      const i64 r0 = (t - t0) * kTile + threadIdx.x * 4;
-      const i64 left = n - r0;
-      if (left <= 0) continue;
-      const int nv = left >= 4 ? 4 : (int)left;
-      ev.load(r0, ev.fastOk && nv == 4, nv);
-      unsigned live = (1u << nv) - 1;
-      if (del) live &= ~(__ldg(del + (r0 >> 5)) >> (r0 & 31)) & 0xfu;
-      rowGroup(ev, live, b, r0, f);
-    }
-  }
+  forEachOwnedTile(L, ev, [&](i64, int b, i64 r0, i64 n, const uint32_t* del) {
+    visitRows(ev, b, r0, n, del, f);
+    return false;
+  });
   ev.finish();
 }
 
@@ -138,17 +141,19 @@ WS_DI void forEachRowStaged(const Launch& L, Ev& ev, unsigned char* stages, int 
     fenceProxyAsync();
   }
   __syncthreads();
-  const i64 K = L.ntiles > (i64)blockIdx.x ? (L.ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+  // this CTA's tiles: the contiguous range [tFirst, tFirst + K) (as forEachOwnedTile)
+  const i64 tFirst = L.ntiles * (i64)blockIdx.x / gridDim.x;
+  const i64 K = L.ntiles * ((i64)blockIdx.x + 1) / gridDim.x - tFirst;
   if (warp == kConsumerWarps) {  // ---- producer warp (one elected lane)
     if (lane == 0) {
-      int pb = 0, pbatch = -1;
+      int pb = K > 0 ? batchOfTile(L, tFirst) : 0, pbatch = -1;
       for (i64 k = 0; k < K; ++k) {
         const int s = (int)(k % S);
         if (k >= S && !mbarWait(smemAddr(&empty[s]), (unsigned)(((k / S) - 1) & 1))) {
           L.err[2] = 1;
           break;
         }
-        const i64 t = blockIdx.x + k * (i64)gridDim.x;
+        const i64 t = tFirst + k;
         while (t >= __ldg(L.tileStart + pb + 1)) ++pb;
         if (pb != pbatch) {
           Ev::stageBind(L, pb, pst);
@@ -171,9 +176,9 @@ WS_DI void forEachRowStaged(const Launch& L, Ev& ev, unsigned char* stages, int 
     return;
   }
   // ---- consumer warps
-  int b = 0, bound = -1;
+  int b = K > 0 ? batchOfTile(L, tFirst) : 0, bound = -1;
   for (i64 k = 0; k < K; ++k) {
-    const i64 t = blockIdx.x + k * (i64)gridDim.x;
+    const i64 t = tFirst + k;
     const int s = (int)(k % S);
     if (!mbarWait(smemAddr(&full[s]), (unsigned)((k / S) & 1))) {
       L.err[2] = 1;
@@ -829,15 +834,7 @@ template <class Ev>
 __device__ void selectCount(const Launch& L) {
   __shared__ int wcount[kThreads / 32];
   Ev ev(L);
-  for (int b = 0; b < L.nb; ++b) {
-  const i64 t0 = __ldg(L.tileStart + b), t1 = __ldg(L.tileStart + b + 1);
-  i64 t = firstOwnedTile(t0);
-  if (t >= t1) continue;
-  ev.bind(L, b);
-  const i64 n = __ldg(L.n + b);
-  const uint32_t* del = L.del[b];
-  for (; t < t1; t += gridDim.x) {
-    const i64 r0 = (t - t0) * kTile + threadIdx.x * 4;
+  forEachOwnedTile(L, ev, [&](i64 t, int, i64 r0, i64 n, const uint32_t* del) {
     int c = 0;
     if (r0 < n) {
       const int nv = n - r0 >= 4 ? 4 : (int)(n - r0);
@@ -857,8 +854,8 @@ __device__ void selectCount(const Launch& L) {
       L.tileCount[t] = s;
     }
     __syncthreads();
-  }
-  }
+    return false;
+  });
   ev.finish();
 }
 
@@ -867,15 +864,7 @@ __device__ void selectWrite(const Launch& L) {
   __shared__ int woff[kThreads / 32];
   Ev ev(L);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int b = 0; b < L.nb; ++b) {
-  const i64 t0 = __ldg(L.tileStart + b), t1 = __ldg(L.tileStart + b + 1);
-  i64 t = firstOwnedTile(t0);
-  if (t >= t1) continue;
-  ev.bind(L, b);
-  const i64 n = __ldg(L.n + b);
-  const uint32_t* del = L.del[b];
-  for (; t < t1; t += gridDim.x) {
-    const i64 r0 = (t - t0) * kTile + threadIdx.x * 4;
+  forEachOwnedTile(L, ev, [&](i64 t, int b, i64 r0, i64 n, const uint32_t* del) {
     unsigned sel = 0;
     if (r0 < n) {
       const int nv = n - r0 >= 4 ? 4 : (int)(n - r0);
@@ -906,8 +895,8 @@ __device__ void selectWrite(const Launch& L) {
     for (int i = 0; i < 4; ++i)
       if ((sel >> i) & 1u) L.outIdx[out0 + k++] = (int32_t)(g0 + i);
     __syncthreads();
-  }
-  }
+    return false;
+  });
   ev.finish();
 }
 

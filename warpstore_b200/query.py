@@ -20,6 +20,12 @@ from dataclasses import dataclass, field
 from . import abi
 
 
+# Typing of compiled expressions, (ExprEnv, Prog) -> bool.  None: the library's own (ws_prog_is_int).
+# A caller timing another implementation of the operators sets its own, so that building the plans
+# loads nothing of this library's native code.
+TYPER = None
+
+
 def _i2d(v: int) -> float:
     """The double whose bit pattern is the int64 v (integer literals, src/engine_core.h:1505-1514)."""
     return struct.unpack("<d", struct.pack("<q", v))[0]
@@ -149,7 +155,9 @@ class Env:
         return abi.Prog(start, self.ncode - start)
 
     def is_int(self, prog: abi.Prog) -> bool:
-        """Static type of a compiled expression (the library's typing, host only)."""
+        """Static type of a compiled expression: the library's typing (host only), or TYPER's when set."""
+        if TYPER is not None:
+            return bool(TYPER(self.env, prog))
         from ._lib import lib
         return bool(lib().ws_prog_is_int(C.byref(self.env), prog))
 

@@ -280,11 +280,10 @@ def join_aggregate_plans(cutoff: int = 1203):
     return eb, where, ej, aq, ds
 
 
-def join_aggregate_run(build: Table, probe: Table, plans, impl: str = "ours", timer=None):
+def join_aggregate_run(build: Table, probe: Table, plans, timer=None):
     """The engine's join pipeline on the device: select build rows (order_date < cutoff), gather their
     keys, inner hash join with the probe keys, gather the probe's gkey and cents for the pairs, dense
-    GROUP BY gkey: COUNT, SUM(cents).  impl "ours" runs this library's operators, "reference" the
-    reference's (oracle/_ref, tests only).  timer(name) -> context manager timing a stage.
+    GROUP BY gkey: COUNT, SUM(cents).  timer(name) -> context manager timing a stage.
     Returns (keys, accs in the engine format, pairs)."""
     import contextlib
 
@@ -295,53 +294,33 @@ def join_aggregate_run(build: Table, probe: Table, plans, impl: str = "ours", ti
     probe.to_device()
     keyv = contiguous_view(build, 0, True)
     fkv = contiguous_view(probe, 0, True)
-    if impl == "ours":
-        ops.jit_set_mode(abi.JIT_SYNC)
-        fp = abi.AggPlan()
-        fp.hasWhere, fp.where, fp.naggs = 1, where, 1
-        fp.ops[0] = abi.AGG_COUNT
-        fprog = ops.jit_get(eb.env, eb.ncols, fp, abi.JF_FLAGM, "join build filter")
-        aprog = ops.jit_get(ej.env, ej.ncols, aq.plan, abi.JF_DENSE, "join aggregate")
-        with timer("select"):
-            idx, mb, _ = ops.select_multi(eb.env, where, build.batches(True), eb.ncols, fprog)
-        bkeys = ops.DeviceBuffer(max(mb, 1) * 8)
-        with timer("gather build keys"):
-            ops.gather(keyv.p, abi.PT_I64, idx, mb, bkeys.ptr)
-        with timer("join"):
-            ob, op, m = ops.hash_join(abi.ColView(bkeys.ptr, abi.T_I64, 0, 0, 0), mb, fkv, probe.n)
-        gk, ct = ops.DeviceBuffer(max(m, 1) * 4), ops.DeviceBuffer(max(m, 1) * 8)
-        with timer("gather probe columns"):
-            ops.gather(probe.cols[2].dev.ptr, abi.PT_I32, op, m, gk.ptr)
-            ops.gather(probe.cols[1].dev.ptr, abi.PT_I64, op, m, ct.ptr)
-        with timer("aggregate"):
-            agg = ops.GpuAggregator(aq.plan, 1024, ds)
-            agg.add_batches(ej.ncols, [(m, 0, [abi.ColView(gk.ptr, abi.T_I32, 0, 0, 0),
-                                               abi.ColView(ct.ptr, abi.T_I64, 0, 0, 0)])])
-            agg.run(ej.env, aprog)
-            keys, accs, _ = agg.fetch(exact=False)
-        agg.close()
-        for p in (idx, ob, op):
-            ops.tmp_free(p)
-        ops.jit_set_mode(-1)
-        return keys, accs, m
-    from oracle import ref  # the reference's operators (test infrastructure)
+    ops.jit_set_mode(abi.JIT_SYNC)
+    fp = abi.AggPlan()
+    fp.hasWhere, fp.where, fp.naggs = 1, where, 1
+    fp.ops[0] = abi.AGG_COUNT
+    fprog = ops.jit_get(eb.env, eb.ncols, fp, abi.JF_FLAGM, "join build filter")
+    aprog = ops.jit_get(ej.env, ej.ncols, aq.plan, abi.JF_DENSE, "join aggregate")
     with timer("select"):
-        idx, mb, _ = ref.select_multi_dev(eb.env, where, build.batches(True), eb.ncols)
+        idx, mb, _ = ops.select_multi(eb.env, where, build.batches(True), eb.ncols, fprog)
     bkeys = ops.DeviceBuffer(max(mb, 1) * 8)
     with timer("gather build keys"):
-        ref.gather(keyv.p, abi.PT_I64, idx, mb, bkeys.ptr)
+        ops.gather(keyv.p, abi.PT_I64, idx, mb, bkeys.ptr)
     with timer("join"):
-        ob, op, m, _ = ref.hash_join_dev(abi.ColView(bkeys.ptr, abi.T_I64, 0, 0, 0), mb, fkv, probe.n)
+        ob, op, m = ops.hash_join(abi.ColView(bkeys.ptr, abi.T_I64, 0, 0, 0), mb, fkv, probe.n)
     gk, ct = ops.DeviceBuffer(max(m, 1) * 4), ops.DeviceBuffer(max(m, 1) * 8)
     with timer("gather probe columns"):
-        ref.gather(probe.cols[2].dev.ptr, abi.PT_I32, op, m, gk.ptr)
-        ref.gather(probe.cols[1].dev.ptr, abi.PT_I64, op, m, ct.ptr)
+        ops.gather(probe.cols[2].dev.ptr, abi.PT_I32, op, m, gk.ptr)
+        ops.gather(probe.cols[1].dev.ptr, abi.PT_I64, op, m, ct.ptr)
     with timer("aggregate"):
-        keys, accs, _, ovf, _ = ref.aggregate(ej.env, ej.ncols, aq.plan,
-                                              [(m, 0, [abi.ColView(gk.ptr, abi.T_I32, 0, 0, 0),
-                                                       abi.ColView(ct.ptr, abi.T_I64, 0, 0, 0)])], ds, 1024)
+        agg = ops.GpuAggregator(aq.plan, 1024, ds)
+        agg.add_batches(ej.ncols, [(m, 0, [abi.ColView(gk.ptr, abi.T_I32, 0, 0, 0),
+                                           abi.ColView(ct.ptr, abi.T_I64, 0, 0, 0)])])
+        agg.run(ej.env, aprog)
+        keys, accs, _ = agg.fetch(exact=False)
+    agg.close()
     for p in (idx, ob, op):
-        ref.free(p)
+        ops.tmp_free(p)
+    ops.jit_set_mode(-1)
     return keys, accs, m
 
 
@@ -427,30 +406,23 @@ def grow_capacity(cap: int, groups: int) -> int:
     return c
 
 
-def hash_aggregate_run(batches: list, e, aq, cap: int, impl: str = "ours", jit=None):
+def hash_aggregate_run(batches: list, e, aq, cap: int, jit=None):
     """GROUP BY over device batches with the engine's overflow retry: (keys, accs engine format,
     final capacity, runs)."""
     from . import ops
     runs = 0
     while True:
         runs += 1
-        if impl == "ours":
-            agg = ops.GpuAggregator(aq.plan, cap)
-            agg.add_batches(e.ncols, batches)
-            agg.run(e.env, jit)
-            if agg.overflowed():
-                g = agg.group_count()
-                agg.close()
-                cap = grow_capacity(cap, g)
-                continue
-            keys, accs, _ = agg.fetch(exact=False)
+        agg = ops.GpuAggregator(aq.plan, cap)
+        agg.add_batches(e.ncols, batches)
+        agg.run(e.env, jit)
+        if agg.overflowed():
+            g = agg.group_count()
             agg.close()
-            return keys, accs, cap, runs
-        from oracle import ref  # the reference's operators (test infrastructure)
-        keys, accs, g, ovf, _ = ref.aggregate(e.env, e.ncols, aq.plan, batches, None, cap)
-        if ovf:
             cap = grow_capacity(cap, g)
             continue
+        keys, accs, _ = agg.fetch(exact=False)
+        agg.close()
         return keys, accs, cap, runs
 
 
@@ -509,13 +481,12 @@ def distinct_phase2(plan: abi.AggPlan, p1: abi.AggPlan, keys_ptr: int, accs_ptr:
     return env2, nk + 1 + na, p2
 
 
-def distinct_aggregate_run(batches: list, e, aq, dprog, rows_in: int, impl: str = "ours", timer=None,
-                           sizing: str = "plain"):
+def distinct_aggregate_run(batches: list, e, aq, dprog, rows_in: int, timer=None, sizing: str = "plain"):
     """GROUP BY keys with COUNT(DISTINCT x) as the engine runs it: phase 1 hash GROUP BY (keys, x)
     with capacity pow2 >= min(rows, 2^22) and the overflow retry, compaction on the device, phase 2
     GROUP BY keys over the distinct pairs (src/engine_select.cpp:1397-1492).  Returns (keys, accs in
     the engine format with the distinct count as the last slot, phase-1 runs, distinct pairs).
-    sizing "learned" (ours only): the phase-1 table is sized from the estimator's prediction of the
+    sizing "learned": the phase-1 table is sized from the estimator's prediction of the
     pair count instead (estimator.py), the plain overflow retry remaining the fallback."""
     import contextlib
 
@@ -526,62 +497,41 @@ def distinct_aggregate_run(batches: list, e, aq, dprog, rows_in: int, impl: str 
     while cap1 < min(max(rows_in, 1), 1 << 22):
         cap1 <<= 1
     runs = 0
-    if impl == "ours":
-        ops.jit_set_mode(abi.JIT_SYNC)
-        try:
-            jit1 = ops.jit_get(e.env, e.ncols, p1, abi.JF_GROUPED, "aggregate (distinct pairs)")
-            with timer("phase 1 (keys, x)"):
-                if sizing == "learned":
-                    from . import estimator
-                    cap1 = estimator.learned_capacity(estimator.estimate_groups(e.env, e.ncols, p1, batches))
-                while True:
-                    runs += 1
-                    a1 = ops.GpuAggregator(p1, cap1)
-                    a1.add_batches(e.ncols, batches)
-                    a1.run(e.env, jit1)
-                    if a1.overflowed():
-                        g = a1.group_count()
-                        a1.close()
-                        cap1 = grow_capacity(cap1, g)
-                        continue
-                    kp, ap, g1 = a1.compact()
+    ops.jit_set_mode(abi.JIT_SYNC)
+    try:
+        jit1 = ops.jit_get(e.env, e.ncols, p1, abi.JF_GROUPED, "aggregate (distinct pairs)")
+        with timer("phase 1 (keys, x)"):
+            if sizing == "learned":
+                from . import estimator
+                cap1 = estimator.learned_capacity(estimator.estimate_groups(e.env, e.ncols, p1, batches))
+            while True:
+                runs += 1
+                a1 = ops.GpuAggregator(p1, cap1)
+                a1.add_batches(e.ncols, batches)
+                a1.run(e.env, jit1)
+                if a1.overflowed():
+                    g = a1.group_count()
                     a1.close()
-                    break
-            with timer("phase 2 (keys)"):
-                env2, nc2, p2 = distinct_phase2(aq.plan, p1, kp, ap, g1)
-                cap2 = 1024
-                while cap2 < 2 * g1:
-                    cap2 <<= 1
-                jit2 = ops.jit_get(env2, nc2, p2, abi.JF_GROUPED, "count distinct")
-                a2 = ops.GpuAggregator(p2, cap2)
-                a2.add_batches(nc2, [(g1, 0, [env2.cols[c] for c in range(nc2)])])
-                a2.run(env2, jit2)
-                if a2.overflowed():
-                    raise RuntimeError("phase 2 overflowed a table of twice the pair count")
-                keys, accs, _ = a2.fetch(exact=False)
-                a2.close()
-            ops.tmp_free(kp)
-            ops.tmp_free(ap)
-        finally:
-            ops.jit_set_mode(-1)
-        return keys, accs, runs, g1
-    from oracle import ref  # the reference's operators (test infrastructure)
-    with timer("phase 1 (keys, x)"):
-        while True:
-            runs += 1
-            kp, ap, g1, ovf, _ = ref.aggregate_compact(e.env, e.ncols, p1, batches, None, cap1)
-            if ovf:
-                cap1 = grow_capacity(cap1, g1)
-                continue
-            break
-    with timer("phase 2 (keys)"):
-        env2, nc2, p2 = distinct_phase2(aq.plan, p1, kp, ap, g1)
-        cap2 = 1024
-        while cap2 < 2 * g1:
-            cap2 <<= 1
-        keys, accs, _, ovf, _ = ref.aggregate(env2, nc2, p2, [(g1, 0, [env2.cols[c] for c in range(nc2)])], None, cap2)
-        if ovf:
-            raise RuntimeError("phase 2 overflowed a table of twice the pair count")
-    ref.free(kp)
-    ref.free(ap)
+                    cap1 = grow_capacity(cap1, g)
+                    continue
+                kp, ap, g1 = a1.compact()
+                a1.close()
+                break
+        with timer("phase 2 (keys)"):
+            env2, nc2, p2 = distinct_phase2(aq.plan, p1, kp, ap, g1)
+            cap2 = 1024
+            while cap2 < 2 * g1:
+                cap2 <<= 1
+            jit2 = ops.jit_get(env2, nc2, p2, abi.JF_GROUPED, "count distinct")
+            a2 = ops.GpuAggregator(p2, cap2)
+            a2.add_batches(nc2, [(g1, 0, [env2.cols[c] for c in range(nc2)])])
+            a2.run(env2, jit2)
+            if a2.overflowed():
+                raise RuntimeError("phase 2 overflowed a table of twice the pair count")
+            keys, accs, _ = a2.fetch(exact=False)
+            a2.close()
+        ops.tmp_free(kp)
+        ops.tmp_free(ap)
+    finally:
+        ops.jit_set_mode(-1)
     return keys, accs, runs, g1
