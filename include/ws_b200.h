@@ -58,6 +58,49 @@ int ws_gpu_trim_pool(void);
 int ws_host_alloc(size_t bytes, void** out);
 int ws_host_free(void* p);
 
+/* ---- tiered column storage (src/gpu.h:19-47: gpuSetVramLimit, gpuVramUsed, gpuVramFill, placeColumn,
+ *      releaseColumn, vramAcquire, vramRelease, hostMap, hostUnmap, gpuVramLimit, gpuVramFree).
+ * Segment columns live in device memory while the library's VRAM budget (ws_set_vram_limit; default
+ * none) has room, else their host bytes are pinned and mapped and kernels read them over PCIe.  Device
+ * copies made here are counted against the budget until released. */
+int ws_set_vram_limit(int64_t bytes);   /* INT64_MAX: no limit */
+int64_t ws_vram_used(void);             /* bytes of device copies made by ws_place_column / ws_vram_acquire /
+                                           ws_patch_column / ws_update_column and not yet released */
+int64_t ws_vram_limit(void);
+int64_t ws_vram_free(void);             /* free device memory (cudaMemGetInfo), 0 without a device */
+double ws_vram_fill(void);              /* used / limit, or the device's used fraction without a limit */
+/* placeColumn: *out = a device copy of host[0, bytes) (*mapped = 0) when the budget has room and
+ * host_only is 0, else host is pinned + mapped and *out its device address (*mapped = 1). */
+int ws_place_column(void* host, size_t bytes, int host_only, void** out, int* mapped);
+int ws_release_column(void* dev, void* host, size_t bytes, int mapped);
+/* vramAcquire: a device copy of host bytes, or *out = NULL when it does not fit (no error). */
+int ws_vram_acquire(const void* host, size_t bytes, void** out);
+int ws_vram_release(void* dev, size_t bytes);
+/* hostMap: host bytes pinned + mapped, *out = their device address (NULL when registering fails). */
+int ws_host_map(void* host, size_t bytes, void** out);
+int ws_host_unmap(void* host);
+
+/* ---- column-level UPDATE (src/gpu.h:24-41: gpuPatchColumn, gpuUpdateColumn).  Both return a new
+ * device copy of the column (counted against the VRAM budget; release with ws_vram_release), or
+ * *out = NULL when it does not fit.  rows (and vals) are host arrays of m entries. */
+/* gpuPatchColumn: the column (bytes, width 4 or 8) with rows[i] set to the width-byte value vals[i]. */
+int ws_patch_column(const void* old_dev, size_t bytes, int width, const int32_t* rows, const void* vals, int64_t m,
+                    void** out);
+/* gpuUpdateColumn (GpuUpdate, field for field): kind 0 sets rows[i] to i0 / d0, 1 to src[rows[i]],
+ * 2 to src[rows[i]] + add (integers, checked) / + add_d (doubles).  Integers must stay in [lo, hi]; NULLs
+ * (nul / NaN) stay NULL unless not_null (then bad).  Out: bad (nothing returned), saw_null, and mn / mx of
+ * the new non-NULL values (+inf / -inf when none). */
+typedef struct ws_update {
+  int32_t kind;
+  int64_t i0, add, nul, lo, hi;
+  double d0, add_d;
+  uint8_t not_null;
+  uint8_t bad, saw_null;
+  double mn, mx;
+} ws_update;
+int ws_update_column(const void* old_dev, const void* src, int64_t n, int w, int f64, const int32_t* rows, int64_t m,
+                     ws_update* u, void** out);
+
 /* ---- aggregation (src/gpu.h:84-130, class GpuAggregator).
  * Batches (segments, write buffers or a joined relation) are collected with ws_agg_add_batch and
  * aggregated by ws_agg_run in one pass.  Without GROUP BY there is one result row; with a dense spec
@@ -296,6 +339,34 @@ typedef struct ws_serve_options {
 } ws_serve_options;
 int ws_serve(ws_serve_query* queries, int n, const ws_serve_options* opt, double* wall_s);
 
+/* ---- distinct values, bitmaps and temp-table columns (src/gpu.h:150-167) */
+/* gpuDistinctInts: the distinct values in [base, base + span) of an integer expression at rows idx[j]
+ * (rows 0..m-1 when idx is null), ascending, NULLs skipped.  As the engine's: only programs built of
+ * integer columns (t 0, 1, 3, 4), integer literals, + - * and negation (stack depth <= 16) are
+ * evaluated (checked arithmetic); any other program yields no values.  out: max_out slots; fewer than
+ * the count: WS_ERR_SIZE with *count set. */
+int ws_distinct_ints(const ws_expr_env* env, int ncols, ws_prog prog, const int32_t* idx, int64_t m, int64_t base,
+                     int64_t span, int64_t* out, int64_t max_out, int64_t* count);
+/* gpuBitsFromColumn: *bits (nbits bits, cleared, at least one word; free with ws_dev_free) gets bit
+ * (v - base) of every non-NULL value v in [base, base + nbits) of an INT (out 0) / BIGINT (out 1) device
+ * column of n values; *saw_null: any NULL. */
+int ws_bits_from_column(const void* col, int out, int64_t n, int64_t base, int64_t nbits, uint32_t** bits,
+                        int* saw_null);
+/* gpuTempColumn (TempColSpec, field for field): one column of a temp table built from compacted GROUP BY
+ * results (keys [k * g + i], accs [a * g + i] on the device).  src 0: key idx; 1: aggregate slot idx with
+ * kind 0 value / div, 1 int64 bits, 2 split sum (hi * 2^32 + lo), 3 count, 4 average (sum / div / count);
+ * cnt >= 0: a group whose cnt slot is 0 is NULL; mul != 1 multiplies into a double.  out 0 int32, 1 int64,
+ * 2 double (NULLs: sentinels / NaN).  *col (ws_dev_free): g values; *mn / *mx: of an integer output
+ * (-inf / +inf for doubles or no value). */
+typedef struct ws_temp_col_spec {
+  int8_t src;
+  int32_t idx, hi, cnt;
+  uint8_t kind, key_int, sum_bits, out;
+  double div, mul;
+} ws_temp_col_spec;
+int ws_temp_column(const double* keys, int nk, const double* accs, int na, int64_t g, const ws_temp_col_spec* s,
+                   void** col, double* mn, double* mx);
+
 /* ---- ORDER BY (src/gpu.h:197-199) */
 /* gpuSortPerm: stable permutation sorting rows 0..m-1 by keys[0] (most significant) .. keys[nkeys-1],
  * each ascending or descending (desc[k] != 0); NULL (NaN) sorts as -inf (first ascending, last
@@ -303,6 +374,9 @@ int ws_serve(ws_serve_query* queries, int n, const ws_serve_options* opt, double
 int ws_sort_perm(const double* const* keys, const int* desc, int nkeys, int64_t m, int32_t** out_perm);
 /* gpuMapRank: keys[j] = rank[(int)keys[j]] (dictionary code -> lexicographic rank), NULL -> -1. */
 int ws_map_rank(double* keys, const int32_t* rank, int64_t m);
+/* gpuSortPermHost: the stable ascending sort permutation of a host column (ptype WS_PT_I32 / I64 / F64,
+ * keys compared as doubles), into the host array perm[n] (used when flushing sorted segments). */
+int ws_sort_perm_host(const void* host_col, int ptype, int64_t n, int32_t* perm);
 
 /* ---- compiled plans (src/jit.h:33-75) */
 typedef struct ws_jit_info {
@@ -329,6 +403,12 @@ int ws_jit_get(const ws_expr_env* env, int ncols, const ws_agg_plan* plan, int f
 int ws_prog_is_int(const ws_expr_env* env, ws_prog p);
 int ws_jit_program_info(const ws_jit_program* p, ws_jit_info* info);
 int ws_jit_source_of(int id, char* buf, size_t size, size_t* needed);
+/* The kind (field 0: "aggregate (dense)", ...), query text (1: the query that first compiled it) or
+ * generated source (2) of a cached plan (jitPlanCache / jitSourceOf, src/jit.h:61-73). */
+int ws_jit_plan_text(int id, int field, char* buf, size_t size, size_t* needed);
+/* Ids of the plans the calling thread's last query (ws_jit_begin_query .. ws_jit_end_query) used
+ * (JitQueryInfo::ids, src/jit.h:51-56); WS_ERR_SIZE when more than max_ids, with *n set. */
+int ws_jit_last_query_plans(int* ids, int max_ids, int* n);
 int ws_jit_plan_cache_count(void);
 int ws_jit_plan_cache_row(int i, ws_jit_info* info);
 int ws_jit_clear_cache(void);

@@ -7,6 +7,8 @@
 // The engine's own devtypes.h defines ColView / ExprEnv / AggPlan / DenseSpec / Prog with the same
 // layout as ws_types.h (checked below); define WS_GPU_ENGINE_TYPES when it is included first.
 #pragma once
+#include <algorithm>
+#include <cstddef>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
@@ -69,6 +71,65 @@ inline void d2h(void* dst, const void* src, size_t b) { wsCheck(ws_d2h(dst, src,
 inline void d2d(void* dst, const void* src, size_t b) { wsCheck(ws_d2d(dst, src, b)); }
 inline void gpuSync() { wsCheck(ws_gpu_sync()); }
 
+// ---- tiered column storage (src/gpu.h:19-47)
+inline void gpuSetVramLimit(int64_t bytes) { wsCheck(ws_set_vram_limit(bytes)); }
+inline int64_t gpuVramUsed() { return ws_vram_used(); }
+inline double gpuVramFill() { return ws_vram_fill(); }
+inline int64_t gpuVramLimit() { return ws_vram_limit(); }
+inline int64_t gpuVramFree() { return ws_vram_free(); }
+inline void* placeColumn(void* host, size_t bytes, bool& mapped, bool hostOnly = false) {
+  void* d = nullptr;
+  int m = 0;
+  wsCheck(ws_place_column(host, bytes, hostOnly ? 1 : 0, &d, &m));
+  mapped = m != 0;
+  return d;
+}
+inline void releaseColumn(void* dev, void* host, size_t bytes, bool mapped) {
+  wsCheck(ws_release_column(dev, host, bytes, mapped ? 1 : 0));
+}
+inline void* vramAcquire(const void* host, size_t bytes) {
+  void* d = nullptr;
+  wsCheck(ws_vram_acquire(host, bytes, &d));
+  return d;
+}
+inline void vramRelease(void* dev, size_t bytes) { wsCheck(ws_vram_release(dev, bytes)); }
+inline void* hostMap(void* host, size_t bytes) {
+  void* d = nullptr;
+  wsCheck(ws_host_map(host, bytes, &d));
+  return d;
+}
+inline void hostUnmap(void* host) { ws_host_unmap(host); }
+// column-level UPDATE (src/gpu.h:24-41)
+inline void* gpuPatchColumn(const void* oldDev, size_t bytes, int width, const int32_t* rows, const void* vals, int64_t m) {
+  void* d = nullptr;
+  wsCheck(ws_patch_column(oldDev, bytes, width, rows, vals, m, &d));
+  return d;
+}
+struct GpuUpdate {  // the engine's, field for field (ws_update)
+  int kind = 0;
+  int64_t i0 = 0, add = 0, nul = 0, lo = 0, hi = 0;
+  double d0 = 0, addD = 0;
+  bool notNull = false;
+  bool bad = false, sawNull = false;
+  double mn = 0, mx = 0;
+};
+static_assert(sizeof(GpuUpdate) == sizeof(ws_update) && offsetof(GpuUpdate, i0) == offsetof(ws_update, i0) &&
+                  offsetof(GpuUpdate, hi) == offsetof(ws_update, hi) && offsetof(GpuUpdate, addD) == offsetof(ws_update, add_d) &&
+                  offsetof(GpuUpdate, notNull) == offsetof(ws_update, not_null) &&
+                  offsetof(GpuUpdate, sawNull) == offsetof(ws_update, saw_null) && offsetof(GpuUpdate, mn) == offsetof(ws_update, mn) &&
+                  offsetof(GpuUpdate, mx) == offsetof(ws_update, mx),
+              "GpuUpdate and ws_update differ");
+inline void* gpuUpdateColumn(const void* old, const void* src, int64_t n, int w, bool f64, const int32_t* rows, int64_t m,
+                             GpuUpdate& u) {
+  ws_update c{};
+  c.kind = u.kind, c.i0 = u.i0, c.add = u.add, c.nul = u.nul, c.lo = u.lo, c.hi = u.hi, c.d0 = u.d0, c.add_d = u.addD;
+  c.not_null = u.notNull ? 1 : 0;
+  void* d = nullptr;
+  wsCheck(ws_update_column(old, src, n, w, f64 ? 1 : 0, rows, m, &c, &d));
+  u.bad = c.bad != 0, u.sawNull = c.saw_null != 0, u.mn = c.mn, u.mx = c.mx;
+  return d;
+}
+
 // RAII temp device array (src/gpu.h:59-79)
 template <class T>
 struct DevVec {
@@ -116,11 +177,57 @@ inline const JitProgram* jitGet(const ExprEnv& env, int ncols, const AggPlan& pl
 }
 inline bool progIsInt(const ExprEnv& env, Prog p) { return ws_prog_is_int((const ws_expr_env*)&env, *(const ws_prog*)&p) != 0; }
 inline void jitBeginQuery(const std::string& sql) { ws_jit_begin_query(sql.c_str()); }
-inline ws_jit_query_info jitEndQuery(double queryMs) {
+// src/jit.h:51-56
+struct JitQueryInfo {
+  int compiled = 0, hits = 0, fromDisk = 0, background = 0;
+  double compileMs = 0;
+  std::vector<int> ids;
+};
+inline JitQueryInfo jitEndQuery(double queryMs) {
   ws_jit_query_info i{};
   ws_jit_end_query(queryMs, &i);
-  return i;
+  JitQueryInfo r;
+  r.compiled = i.compiled, r.hits = i.hits, r.fromDisk = i.from_disk, r.background = i.background;
+  r.compileMs = i.compile_ms;
+  int n = 0;
+  if (ws_jit_last_query_plans(nullptr, 0, &n) == WS_ERR_SIZE) {
+    r.ids.resize((size_t)n);
+    ws_jit_last_query_plans(r.ids.data(), n, &n);
+  }
+  return r;
 }
+inline std::string wsJitPlanText(int id, int field) {
+  size_t need = 0;
+  if (ws_jit_plan_text(id, field, nullptr, 0, &need) != WS_OK || need == 0) return "";
+  std::string t(need, '\0');
+  ws_jit_plan_text(id, field, t.data(), need, &need);
+  t.resize(need - 1);
+  return t;
+}
+// src/jit.h:61-73
+struct PlanCacheRow {
+  int id;
+  std::string kind;
+  std::string origin;  // "compiled" or "disk"
+  double compileMs;
+  int64_t execs;
+  double avgMs, lastMs;
+  size_t sourceBytes;
+  std::string sql;
+};
+inline std::vector<PlanCacheRow> jitPlanCache() {
+  std::vector<PlanCacheRow> rows;
+  const int n = ws_jit_plan_cache_count();
+  for (int i = 0; i < n; ++i) {
+    ws_jit_info j{};
+    if (ws_jit_plan_cache_row(i, &j) != WS_OK) continue;
+    rows.push_back({j.id, wsJitPlanText(j.id, 0), j.from_disk ? "disk" : "compiled", j.compile_ms, j.execs,
+                    j.execs ? j.total_ms / (double)j.execs : 0.0, j.last_ms, (size_t)j.source_bytes,
+                    wsJitPlanText(j.id, 1)});
+  }
+  return rows;
+}
+inline std::string jitSourceOf(int id) { return wsJitPlanText(id, 2); }
 inline void jitClearCache() { ws_jit_clear_cache(); }
 
 // ---- aggregation (src/gpu.h:84-130)
@@ -307,6 +414,52 @@ inline void gpuEvalAtInt(const ExprEnv& env, Prog prog, const int32_t* idx, int6
   wsCheck(ws_eval_at_int((const ws_expr_env*)&env, WS_MAX_COLS, *(const ws_prog*)&prog, idx, m, out));
 }
 
+// ---- distinct values, bitmaps, temp-table columns (src/gpu.h:150-167)
+inline std::vector<int64_t> gpuDistinctInts(const ExprEnv& env, Prog prog, const int32_t* idx, int64_t m, int64_t base,
+                                            int64_t span) {
+  std::vector<int64_t> out((size_t)std::min<int64_t>(std::max<int64_t>(std::min(span, m), 0), 1 << 16));
+  int64_t n = 0;
+  int rc = ws_distinct_ints((const ws_expr_env*)&env, WS_MAX_COLS, *(const ws_prog*)&prog, idx, m, base, span, out.data(),
+                            (int64_t)out.size(), &n);
+  if (rc == WS_ERR_SIZE) {
+    out.resize((size_t)n);
+    rc = ws_distinct_ints((const ws_expr_env*)&env, WS_MAX_COLS, *(const ws_prog*)&prog, idx, m, base, span, out.data(),
+                          (int64_t)out.size(), &n);
+  }
+  wsCheck(rc);
+  out.resize((size_t)n);
+  return out;
+}
+inline uint32_t* gpuBitsFromColumn(const void* col, int out, int64_t n, int64_t base, int64_t nbits, bool* sawNull) {
+  uint32_t* bits = nullptr;
+  int nul = 0;
+  wsCheck(ws_bits_from_column(col, out, n, base, nbits, &bits, &nul));
+  if (sawNull) *sawNull = nul != 0;
+  return bits;
+}
+struct TempColSpec {  // the engine's, field for field (ws_temp_col_spec)
+  int8_t src = 0;
+  int idx = 0, hi = -1, cnt = -1;
+  uint8_t kind = 0;
+  uint8_t keyInt = 0, sumBits = 0;
+  uint8_t out = 2;
+  double div = 1;
+  double mul = 1;
+};
+static_assert(sizeof(TempColSpec) == sizeof(ws_temp_col_spec) && offsetof(TempColSpec, idx) == offsetof(ws_temp_col_spec, idx) &&
+                  offsetof(TempColSpec, cnt) == offsetof(ws_temp_col_spec, cnt) &&
+                  offsetof(TempColSpec, kind) == offsetof(ws_temp_col_spec, kind) &&
+                  offsetof(TempColSpec, out) == offsetof(ws_temp_col_spec, out) &&
+                  offsetof(TempColSpec, div) == offsetof(ws_temp_col_spec, div) &&
+                  offsetof(TempColSpec, mul) == offsetof(ws_temp_col_spec, mul),
+              "TempColSpec and ws_temp_col_spec differ");
+inline void* gpuTempColumn(const double* keys, int nk, const double* accs, int na, int64_t g, const TempColSpec& s, double& mn,
+                           double& mx) {
+  void* col = nullptr;
+  wsCheck(ws_temp_column(keys, nk, accs, na, g, (const ws_temp_col_spec*)&s, &col, &mn, &mx));
+  return col;
+}
+
 // ---- ORDER BY (src/gpu.h:197-199)
 inline DevVec<int32_t> gpuSortPerm(const std::vector<std::pair<const double*, bool>>& keys, int64_t m) {
   std::vector<const double*> k;
@@ -317,5 +470,11 @@ inline DevVec<int32_t> gpuSortPerm(const std::vector<std::pair<const double*, bo
   return DevVec<int32_t>(perm, m);
 }
 inline void gpuMapRank(double* keys, const int32_t* rank, int64_t m) { wsCheck(ws_map_rank(keys, rank, m)); }
+template <class PType>
+inline std::vector<int32_t> gpuSortPermHost(const void* hostCol, PType t, int64_t n) {
+  std::vector<int32_t> perm((size_t)std::max<int64_t>(n, 0));
+  if (n > 0) wsCheck(ws_sort_perm_host(hostCol, (int)t, n, perm.data()));
+  return perm;
+}
 
 }  // namespace gdb

@@ -37,6 +37,28 @@ SIGNATURES = {
     "ws_gpu_trim_pool": (C.c_int, []),
     "ws_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(P)]),
     "ws_host_free": (C.c_int, [P]),
+    "ws_set_vram_limit": (C.c_int, [C.c_int64]),
+    "ws_vram_used": (C.c_int64, []),
+    "ws_vram_limit": (C.c_int64, []),
+    "ws_vram_free": (C.c_int64, []),
+    "ws_vram_fill": (C.c_double, []),
+    "ws_place_column": (C.c_int, [P, C.c_size_t, C.c_int, C.POINTER(P), C.POINTER(C.c_int)]),
+    "ws_release_column": (C.c_int, [P, P, C.c_size_t, C.c_int]),
+    "ws_vram_acquire": (C.c_int, [P, C.c_size_t, C.POINTER(P)]),
+    "ws_vram_release": (C.c_int, [P, C.c_size_t]),
+    "ws_host_map": (C.c_int, [P, C.c_size_t, C.POINTER(P)]),
+    "ws_host_unmap": (C.c_int, [P]),
+    "ws_patch_column": (C.c_int, [P, C.c_size_t, C.c_int, P, P, C.c_int64, C.POINTER(P)]),
+    "ws_update_column": (C.c_int, [P, P, C.c_int64, C.c_int, C.c_int, P, C.c_int64, C.POINTER(abi.Update),
+                                   C.POINTER(P)]),
+    "ws_distinct_ints": (C.c_int, [C.POINTER(abi.ExprEnv), C.c_int, abi.Prog, P, C.c_int64, C.c_int64, C.c_int64, P,
+                                   C.c_int64, I64P]),
+    "ws_bits_from_column": (C.c_int, [P, C.c_int, C.c_int64, C.c_int64, C.c_int64, C.POINTER(P), C.POINTER(C.c_int)]),
+    "ws_temp_column": (C.c_int, [P, C.c_int, P, C.c_int, C.c_int64, C.POINTER(abi.TempColSpec), C.POINTER(P),
+                                 C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "ws_sort_perm_host": (C.c_int, [P, C.c_int, C.c_int64, P]),
+    "ws_jit_plan_text": (C.c_int, [C.c_int, C.c_int, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "ws_jit_last_query_plans": (C.c_int, [P, C.c_int, C.POINTER(C.c_int)]),
     "ws_agg_create": (C.c_int, [C.POINTER(abi.AggPlan), C.c_int64, C.POINTER(abi.DenseSpec), C.POINTER(P)]),
     "ws_agg_destroy": (None, [P]),
     "ws_agg_add_batch": (C.c_int, [P, C.POINTER(abi.ExprEnv), C.c_int, C.c_int64, P]),

@@ -109,6 +109,20 @@ class FetchStatus(C.Structure):
     _fields_ = [("groups", C.c_int64), ("overflow", C.c_int32), ("error", C.c_int32)]
 
 
+class Update(C.Structure):
+    """ws_update (include/ws_b200.h; the engine's GpuUpdate)."""
+    _fields_ = [("kind", C.c_int32), ("i0", C.c_int64), ("add", C.c_int64), ("nul", C.c_int64), ("lo", C.c_int64),
+                ("hi", C.c_int64), ("d0", C.c_double), ("add_d", C.c_double), ("not_null", C.c_uint8),
+                ("bad", C.c_uint8), ("saw_null", C.c_uint8), ("mn", C.c_double), ("mx", C.c_double)]
+
+
+class TempColSpec(C.Structure):
+    """ws_temp_col_spec (include/ws_b200.h; the engine's TempColSpec)."""
+    _fields_ = [("src", C.c_int8), ("idx", C.c_int32), ("hi", C.c_int32), ("cnt", C.c_int32), ("kind", C.c_uint8),
+                ("key_int", C.c_uint8), ("sum_bits", C.c_uint8), ("out", C.c_uint8), ("div", C.c_double),
+                ("mul", C.c_double)]
+
+
 class EstimatorWeights(C.Structure):
     """ws_estimator_weights (include/ws_b200.h)."""
     _fields_ = [("hidden", C.c_int), ("w1", C.c_void_p), ("b1", C.c_void_p), ("w2", C.c_void_p), ("b2", C.c_void_p),

@@ -34,6 +34,7 @@ std::string gDiskDir;
 thread_local std::string tSql;
 thread_local ws_jit_query_info tInfo;
 thread_local std::vector<ws_jit_program*> tUsed;
+thread_local std::vector<int> tLastIds;  // plans used by the calling thread's last ended query
 
 int jitMode() { return tMode >= 0 ? tMode : gDefaultMode.load(); }
 
@@ -731,6 +732,30 @@ int ws_jit_source_of(int id, char* buf, size_t size, size_t* needed) {
   return WS_ERR_ARG;
 }
 
+int ws_jit_plan_text(int id, int field, char* buf, size_t size, size_t* needed) {
+  if (field < 0 || field > 2) return WS_ERR_ARG;
+  std::lock_guard<std::mutex> g(gMu);
+  for (auto& p : gById)
+    if (p->id == id) {
+      const std::string& t = field == 0 ? p->kind : field == 1 ? p->sql : p->source;
+      if (needed) *needed = t.size() + 1;
+      if (buf && size) {
+        const size_t n = std::min(size - 1, t.size());
+        memcpy(buf, t.data(), n);
+        buf[n] = 0;
+      }
+      return WS_OK;
+    }
+  if (needed) *needed = 0;
+  return WS_ERR_ARG;
+}
+
+int ws_jit_last_query_plans(int* ids, int max_ids, int* n) {
+  *n = (int)tLastIds.size();
+  for (int i = 0; i < *n && i < max_ids; ++i) ids[i] = tLastIds[(size_t)i];
+  return *n > max_ids ? WS_ERR_SIZE : WS_OK;
+}
+
 int ws_jit_plan_cache_count(void) {
   std::lock_guard<std::mutex> g(gMu);
   return (int)gById.size();
@@ -765,6 +790,8 @@ int ws_jit_begin_query(const char* sql) {
 }
 int ws_jit_end_query(double query_ms, ws_jit_query_info* info) {
   std::lock_guard<std::mutex> g(gMu);
+  tLastIds.clear();
+  for (ws_jit_program* p : tUsed) tLastIds.push_back(p->id);
   for (ws_jit_program* p : tUsed) {
     ++p->execs;
     p->totalMs += query_ms;

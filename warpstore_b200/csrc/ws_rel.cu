@@ -2,6 +2,8 @@
 // dictionary code remaps, NULL-aware and encoded gathers, expression evaluation at row indices
 // (projection and post-aggregation keys), and the stable multi-key sort permutation of ORDER BY
 // (reference: src/gpu.cu:149-163, :802-888, :1011-1087, :1323-1367).
+#include <climits>
+#include <cmath>
 #include <cstring>
 
 #include "ws_internal.h"
@@ -256,6 +258,143 @@ __global__ void kMapRank(double* keys, const int32_t* rank, int64_t m) {
   WS_GRID_STRIDE(j, m) keys[j] = keys[j] != keys[j] ? -1.0 : (double)__ldg(rank + (int64_t)keys[j]);
 }
 
+// ---------------------------------------------------------------- distinct values, bitmaps, temp columns
+// bit (v - base) of every non-NULL value v in [base, base + span) of an exact int64 array
+__global__ void kDistinctBits(const i64* v, int64_t m, i64 base, i64 span, uint32_t* bits) {
+  WS_GRID_STRIDE(j, m) {
+    const i64 x = v[j];
+    if (x == (i64)WS_NULL_I64) continue;
+    const u64 k = (u64)x - (u64)base;
+    if ((i64)k < 0 || (i64)k >= span || x < base) continue;
+    const uint32_t bit = 1u << (k & 31);
+    if (!(__ldg(bits + (k >> 5)) & bit)) atomicOr(bits + (k >> 5), bit);
+  }
+}
+// bit (v - base) of the non-NULL values of an INT (out 0) / BIGINT (out 1) column; *nul: any NULL
+__global__ void kBitsFromColumn(const void* col, int out, int64_t n, i64 base, i64 nbits, uint32_t* bits, int* nul) {
+  int sawNull = 0;
+  WS_GRID_STRIDE(i, n) {
+    i64 v;
+    if (out == 1) {
+      v = ((const i64*)col)[i];
+      if (v == (i64)WS_NULL_I64) {
+        sawNull = 1;
+        continue;
+      }
+    } else {
+      const int x = ((const int*)col)[i];
+      if (x == WS_NULL_I32) {
+        sawNull = 1;
+        continue;
+      }
+      v = x;
+    }
+    const i64 k = v - base;
+    if (k >= 0 && k < nbits) atomicOr(bits + (k >> 5), 1u << (k & 31));
+  }
+  if (__any_sync(0xffffffffu, sawNull) && (threadIdx.x & 31) == 0) atomicOr(nul, 1);
+}
+// One temp-table column from compacted groups (column-major keys / accs); min / max of an integer
+// output over the non-NULL groups (mnmx[0] / [1]).
+__global__ void kTempColumn(const double* keys, const double* accs, int64_t g, const __grid_constant__ ws_temp_col_spec s,
+                            void* out, long long* mnmx) {
+  long long mn = LLONG_MAX, mx = LLONG_MIN;
+  WS_GRID_STRIDE(r, g) {
+    auto A = [&](int j) { return accs[(int64_t)j * g + r]; };
+    auto bits = [](double d) { return (i64)__double_as_longlong(d); };
+    bool nul = s.src == 1 && s.cnt >= 0 && A(s.cnt) == 0;
+    bool isInt = false;
+    i64 iv = 0;
+    double dv = 0;
+    if (s.src == 0) {
+      const double k = keys[(int64_t)s.idx * g + r];
+      if (s.key_int) {
+        iv = bits(k);
+        isInt = true;
+        nul = iv == (i64)WS_NULL_I64 || iv == (i64)WS_NULL_I32;
+      } else {
+        dv = k;
+        nul = k != k;
+      }
+    } else if (!nul) {
+      switch (s.kind) {
+        case 1: iv = bits(A(s.idx)); isInt = true; break;
+        case 2: iv = (i64)((u64)bits(A(s.hi)) * 4294967296ull + (u64)bits(A(s.idx))); isInt = true; break;
+        case 3: iv = (i64)A(s.idx); isInt = true; break;
+        case 4: {
+          const double sum = s.sum_bits ? (s.hi >= 0 ? (double)bits(A(s.hi)) * 4294967296.0 + (double)bits(A(s.idx))
+                                                     : (double)bits(A(s.idx)))
+                                        : A(s.idx);
+          dv = sum / s.div / A(s.cnt);
+          break;
+        }
+        default:
+          dv = A(s.idx) / s.div;
+          nul = dv != dv;
+      }
+    }
+    if (s.mul != 1 && !nul) {
+      dv = (isInt ? (double)iv : dv) * s.mul;
+      isInt = false;
+    }
+    if (s.out == 2) {
+      ((double*)out)[r] = nul ? __longlong_as_double(0x7ff8000000000000ll) : isInt ? (double)iv : dv;
+      continue;
+    }
+    const long long v = nul ? 0 : isInt ? iv : llround(dv);
+    if (!nul) mn = v < mn ? v : mn, mx = v > mx ? v : mx;
+    if (s.out == 1) ((i64*)out)[r] = nul ? (i64)WS_NULL_I64 : v;
+    else ((int32_t*)out)[r] = nul ? WS_NULL_I32 : (int32_t)v;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const long long a = __shfl_xor_sync(0xffffffffu, mn, o), b = __shfl_xor_sync(0xffffffffu, mx, o);
+    mn = a < mn ? a : mn;
+    mx = b > mx ? b : mx;
+  }
+  if ((threadIdx.x & 31) == 0 && mn <= mx) {
+    atomicMin(&mnmx[0], mn);
+    atomicMax(&mnmx[1], mx);
+  }
+}
+// host column of ptype -> double sort keys
+__global__ void kToDouble(const void* src, int ptype, int64_t n, double* out) {
+  WS_GRID_STRIDE(i, n) {
+    out[i] = ptype == WS_PT_I32 ? (double)((const int*)src)[i]
+             : ptype == WS_PT_I64 ? (double)((const i64*)src)[i] : ((const double*)src)[i];
+  }
+}
+
+// The engine evaluates gpuDistinctInts' program exactly only when it is built of integer columns,
+// integer literals, + - * and negation within a 16-deep stack (src/gpu.cu:826-865); any other program
+// yields no values.
+bool exactIntProgram(const ws_expr_env& env, ws_prog p) {
+  int sp = 0;
+  for (int i = 0; i < p.len; ++i) {
+    const ws_instr in = env.code[p.start + i];
+    switch (in.op) {
+      case WS_OP_COL: {
+        const int t = env.cols[in.arg].t;
+        if (t == 2 || t == 5 || t == 6 || sp >= 16) return false;
+        ++sp;
+        break;
+      }
+      case WS_OP_CONST:
+        if (!in.isInt || sp >= 16) return false;
+        ++sp;
+        break;
+      case WS_OP_ADD: case WS_OP_SUB: case WS_OP_MUL:
+        if (sp < 2) return false;
+        --sp;
+        break;
+      case WS_OP_NEG:
+        if (sp < 1) return false;
+        break;
+      default: return false;
+    }
+  }
+  return sp == 1;
+}
+
 double kNullF64() {  // the engine's NULL double: the canonical quiet NaN
   const uint64_t b = 0x7ff8000000000000ull;
   double d;
@@ -423,6 +562,116 @@ int ws_sort_perm(const double* const* keys, const int* desc, int nkeys, int64_t 
       }
     }
     *out_perm = perm.release();
+  });
+}
+
+int ws_distinct_ints(const ws_expr_env* env, int ncols, ws_prog prog, const int32_t* idx, int64_t m, int64_t base,
+                     int64_t span, int64_t* out, int64_t max_out, int64_t* count) {
+  return guardedCall([&] {
+    *count = 0;
+    if (m <= 0 || span <= 0) return;
+    if (prog.start < 0 || prog.len <= 0 || prog.start + prog.len > WS_MAX_CODE)
+      throw Error("ws_distinct_ints: program outside the code array", WS_ERR_ARG);
+    if (!exactIntProgram(*env, prog)) return;
+    if (span > ((int64_t)1 << 40)) throw Error("ws_distinct_ints: span too large for a bitmap", WS_ERR_ARG);
+    DBuf<uint8_t> pb, cb;
+    const EvalSpec s = evalSpec(*env, ncols, prog, pb);
+    const ws_col_view* cv = uploadCols(*env, ncols, cb);
+    DBuf<i64> vals(m);
+    WS_LAUNCH(kEvalAtInt, gridFor(m), 256, 0, s, cv, envK(*env), idx, m, (int64_t*)vals.p);
+    const int64_t words = (span + 31) / 32;
+    DBuf<uint32_t> bits(words);
+    WS_CK(cudaMemsetAsync(bits.p, 0, (size_t)words * 4, stream()));
+    WS_LAUNCH(kDistinctBits, gridFor(m), 256, 0, vals.p, m, base, span, bits.p);
+    std::vector<uint32_t> h((size_t)words);
+    d2hLarge(h.data(), bits.p, (size_t)words * 4);
+    int64_t c = 0;
+    for (int64_t w = 0; w < words; ++w)
+      for (uint32_t b = h[(size_t)w]; b; b &= b - 1) {
+        if (c < max_out && out) out[c] = base + w * 32 + __builtin_ctz(b);
+        ++c;
+      }
+    *count = c;
+    if (c > max_out) throw Error("ws_distinct_ints: more distinct values than out holds", WS_ERR_SIZE);
+  });
+}
+
+int ws_bits_from_column(const void* col, int out, int64_t n, int64_t base, int64_t nbits, uint32_t** bits,
+                        int* saw_null) {
+  return guardedCall([&] {
+    ensureInit();
+    *bits = nullptr;
+    *saw_null = 0;
+    if (nbits < 0 || n < 0 || (out != 0 && out != 1)) throw Error("ws_bits_from_column: bad arguments", WS_ERR_ARG);
+    const size_t bytes = std::max<size_t>(4, (size_t)((nbits + 31) / 32) * 4);
+    uint32_t* b = nullptr;
+    WS_CK(cudaMalloc(&b, bytes));
+    try {
+      WS_CK(cudaMemsetAsync(b, 0, bytes, stream()));
+      DBuf<int> nul(1);
+      WS_CK(cudaMemsetAsync(nul.p, 0, 4, stream()));
+      if (n > 0) WS_LAUNCH(kBitsFromColumn, gridFor(n), 256, 0, col, out, n, base, nbits, b, nul.p);
+      int h = 0;
+      d2hSync(&h, nul.p, 4);
+      *saw_null = h != 0;
+    } catch (...) {
+      cudaStreamSynchronize(stream());
+      cudaFree(b);
+      throw;
+    }
+    *bits = b;
+  });
+}
+
+int ws_temp_column(const double* keys, int nk, const double* accs, int na, int64_t g, const ws_temp_col_spec* s,
+                   void** col, double* mn, double* mx) {
+  return guardedCall([&] {
+    ensureInit();
+    *col = nullptr;
+    if (g < 0 || s->out > 2 || (s->src == 0 && (s->idx < 0 || s->idx >= nk)) ||
+        (s->src == 1 && (s->idx < 0 || s->idx >= na || s->hi >= na || s->cnt >= na)))
+      throw Error("ws_temp_column: spec outside the groups' keys / slots", WS_ERR_ARG);
+    const size_t w = s->out == 0 ? 4 : 8;
+    void* o = nullptr;
+    WS_CK(cudaMalloc(&o, std::max<size_t>(1, (size_t)g * w)));
+    long long h[2] = {LLONG_MAX, LLONG_MIN};
+    try {
+      DBuf<long long> mm(2);
+      uint8_t* st = pinnedStage(sizeof h);
+      memcpy(st, h, sizeof h);
+      h2dAsync(mm.p, st, sizeof h);
+      stageCopied();
+      if (g > 0) WS_LAUNCH(kTempColumn, gridFor(g), 256, 0, keys, accs, g, *s, o, mm.p);
+      d2hSync(h, mm.p, sizeof h);
+    } catch (...) {
+      cudaStreamSynchronize(stream());
+      cudaFree(o);
+      throw;
+    }
+    *mn = s->out == 2 || h[0] > h[1] ? -INFINITY : (double)h[0];
+    *mx = s->out == 2 || h[0] > h[1] ? INFINITY : (double)h[1];
+    *col = o;
+  });
+}
+
+int ws_sort_perm_host(const void* host_col, int ptype, int64_t n, int32_t* perm) {
+  return guardedCall([&] {
+    if (n <= 0) return;
+    if (ptype != WS_PT_I32 && ptype != WS_PT_I64 && ptype != WS_PT_F64)
+      throw Error("ws_sort_perm_host: ptype must be I32, I64 or F64", WS_ERR_ARG);
+    const size_t esz = ptype == WS_PT_I32 ? 4 : 8;
+    DBuf<uint8_t> raw((int64_t)(n * esz));
+    WS_CK(cudaMemcpyAsync(raw.p, host_col, (size_t)n * esz, cudaMemcpyHostToDevice, stream()));
+    DBuf<double> k(n);
+    WS_LAUNCH(kToDouble, gridFor(n), 256, 0, raw.p, ptype, n, k.p);
+    const double* keys[1] = {k.p};
+    const int desc[1] = {0};
+    int32_t* p = nullptr;
+    const int rc = ws_sort_perm(keys, desc, 1, n, &p);
+    if (rc != WS_OK) throw Error(ws_last_error(), rc);
+    DBuf<int32_t> pp;
+    pp.p = p, pp.n = n;
+    d2hLarge(perm, p, (size_t)n * 4);
   });
 }
 

@@ -456,8 +456,96 @@ def map_rank(keys_ptr: int, rank_ptr: int, m: int):
     check(lib().ws_map_rank(keys_ptr, rank_ptr, m))
 
 
+# ---------------------------------------------------------------- tiered storage, UPDATE, distinct, temp columns
+def set_vram_limit(nbytes: int):
+    check(lib().ws_set_vram_limit(int(nbytes)))
+
+
+def vram_used() -> int:
+    return lib().ws_vram_used()
+
+
+def place_column(host: np.ndarray, host_only: bool = False):
+    """(device pointer, mapped) of a host column placed like the engine's placeColumn."""
+    out, mapped = P(), C.c_int()
+    check(lib().ws_place_column(host.ctypes.data, host.nbytes, int(host_only), C.byref(out), C.byref(mapped)))
+    return out.value, bool(mapped.value)
+
+
+def release_column(dev: int, host: np.ndarray, mapped: bool):
+    check(lib().ws_release_column(dev, host.ctypes.data, host.nbytes, int(mapped)))
+
+
+def vram_acquire(host: np.ndarray) -> int | None:
+    out = P()
+    check(lib().ws_vram_acquire(host.ctypes.data, host.nbytes, C.byref(out)))
+    return out.value
+
+
+def vram_release(dev: int, nbytes: int):
+    check(lib().ws_vram_release(dev, nbytes))
+
+
+def host_map(host: np.ndarray) -> int | None:
+    out = P()
+    check(lib().ws_host_map(host.ctypes.data, host.nbytes, C.byref(out)))
+    return out.value
+
+
+def host_unmap(host: np.ndarray):
+    check(lib().ws_host_unmap(host.ctypes.data))
+
+
+def patch_column(old_ptr: int, nbytes: int, width: int, rows: np.ndarray, vals: np.ndarray) -> int | None:
+    rows = np.ascontiguousarray(rows, dtype=np.int32)
+    vals = np.ascontiguousarray(vals)
+    out = P()
+    check(lib().ws_patch_column(old_ptr, nbytes, width, rows.ctypes.data, vals.ctypes.data, rows.size, C.byref(out)))
+    return out.value
+
+
+def update_column(old_ptr: int, src_ptr: int, n: int, w: int, f64: bool, rows: np.ndarray, u: abi.Update) -> int | None:
+    rows = np.ascontiguousarray(rows, dtype=np.int32)
+    out = P()
+    check(lib().ws_update_column(old_ptr, src_ptr, n, w, int(f64), rows.ctypes.data, rows.size, C.byref(u), C.byref(out)))
+    return out.value
+
+
+def distinct_ints(env: abi.ExprEnv, ncols: int, prog: abi.Prog, idx_ptr: int | None, m: int, base: int,
+                  span: int) -> np.ndarray:
+    cap = max(1, min(span, m))
+    out = np.empty(cap, dtype=np.int64)
+    n = C.c_int64()
+    check(lib().ws_distinct_ints(C.byref(env), ncols, prog, idx_ptr, m, base, span, out.ctypes.data, cap, C.byref(n)))
+    return out[:n.value]
+
+
+def bits_from_column(col_ptr: int, out: int, n: int, base: int, nbits: int):
+    """(device pointer of the bitmap (ws_dev_free), saw_null)."""
+    bits, nul = P(), C.c_int()
+    check(lib().ws_bits_from_column(col_ptr, out, n, base, nbits, C.byref(bits), C.byref(nul)))
+    return bits.value, bool(nul.value)
+
+
+def temp_column(keys_ptr: int, nk: int, accs_ptr: int, na: int, g: int, spec: abi.TempColSpec):
+    """(device pointer of the column (ws_dev_free), mn, mx)."""
+    col, mn, mx = P(), C.c_double(), C.c_double()
+    check(lib().ws_temp_column(keys_ptr, nk, accs_ptr, na, g, C.byref(spec), C.byref(col), C.byref(mn), C.byref(mx)))
+    return col.value, mn.value, mx.value
+
+
+def sort_perm_host(col: np.ndarray, ptype: int) -> np.ndarray:
+    col = np.ascontiguousarray(col)
+    perm = np.empty(max(col.size, 1), dtype=np.int32)
+    check(lib().ws_sort_perm_host(col.ctypes.data, ptype, col.size, perm.ctypes.data))
+    return perm[:col.size]
+
+
 __all__ = ["DeviceBuffer", "Executor", "GpuAggregator", "WsError", "agg_nokeys_noalloc", "bits_to_double", "codegen_compile_check",
            "codegen_source", "cross_join", "device_to_array", "encode_column", "eval_at", "eval_at_int", "gather", "gather_bytes",
            "gather_enc", "gather_multi", "gather_null", "gpu_init", "hash_join", "hash_join_outer", "hash_join_parts",
            "jit_get", "jit_info", "jit_set_cache_dir", "jit_set_default_mode", "jit_set_mode", "kernel_launches",
-           "key_bitmap", "map_rank", "remap_codes", "select_multi", "set_bits", "sort_perm", "sync", "tmp_free"]
+           "key_bitmap", "map_rank", "remap_codes", "select_multi", "set_bits", "sort_perm", "sync", "tmp_free",
+           "set_vram_limit", "vram_used", "place_column", "release_column", "vram_acquire", "vram_release", "host_map",
+           "host_unmap", "patch_column", "update_column", "distinct_ints", "bits_from_column", "temp_column",
+           "sort_perm_host"]
