@@ -1,5 +1,6 @@
-"""ctypes wrapper of oracle/_ref/libwsref.so: the reference's own GPU operators (interpreted kernels of
-Warpstore src/gpu.cu built for sm_100a) — TEST INFRASTRUCTURE ONLY, called by tests/."""
+"""ctypes wrapper of oracle/_ref/libwsref.so: the reference's own GPU operators (Warpstore src/gpu.cu and
+src/jit.cu built for sm_100a; by default each aggregation / selection runs the reference's compiled plan,
+set_compiled(False) its interpreted kernels) — TEST INFRASTRUCTURE ONLY, called by tests/."""
 from __future__ import annotations
 
 import ctypes as C
@@ -41,10 +42,21 @@ def lib() -> C.CDLL:
         l.wsref_free.argtypes = [P]
         l.wsref_select_multi_dev.argtypes = [C.POINTER(abi.ExprEnv), C.c_int, abi.Prog, C.c_int, P, P, P, C.c_int,
                                              C.POINTER(C.c_int64), C.POINTER(P), C.POINTER(C.c_float)]
+        l.wsref_set_compiled.argtypes = [C.c_int]
         if l.wsref_init():
             raise RuntimeError(l.wsref_error().decode())
         _lib = l
     return _lib
+
+
+def set_compiled(on: bool):
+    """Compiled plans (the engine's production path, default) or the interpreted kernels."""
+    lib().wsref_set_compiled(1 if on else 0)
+
+
+def last_compiled() -> bool:
+    """The calling thread's last aggregation / selection ran a compiled plan."""
+    return bool(lib().wsref_last_compiled())
 
 
 def _check(rc):

@@ -1,10 +1,13 @@
-// Harness around the reference's own GPU operators (Warpstore src/gpu.cu, built for sm_100a from its
-// sources by oracle/build_ref.py) — TEST INFRASTRUCTURE ONLY: a second parity checker that runs the
-// reference on the same inputs, and its timing for comparison.  Only tests/ call it.
+// Harness around the reference's own GPU operators (Warpstore src/gpu.cu and src/jit.cu, built for
+// sm_100a from their sources by oracle/build_ref.py) — TEST INFRASTRUCTURE ONLY: a second parity
+// checker that runs the reference on the same inputs, and its timing for comparison.  Only tests/
+// call it.
 //
-// The reference's runtime-compiled plans (src/jit.cu) need a build-generated header and are not built;
-// its operators run their ahead-of-time kernels with the bytecode interpreter (jit = nullptr), the
-// engine's path with codegen OFF.  jitLaunch is therefore never reached (stub below).
+// By default the operators run the engine's production path: each aggregation and selection first
+// gets its compiled plan (jitGet in JIT_SYNC mode: NVRTC compiles before the first run, outside the
+// timed region) and hands it to the operator, as src/engine_select.cpp:1379-1392 and
+// src/engine_core.h:4372-4378 do.  wsref_set_compiled(0) selects the interpreted kernels instead (the
+// engine with codegen OFF).
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -13,15 +16,11 @@
 #include "gpu.h"
 #include "jit.h"
 
-namespace gdb {
-void jitLaunch(const JitProgram*, JitFn, unsigned, unsigned, size_t, void**) {
-  throw SqlError("reference harness: compiled plans are not built", 1105);
-}
-}  // namespace gdb
-
 using namespace gdb;
 
 static thread_local char gErr[512];
+static bool gCompiled = true;                // run compiled plans (the engine's production path)
+static thread_local int gLastCompiled = 0;  // the last aggregation / selection ran a compiled plan
 
 template <class F>
 static int guard(F&& f) {
@@ -34,11 +33,37 @@ static int guard(F&& f) {
   }
 }
 
+// The compiled plan the engine would run for an aggregation or a filter (nullptr: interpreted).
+static const JitProgram* aggPlanFor(const ExprEnv& env, int ncols, const AggPlan& plan, const DenseSpec* dense) {
+  if (!gCompiled) return nullptr;
+  jitSetMode(JIT_SYNC);
+  const JitFn fn = !plan.nkeys ? JF_NOKEYS : (dense && dense->G) ? JF_DENSE : JF_GROUPED;
+  return jitGet(env, ncols, plan, fn, "harness aggregate");
+}
+static const JitProgram* filterPlanFor(const ExprEnv& env, int ncols, bool hasWhere, Prog where) {
+  if (!gCompiled || !hasWhere) return nullptr;
+  jitSetMode(JIT_SYNC);
+  AggPlan fp;
+  fp.hasWhere = true;
+  fp.where = where;
+  return jitGet(env, ncols, fp, JF_FLAGM, "harness filter");
+}
+
 extern "C" {
 
 const char* wsref_error() { return gErr; }
 
-int wsref_init() { return guard([] { gpuInit(); }); }
+int wsref_init() {
+  return guard([] {
+    gpuInit();
+    jitSetDefaultMode(JIT_SYNC);
+  });
+}
+int wsref_set_compiled(int on) {
+  gCompiled = on != 0;
+  return 0;
+}
+int wsref_last_compiled() { return gLastCompiled; }
 
 // Result of the last wsref_aggregate on this thread, copied out by wsref_take.
 static thread_local std::vector<double> gKeys, gAccs;
@@ -54,6 +79,10 @@ int wsref_aggregate(const ExprEnv* envIn, int ncols, const AggPlan* plan, const 
     std::vector<uint8_t> envBuf(sizeof(ExprEnv));
     ExprEnv* env = (ExprEnv*)envBuf.data();
     memcpy(env, envIn, sizeof(ExprEnv));
+    if (nb > 0)
+      for (int c = 0; c < ncols; ++c) env->cols[c] = bcols[c];
+    const JitProgram* jit = aggPlanFor(*env, ncols, *plan, dense);
+    gLastCompiled = jit != nullptr;
     GpuAggregator agg(*plan, cap, dense);
     for (int b = 0; b < nb; ++b) {
       for (int c = 0; c < ncols; ++c) env->cols[c] = bcols[(int64_t)b * ncols + c];
@@ -63,7 +92,7 @@ int wsref_aggregate(const ExprEnv* envIn, int ncols, const AggPlan* plan, const 
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, cudaStreamPerThread);
-    agg.run(*env, nullptr);
+    agg.run(*env, jit);
     cudaEventRecord(e1, cudaStreamPerThread);
     *overflow = agg.overflowed() ? 1 : 0;
     cudaEventSynchronize(e1);
@@ -92,6 +121,10 @@ int wsref_aggregate_compact(const ExprEnv* envIn, int ncols, const AggPlan* plan
     std::vector<uint8_t> envBuf(sizeof(ExprEnv));
     ExprEnv* env = (ExprEnv*)envBuf.data();
     memcpy(env, envIn, sizeof(ExprEnv));
+    if (nb > 0)
+      for (int c = 0; c < ncols; ++c) env->cols[c] = bcols[c];
+    const JitProgram* jit = aggPlanFor(*env, ncols, *plan, dense);
+    gLastCompiled = jit != nullptr;
     GpuAggregator agg(*plan, cap, dense);
     for (int b = 0; b < nb; ++b) {
       for (int c = 0; c < ncols; ++c) env->cols[c] = bcols[(int64_t)b * ncols + c];
@@ -101,7 +134,7 @@ int wsref_aggregate_compact(const ExprEnv* envIn, int ncols, const AggPlan* plan
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, cudaStreamPerThread);
-    agg.run(*env, nullptr);
+    agg.run(*env, jit);
     cudaEventRecord(e1, cudaStreamPerThread);
     *overflow = agg.overflowed() ? 1 : 0;
     cudaEventSynchronize(e1);
@@ -165,7 +198,9 @@ int wsref_select_multi(const ExprEnv* envIn, int hasWhere, Prog where, int nb, c
     std::vector<ColView> cols(bcols, bcols + (size_t)nb * ncols);
     DevVec<int32_t> out;
     std::vector<int64_t> per;
-    *m = gpuSelectMulti(*envIn, hasWhere != 0, where, n, d, cols, ncols, out, per, nullptr);
+    const JitProgram* jit = filterPlanFor(*envIn, ncols, hasWhere != 0, where);
+    gLastCompiled = jit != nullptr;
+    *m = gpuSelectMulti(*envIn, hasWhere != 0, where, n, d, cols, ncols, out, per, jit);
     for (int b = 0; b < nb; ++b) perBatch[b] = per[b];
     if (*m <= maxm && *m > 0) d2h(idx, out.p, 4 * *m);
   });
@@ -225,11 +260,13 @@ int wsref_select_multi_dev(const ExprEnv* envIn, int hasWhere, Prog where, int n
     std::vector<ColView> cols(bcols, bcols + (size_t)nb * ncols);
     DevVec<int32_t> out;
     std::vector<int64_t> per;
+    const JitProgram* jit = filterPlanFor(*envIn, ncols, hasWhere != 0, where);
+    gLastCompiled = jit != nullptr;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, cudaStreamPerThread);
-    *m = gpuSelectMulti(*envIn, hasWhere != 0, where, n, d, cols, ncols, out, per, nullptr);
+    *m = gpuSelectMulti(*envIn, hasWhere != 0, where, n, d, cols, ncols, out, per, jit);
     cudaEventRecord(e1, cudaStreamPerThread);
     cudaEventSynchronize(e1);
     cudaEventElapsedTime(ms, e0, e1);

@@ -121,6 +121,36 @@ def test_sums_beyond_int64_are_exact():
     assert ds is not None
 
 
+@pytest.mark.parametrize("where_big", ["first", "middle", "last"])
+def test_bounded_sums_switch_to_tested_additions(where_big):
+    """Integer sums are added without overflow tests while the arguments stay below the launch's bound,
+    and a thread that meets a larger argument tests every later addition: a few huge values (sums past
+    int64) among small ones, at the start, middle or end of the scan, in no-key, dense and hash plans;
+    products whose operands exceed 32 bits take the tested multiplication (overflow flag included)."""
+    n = 1_500_000
+    rng = np.random.default_rng(17)
+    v = rng.integers(-1000, 1000, n, dtype=np.int64)
+    pos = {"first": 0, "middle": n // 2, "last": n - 700}[where_big]
+    v[pos:pos + 600] = rng.integers(2**61, 2**62, 600, dtype=np.int64) * rng.choice([-1, 1], 600)
+    u = rng.integers(-1000, 1000, n, dtype=np.int64)
+    w = rng.integers(1, 50, n, dtype=np.int64)
+    w[pos + 100:pos + 110] = 3_000_000_000  # beyond int32: those rows take the tested products
+    t = W.Table(n, seg_rows=1 << 18)
+    t.add("k", abi.T_I32, rng.integers(0, 5, n, dtype=np.int32))
+    t.add("v", abi.T_I64, v)
+    t.add("u", abi.T_I64, u)
+    t.add("w", abi.T_I64, w)
+    for keys in ([], [(q.col(0), True)]):
+        e = W.env_for(t)
+        aq = q.AggQuery(e, None, keys, [q.Agg("SUM", q.col(1), "BIGINT", True),
+                                        q.Agg("SUM", q.col(2) * q.col(3) - q.ilit(7), "BIGINT", False),
+                                        q.Agg("SUM", q.col(1) + q.col(2) * q.ilit(3), "BIGINT", False),
+                                        q.Agg("COUNT")])
+        check(t, e, aq)
+        if keys:
+            check(t, e, aq, dense=q.dense_spec(aq.plan, [(0, 4)], n))
+
+
 def test_encoded_columns_nulls_and_deletes():
     n = 700_000
     rng = np.random.default_rng(11)

@@ -1,5 +1,6 @@
-"""Parity with the reference itself: the reference's own GPU operators (Warpstore src/gpu.cu built for
-sm_100a into oracle/_ref, interpreted kernels) run on the same device inputs as ours.
+"""Parity with the reference itself: the reference's own GPU operators (Warpstore src/gpu.cu and src/jit.cu
+built for sm_100a into oracle/_ref) run on the same device inputs as ours — its compiled plans (the
+engine's production path), and for the aggregations and known answers its interpreted kernels too.
 
 Compared in the engine's result format (the reference's fetch): keys, COUNT, integer MIN / MAX and
 split BIGINT sums (recombined as the engine does) bit-exact; DOUBLE sums within 1e-12 relative.
@@ -74,28 +75,45 @@ def compare_engine_format(aq, keys_a, accs_a, keys_b, accs_b, hi_b=None):
             np.testing.assert_allclose(aa[:, s], ab[:, s], rtol=1e-12, err_msg=f"{a.fn} slot {s}")
 
 
+def ref_aggregate(e, aq, batches, dense, cap, compiled):
+    """The reference's aggregation, compiled plan or interpreted; the second run is timed (plan
+    compiled, pool warm).  (keys, accs, milliseconds of run() + overflowed())."""
+    ref.set_compiled(compiled)
+    try:
+        for _ in range(2):
+            rk, ra, _, ovf, rms = ref.aggregate(e.env, e.ncols, aq.plan, batches, dense, cap)
+            assert not ovf
+            assert ref.last_compiled() == compiled, "the reference did not run the plan kind asked for"
+    finally:
+        ref.set_compiled(True)
+    return rk, ra, rms
+
+
 def test_filter_groupby_vs_reference():
     t = W.filter_groupby_1m(1 << 20, seed=0)
     e, aq = W.filter_groupby_1m_query(t)
     t.to_device()
-    rk, ra, _, ovf, rms = ref.aggregate(e.env, e.ncols, aq.plan, t.batches(True), None, 1024)
-    assert not ovf
+    rk, ra, rms = ref_aggregate(e, aq, t.batches(True), None, 1024, True)
+    ik, ia, ims = ref_aggregate(e, aq, t.batches(True), None, 1024, False)
     ok_, oa, oms = ours(t, e, aq, None, 1024, abi.JF_GROUPED)
     compare_engine_format(aq, ok_, oa, rk, ra)
-    print(f"\n[timing] filter_groupby_1m hash: reference {rms:.3f} ms, ours {oms:.3f} ms")
+    compare_engine_format(aq, ok_, oa, ik, ia)
+    print(f"\n[timing] filter_groupby_1m hash: reference compiled {rms:.3f} ms (interpreted {ims:.3f} ms), "
+          f"ours {oms:.3f} ms")
 
 
 def test_pricing_summary_vs_reference():
     t = W.pricing_summary(8 * W.SEG_ROWS, seed=2)
     e, aq, ds = W.pricing_summary_query(t)
     t.to_device()
-    rk, ra, _, ovf, rms = ref.aggregate(e.env, e.ncols, aq.plan, t.batches(True), ds, 1024)
-    assert not ovf
+    rk, ra, rms = ref_aggregate(e, aq, t.batches(True), ds, 1024, True)
+    ik, ia, ims = ref_aggregate(e, aq, t.batches(True), ds, 1024, False)
     ok_, oa, oms = ours(t, e, aq, ds, 1024, abi.JF_DENSE)
     compare_engine_format(aq, ok_, oa, rk, ra)
+    compare_engine_format(aq, ok_, oa, ik, ia)
     rows = t.n
-    print(f"\n[timing] pricing_summary {rows} rows dense: reference {rms:.3f} ms ({rows / rms / 1e6:.1f} G rows/s), "
-          f"ours {oms:.3f} ms ({rows / oms / 1e6:.1f} G rows/s)")
+    print(f"\n[timing] pricing_summary {rows} rows dense: reference compiled {rms:.3f} ms "
+          f"({rows / rms / 1e6:.1f} G rows/s; interpreted {ims:.3f} ms), ours {oms:.3f} ms ({rows / oms / 1e6:.1f} G rows/s)")
 
 
 def test_join_vs_reference():
@@ -167,15 +185,18 @@ def test_select_vs_reference():
     where = e.compile(q.and_(q.col(0).lt(1203), q.col(3).ge(5)))
     t.to_device()
     ri, rp = ref.select_multi(e.env, where, t.batches(True), e.ncols)
+    assert ref.last_compiled()
     ptr, m, per = ops.select_multi(e.env, where, t.batches(True), e.ncols)
     gi = ops.device_to_array(ptr, np.int32, m)
     ops.tmp_free(ptr)
     assert np.array_equal(gi, ri) and list(per) == list(rp)
 
 
+@pytest.mark.parametrize("compiled", [True, False], ids=["compiled", "interpreted"])
 @pytest.mark.parametrize("case", KA.load()["cases"], ids=lambda c: c["name"])
-def test_known_answers_on_reference(case):
-    """The harness itself reproduces the reference's known answers (tests/smoke.py) on the GPU."""
+def test_known_answers_on_reference(case, compiled):
+    """The harness itself reproduces the reference's known answers (tests/smoke.py) on the GPU, with its
+    compiled plans and with its interpreter."""
     g = KA.load()
     st = g["states"][str(case["state"])]
     t = KA.table_of(st)
@@ -184,7 +205,12 @@ def test_known_answers_on_reference(case):
     e, aq, post = KA.plan_of(case, t, bset.ptr)
     bits = KA.deleted_bits(st)
     dbits = ops.DeviceBuffer.from_array(bits) if bits is not None else None
-    rk, ra, hi, ovf, _ = ref.aggregate(e.env, e.ncols, aq.plan, [(t.n, dbits.ptr if dbits else 0, t.views(0, True))])
+    ref.set_compiled(compiled)
+    try:
+        rk, ra, hi, ovf, _ = ref.aggregate(e.env, e.ncols, aq.plan, [(t.n, dbits.ptr if dbits else 0, t.views(0, True))])
+        assert ref.last_compiled() == compiled
+    finally:
+        ref.set_compiled(True)
     assert not ovf
     agg_rows = []
     rkb = rk.view(np.int64) if rk.size else np.zeros((ra.shape[0], 0), np.int64)

@@ -377,9 +377,31 @@ std::string genEvaluator(const ws_expr_env& env, int ncols, const ws_agg_plan& p
   o << "  }\n";
   // per-row common subexpressions (rows that did not pass the filter compute unused values and
   // raise no overflow flag)
+  // Integer products among the temporaries are first computed as 32 x 32-bit products (exact when every
+  // operand fits in int32, no branch); a row with a wider operand recomputes them with tested products.
   o << "  __device__ __forceinline__ void prep(int i, bool live) {\n";
   if (!g.temps.empty()) o << "    unsigned ofl = 0;\n";
-  for (size_t j = 0; j < g.temps.size(); ++j) o << "    t" << j << "[i] = " << g.temps[j].first << ";\n";
+  const std::string mulHead = "ws::imulf(", mulTail = ",ofl)";
+  bool anyMul = false;
+  for (auto& t : g.temps)
+    anyMul |= t.first.compare(0, mulHead.size(), mulHead) == 0 && t.first.size() > mulTail.size() &&
+              t.first.compare(t.first.size() - mulTail.size(), mulTail.size(), mulTail) == 0;
+  if (anyMul) {
+    o << "    unsigned wide = 0;\n";
+    for (size_t j = 0; j < g.temps.size(); ++j) {
+      const std::string& e = g.temps[j].first;
+      const bool mul = e.compare(0, mulHead.size(), mulHead) == 0 && e.size() > mulTail.size() &&
+                       e.compare(e.size() - mulTail.size(), mulTail.size(), mulTail) == 0;
+      o << "    t" << j << "[i] = "
+        << (mul ? "ws::imul32w(" + e.substr(mulHead.size(), e.size() - mulHead.size() - mulTail.size()) + ",wide)" : e)
+        << ";\n";
+    }
+    o << "    if (wide) {\n      ofl = 0;\n";
+    for (size_t j = 0; j < g.temps.size(); ++j) o << "      t" << j << "[i] = " << g.temps[j].first << ";\n";
+    o << "    }\n";
+  } else {
+    for (size_t j = 0; j < g.temps.size(); ++j) o << "    t" << j << "[i] = " << g.temps[j].first << ";\n";
+  }
   if (!g.temps.empty()) o << "    this->ofl |= live ? ofl : 0u;\n";
   o << "  }\n";
   o << "  __device__ __forceinline__ void finish() const { if (ofl) *L.env.ovf = 1; }\n";

@@ -86,6 +86,12 @@ WS_DI i64 isubf(i64 a, i64 b, unsigned& of) {
   of |= (unsigned)((u64)((a ^ b) & (a ^ r)) >> 63);
   return r;
 }
+// 32 x 32-bit product of the operands' low words, exact when both operands fit in int32; `wide` collects
+// the operands that do not (the caller then recomputes with imulf).  Branch-free.
+WS_DI i64 imul32w(i64 a, i64 b, unsigned& wide) {
+  wide |= ((unsigned)((u64)a >> 32) ^ (unsigned)((int)a >> 31)) | ((unsigned)((u64)b >> 32) ^ (unsigned)((int)b >> 31));
+  return (i64)(int)a * (i64)(int)b;
+}
 WS_DI i64 imulf(i64 a, i64 b, unsigned& of) {
   if (a == (i64)(int)a && b == (i64)(int)b) return (i64)(int)a * (i64)(int)b;  // 32 x 32 bits: exact
   const i64 r = (i64)((u64)a * (u64)b);
@@ -460,12 +466,13 @@ WS_DI bool mbarTest(unsigned bar, unsigned parity) {
       : "memory");
   return ok != 0;
 }
-// Waits for the phase with the given parity; gives up after about 2^32 SM cycles (~2 s) and returns false.
-WS_DI bool mbarWait(unsigned bar, unsigned parity) {
+// Waits for the phase with the given parity; gives up after about 2^log2Limit SM cycles (32: ~2 s) and
+// returns false.
+WS_DI bool mbarWait(unsigned bar, unsigned parity, int log2Limit = 32) {
   if (mbarTest(bar, parity)) return true;
   const long long t0 = clock64();
   while (!mbarTest(bar, parity)) {
-    if (clock64() - t0 > (1ll << 32)) return false;
+    if (clock64() - t0 > (1ll << log2Limit)) return false;
     __nanosleep(32);
   }
   return true;
@@ -628,6 +635,9 @@ struct Launch {
   int nkeys, naggs, rowWords; // interpreter only (JIT: compile-time)
   int fastWords;              // interpreter only: words of a register row
   int stages;                 // shared-memory stages of staged scans (0: loads straight from global memory)
+  int sumShift;               // integer SUM words need no overflow test while (argument magnitude >> sumShift)
+                              // is 0 (set at launch from the rows a thread adds; -1: always test)
+  int waitLog2;               // staged scans: a wait for a tile stage gives up after 2^waitLog2 SM cycles
   // aggregation outputs
   u64* part;                  // per-CTA partial rows
   u64* rows;                  // result rows

@@ -153,7 +153,11 @@ struct KernelSet {
   bool interp = true;
 };
 const KernelSet& interpKernels();
-// Launches `f` with the Launch descriptor as its only parameter.
+// Launch.sumShift of a scan of ntiles tiles on `grid` CTAs (the integer SUM bound of ws_kern.cuh).
+int sumShiftFor(int64_t ntiles, unsigned grid);
+// Launch.waitLog2: the staged scans' wait limit (WARPSTORE_B200_WAIT_LIMIT_LOG2, default 32).
+int stagedWaitLog2();
+// Launches `f` with the Launch descriptor as its only parameter (sumShift set for the grid).
 void launchScan(CUfunction f, unsigned grid, size_t smem, const Launch& L, int threads = kThreads);
 // Persistent grid: resident CTAs per SM x SMs, capped by the tile count.
 unsigned persistentGrid(CUfunction f, size_t smem, int64_t ntiles, int threads = kThreads);

@@ -121,8 +121,10 @@ WS_DI void forEachRow(const Launch& L, Ev& ev, F&& f) {
 // warp once it has read the stage).  The producer refills a stage as soon as every consumer warp has
 // released it, so consumers never wait on a CTA-wide barrier.  Tiles that cannot be copied in bulk (a
 // batch's ragged last tile, a column not 16-byte aligned) are marked "direct": their full barrier gets
-// a plain arrive and the consumers read global memory as forEachRow does.  Every wait is bounded; one
-// that runs out sets err[2] and ends that thread's loop.
+// a plain arrive and the consumers read global memory as forEachRow does.  Every wait is bounded
+// (2^L.waitLog2 cycles); one that runs out sets err[2] and ends that warp's loop.  Before the producer
+// warp leaves, it waits (bounded, ~2 s) until the copies of the stages it issued last have landed, so
+// no bulk copy is still writing into the CTA's shared memory when the CTA ends.
 constexpr int kStagedThreads = kThreads + 32;
 
 template <class Ev, class F>
@@ -147,12 +149,14 @@ WS_DI void forEachRowStaged(const Launch& L, Ev& ev, unsigned char* stages, int 
   if (warp == kConsumerWarps) {  // ---- producer warp (one elected lane)
     if (lane == 0) {
       int pb = K > 0 ? batchOfTile(L, tFirst) : 0, pbatch = -1;
+      i64 issued = 0;
       for (i64 k = 0; k < K; ++k) {
         const int s = (int)(k % S);
-        if (k >= S && !mbarWait(smemAddr(&empty[s]), (unsigned)(((k / S) - 1) & 1))) {
+        if (k >= S && !mbarWait(smemAddr(&empty[s]), (unsigned)(((k / S) - 1) & 1), L.waitLog2)) {
           L.err[2] = 1;
           break;
         }
+        issued = k + 1;
         const i64 t = tFirst + k;
         while (t >= __ldg(L.tileStart + pb + 1)) ++pb;
         if (pb != pbatch) {
@@ -171,6 +175,10 @@ WS_DI void forEachRowStaged(const Launch& L, Ev& ev, unsigned char* stages, int 
           mbarArrive(bar);
         }
       }
+      // drain: the last phase issued on each stage completes when its copies have landed (earlier
+      // phases completed before their stage was reissued)
+      for (i64 k = issued > S ? issued - S : 0; k < issued; ++k)
+        if (!mbarWait(smemAddr(&full[(int)(k % S)]), (unsigned)((k / S) & 1))) L.err[2] = 1;
     }
     __syncwarp();
     return;
@@ -180,8 +188,8 @@ WS_DI void forEachRowStaged(const Launch& L, Ev& ev, unsigned char* stages, int 
   for (i64 k = 0; k < K; ++k) {
     const i64 t = tFirst + k;
     const int s = (int)(k % S);
-    if (!mbarWait(smemAddr(&full[s]), (unsigned)((k / S) & 1))) {
-      L.err[2] = 1;
+    if (!__all_sync(0xffffffffu, mbarWait(smemAddr(&full[s]), (unsigned)((k / S) & 1), L.waitLog2))) {
+      if (lane == 0) L.err[2] = 1;
       break;
     }
     while (t >= __ldg(L.tileStart + b + 1)) ++b;
@@ -277,6 +285,31 @@ WS_DI void addCarry(u64* w, u64 x, u64* spillHi) {
   if ((int)((ho ^ hr) & (hx ^ hr)) < 0) atomicAdd(spillHi, (int)hx < 0 ? ~0ull : 1ull);  // signed overflow
   *w = r;
 }
+// Exact integer sums without a test per addition.  A thread adds at most R rows into any one of its
+// integer SUM words.  While every argument x has |x| <= 2^(63 - k), with 2^k >= R, no partial sum of
+// those additions leaves the int64 range, so the words need no overflow test.  The host sets
+// L.sumShift = 31 - k for each launch (-1 when no k applies).  sumMagnitude ORs the high words of the
+// row's SUM arguments' magnitudes (x >= 0: x >> 32; x < 0: ~x >> 32 = (|x| - 1) >> 32); the bound holds
+// while (magnitude >> sumShift) == 0.  A thread that meets a row breaking it switches to tested
+// additions (signed overflow carried into the int128 spill) for the rest of the launch, so words that
+// take unbounded values are always tested from their first such value on.
+template <class Ev>
+WS_DI unsigned sumMagnitude(const Ev& ev, const u64* x) {
+  unsigned m = 0;
+#pragma unroll
+  for (int a = 0; a < Ev::NA; ++a) {
+    if (a >= ev.na()) break;
+    if (ev.kind(a) == SK_ISUM) {
+      const unsigned hi = (unsigned)(x[ev.fwoff(a)] >> 32);
+      m |= hi ^ (unsigned)((int)hi >> 31);
+    }
+  }
+  return m;
+}
+WS_DI bool sumsNeedTests(const Launch& L, unsigned magnitude) {
+  return L.sumShift < 0 || (magnitude >> L.sumShift) != 0;
+}
+
 // w += x (register rows); spill = this group's [slot][2] int128 counters
 template <class Ev>
 WS_DI void fastCombine(const Ev& ev, u64* w, const u64* x, u64* spill) {
@@ -503,6 +536,8 @@ __device__ void aggNoKeys(const Launch& L) {
   __syncthreads();
   u64 f[FW];
   fastIdentity(ev, f);
+  // register rows: a tested addition costs about what the magnitude test of the bounded form does
+  // (no shared-memory ordering is at stake), so every addition is tested here
   scanRows(L, ev, [&](int i, int, i64) {
     u64 x[FW];
     fastOfInput(ev, i, x);
@@ -564,6 +599,7 @@ __device__ void aggDensePriv(const Launch& L) {
     for (int j = tid; j < G * 2 * Ev::NA; j += blockDim.x) spill[j] = 0;
   }
   __syncthreads();
+  bool tested = false;  // this thread's sums take tested additions (sticky, see sumMagnitude)
   auto row = [&](int i, int, i64) {
     i64 gi;
     if (!denseIndex(L, ev, i, gi)) {
@@ -572,8 +608,25 @@ __device__ void aggDensePriv(const Launch& L) {
     }
     u64 x[FW];
     fastOfInput(ev, i, x);
-    u64* sp = spill + (unsigned)gi * (2u * Ev::NA);
+    tested |= sumsNeedTests(L, sumMagnitude(ev, x));
     u64* p = priv + ((unsigned)gi * (unsigned)fw * T + tid);
+    if (!tested) {  // no atomics on this path: the slots' read-modify-writes overlap
+#pragma unroll
+      for (int a = 0; a < Ev::NA; ++a) {
+        if (a >= ev.na()) break;
+        const int o = ev.fwoff(a);
+        u64* q = p + (size_t)o * T;
+        switch (ev.kind(a)) {
+          case SK_COUNT: case SK_ISUM: *q += x[o]; break;
+          case SK_IMIN: case SK_DMIN: if ((i64)x[o] < (i64)*q) *q = x[o]; break;
+          case SK_IMAX: case SK_DMAX: if ((i64)x[o] > (i64)*q) *q = x[o]; break;
+          case SK_DSUM: *q = (u64)__double_as_longlong(__longlong_as_double((i64)*q) + __longlong_as_double((i64)x[o])); break;
+          default: break;
+        }
+      }
+      return;
+    }
+    u64* sp = spill + (unsigned)gi * (2u * Ev::NA);
 #pragma unroll
     for (int a = 0; a < Ev::NA; ++a) {
       if (a >= ev.na()) break;

@@ -709,6 +709,8 @@ static void aggRun(ws_aggregator& A, const ws_expr_env& env, const ws_jit_progra
     prep->smem = sh.smem;
     prep->threads = sh.threads;
     prep->L = L;
+    prep->L.sumShift = sumShiftFor(L.ntiles, grid);
+    prep->L.waitLog2 = stagedWaitLog2();
     prep->desc = std::move(d);
     prep->part = std::move(part);
     prep->ready = true;

@@ -250,8 +250,31 @@ uint8_t* pinnedStage(size_t bytes) {
 }
 void stageCopied() { WS_CK(cudaEventRecord(tStageEv, stream())); }
 
-void launchScan(CUfunction f, unsigned grid, size_t smem, const Launch& L, int threads) {
+int stagedWaitLog2() {
+  // WARPSTORE_B200_WAIT_LIMIT_LOG2 (4..32, default 32 = ~2 s): how long a staged scan waits for a tile
+  // stage before it reports the tile as late (err[2]); a small value makes the waits run out (tests)
+  static const int v = [] {
+    const char* e = getenv("WARPSTORE_B200_WAIT_LIMIT_LOG2");
+    const int x = e ? atoi(e) : 32;
+    return x < 4 ? 4 : x > 32 ? 32 : x;
+  }();
+  return v;
+}
+
+int sumShiftFor(int64_t ntiles, unsigned grid) {
+  // rows one thread adds into a word: 4 per tile, ceil(ntiles / grid) tiles per CTA (contiguous ranges)
+  const int64_t g = grid ? grid : 1;
+  const int64_t rows = std::max<int64_t>(1, (ntiles + g - 1) / g) * 4;
+  int k = 0;
+  while (((int64_t)1 << k) < rows) ++k;
+  return k <= 31 ? 31 - k : -1;
+}
+
+void launchScan(CUfunction f, unsigned grid, size_t smem, const Launch& Lin, int threads) {
   if (smem > 0) WS_CKD(drv().funcSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)smem));
+  Launch L = Lin;
+  L.sumShift = sumShiftFor(L.ntiles, grid);
+  L.waitLog2 = stagedWaitLog2();
   void* args[] = {(void*)&L};
   WS_CKD(drv().launchKernel(f, grid, 1, 1, (unsigned)threads, 1, 1, (unsigned)smem, (CUstream)stream(), args, nullptr));
   countLaunch();
