@@ -89,10 +89,9 @@ __global__ void kGather(const uint8_t* src, int esize, const int32_t* idx, int64
 }
 
 // ---------------------------------------------------------------- hash join
-// Table: cap (power of two) slots of {stored key, int32 build row, pad} (16 bytes, two slots per
-// 32-byte sector).  The stored key is key ^ 2^63, so an all-zero slot is empty: the one key that
-// maps to 0 is INT64_MIN, the BIGINT NULL sentinel, which is never inserted.  Linear probing from
-// h = mix64(key): slot h & (cap - 1).
+// Keys are hashed with h = mix64(key).  The stored key is key ^ 2^63, so an all-zero slot is empty:
+// the one key that maps to 0 is INT64_MIN, the BIGINT NULL sentinel, which is never inserted.  The
+// table's layout (buckets of keys, rows apart) is described at jBucket below.
 //
 // A build side whose table would not stay in L2 is split into P = 2^b passes by the top b bits of h:
 // pass p builds the table of the build keys with h >> (64 - b) == p (reusing one buffer) and probes
@@ -102,11 +101,6 @@ __global__ void kGather(const uint8_t* src, int esize, const int32_t* idx, int64
 // Keys: I32 views widen to int64 (their sentinel is NULL), I64 views as stored, F64 views (bit
 // patterns converted by the engine) truncated, NaN = NULL (src/gpu.cu:180-202).
 constexpr u64 kJSign = 0x8000000000000000ull;
-struct __align__(16) JSlot {
-  u64 key;  // key ^ kJSign; 0 = empty
-  int row;
-  int pad;
-};
 
 __device__ __forceinline__ bool joinKeyStream(const ws_col_view& c, int64_t r, long long& k) {
   if (c.t == 0 || c.t == 3) {
@@ -123,10 +117,25 @@ __device__ __forceinline__ bool joinKeyStream(const ws_col_view& c, int64_t r, l
   return d == d;
 }
 
-// Both slots of a 32-byte sector in one 256-bit load (one L1 request per lane instead of two; the
-// probe's random table reads are bound by L1 requests).  `p` is 32-byte aligned (an even slot).
-__device__ __forceinline__ void ldSector(const JSlot* p, ulonglong2& a, ulonglong2& b) {
-  asm("ld.global.nc.v4.u64 {%0,%1,%2,%3}, [%4];" : "=l"(a.x), "=l"(a.y), "=l"(b.x), "=l"(b.y) : "l"(p));
+// Hash table: buckets of 4 keys, one 32-byte sector each (key ^ 2^63; 0 = empty), and the build row of
+// slot i in a parallel int32 array read only when slot i matched.  The bucket of a key is the low 32
+// bits of its hash scaled to the bucket count (any count: the table is sized to the keys, not to a
+// power of two); a full bucket overflows into the next one, so a probe walks buckets from the key's
+// own until one has an empty slot.  A probe costs one 256-bit load when its bucket is not full.
+__device__ __forceinline__ u64 jBucket(u64 h, u64 nbuckets) {
+  return nbuckets <= 0xffffffffull ? (u64)__umulhi((unsigned)h, (unsigned)nbuckets)
+                                   : ((h & 0xffffffffull) * nbuckets) >> 32;
+}
+// L2 policy for the bucket loads: keep the key table resident while the probe keys stream past
+__device__ __forceinline__ u64 jKeepPolicy() {
+  u64 pol;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ void ldBucket(const u64* p, u64 pol, u64 (&k)[4]) {
+  asm("ld.global.nc.L2::cache_hint.v4.u64 {%0,%1,%2,%3}, [%4], %5;"
+      : "=l"(k[0]), "=l"(k[1]), "=l"(k[2]), "=l"(k[3])
+      : "l"(p), "l"(pol));
 }
 
 struct JPass {
@@ -186,24 +195,36 @@ __global__ void kJoinStats(ws_col_view key, int64_t base, int64_t n, int bits, u
     if (h[i]) atomicAdd(&st[3 + i], h[i]);
 }
 
-// Inserts the pass's build rows of [base, base + n).  The table has >= 2x the pass's keys, so an
-// insert meets an empty slot within cap steps; err is raised otherwise.
-__global__ void kJoinBuild(ws_col_view key, int64_t base, int64_t n, JPass jp, JSlot* t, u64 mask, int* err) {
+// Inserts the pass's build rows of [base, base + n): CAS into the first empty slot of the key's bucket
+// or of the buckets after it.  The table has more slots than the pass's keys, so an insert meets an
+// empty slot within nbuckets steps; err is raised otherwise.  (Measured: giving each thread several
+// rows whose loads overlap ran slower, 0.58 against 0.47 ms for 7.5M keys: the inserts are bound by
+// the table's random DRAM traffic, not by their latency.)
+__global__ void kJoinBuild(ws_col_view key, int64_t base, int64_t n, JPass jp, u64* keys, int* rows, u64 nbuckets,
+                           int* err) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     long long k;
     if (!joinKeyStream(key, base + i, k)) continue;
     const u64 h = mix64((u64)k);
     if (!jp.mine(h)) continue;
     const u64 sk = (u64)k ^ kJSign;
-    u64 s = h & mask;
+    u64 b = jBucket(h, nbuckets);
     bool done = false;
-    for (u64 p = 0; p <= mask; ++p) {
-      if (atomicCAS(&t[s].key, 0ull, sk) == 0ull) {
-        t[s].row = (int)(base + i);
-        done = true;
-        break;
+    for (u64 step = 0; step < nbuckets && !done; ++step) {
+      u64* bk = keys + b * 4;
+      // the bucket through L2 (other threads' inserts are visible there); a slot seen empty may have been
+      // taken since: the CAS decides, and a lost CAS moves on to the next slot
+      const ulonglong2 lo = __ldcg((const ulonglong2*)bk), hi = __ldcg((const ulonglong2*)bk + 1);
+      const u64 seen[4] = {lo.x, lo.y, hi.x, hi.y};
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        if (done || seen[q] != 0ull) continue;
+        if (atomicCAS((unsigned long long*)(bk + q), 0ull, sk) == 0ull) {
+          rows[b * 4 + q] = (int)(base + i);
+          done = true;
+        }
       }
-      s = (s + 1) & mask;
+      b = b + 1 == nbuckets ? 0 : b + 1;
     }
     if (!done) *err = 1;
   }
@@ -213,6 +234,7 @@ __global__ void kJoinBuild(ws_col_view key, int64_t base, int64_t n, JPass jp, J
 // counter per flush (coalesced writes).  Pairs at or past `capacity` are not written: the host
 // reruns with the exact count.
 constexpr int kJThreads = 256, kJPer = 4, kJStage = 256;
+constexpr int kJHashPer = 2;  // probe rows per lane and step of the hash probe (1 and 4 measured slower)
 constexpr int kJWarps = kJThreads / 32;
 
 struct JOut {
@@ -322,83 +344,143 @@ __global__ void __launch_bounds__(kJThreads) kJoinDenseProbe(ws_col_view key, in
   jFlush(out, st, fill, lane);
 }
 
-// ---- hash join probe: each warp takes kJPer x 32 consecutive probe rows per step (one coalesced
-// load per row slot).  A lane keeps its up-to-kJPer keys of this pass in a small queue and walks them
-// one after another, two slots (one 32-byte sector) per step, so that a warp runs as long as its
-// longest queue rather than the sum of its longest probe chains.  Matches are staged as they are
-// found.
-__global__ void __launch_bounds__(kJThreads) kJoinProbe(ws_col_view key, int64_t base, int64_t n, JPass jp,
-                                                        const JSlot* t, unsigned mask, JOut out) {
-  __shared__ int2 stage[kJWarps][kJStage];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int2* st = stage[warp];
-  int fill = 0;  // warp-uniform
-  const int64_t wstep = (int64_t)gridDim.x * kJWarps * 32 * kJPer;
-  for (int64_t w0 = ((int64_t)blockIdx.x * kJWarps + warp) * 32 * kJPer; w0 < n; w0 += wstep) {
-    // queue of this lane's keys in the pass (q0 is the one being walked)
-    u64 qk[kJPer];
-    unsigned qs[kJPer];
-    int qr[kJPer];
-    int nq = 0;
+// ---- hash join probe: each warp takes kJHashPer x 32 consecutive probe rows per step (one coalesced
+// load per row slot), so each lane has kJHashPer keys, and works in rounds of independent loads: the
+// keys; the first bucket of every key; the build row of every key's first matching slot; then the
+// first matches are staged.  Keys with more to do (a second match in their bucket, or a full bucket
+// whose run goes on) are rare; they are queued per warp and walked 32 at a time, one per lane, so the
+// common path stays short and the walks run with all lanes busy.  Matches are staged per warp and
+// written in coalesced runs.
+struct JRest {   // a key whose probe goes on
+  u64 sk;        // stored key
+  u64 bucket;    // its current bucket
+  int probeRow;
+  unsigned m;    // slots of the current bucket that matched and are not emitted yet
+  int flags;     // 1: the current bucket is full (the run goes on); 2: the key has matched
+};
+constexpr int kJRestCap = 64;
+
+// Walks up to 32 queued keys, one per lane (all lanes of the warp call it; n warp-uniform, <= 32).
+__device__ __forceinline__ void jWalk(const JOut& out, int2* st, int& fill, const JRest* q, int cnt, const u64* keys,
+                                      const int* rows, u64 nbuckets, u64 pol, int lane) {
+  const unsigned full = 0xffffffffu;
+  bool live = lane < cnt;
+  JRest e{};
+  if (live) e = q[lane];
+  u64 steps = 0;
+  while (__any_sync(full, live)) {
+    while (__any_sync(full, live && e.m != 0)) {
+      const bool has = live && e.m != 0;
+      int r = 0;
+      if (has) {
+        const int s = __ffs(e.m) - 1;
+        e.m &= e.m - 1;
+        r = __ldg(rows + e.bucket * 4 + s);
+        e.flags |= 2;
+        if (out.matched) out.matched[r - out.rowBase] = 1;
+      }
+      jStage(out, st, fill, has, r, e.probeRow, lane);
+    }
+    bool unmatched = false;
+    if (live) {
+      if ((e.flags & 1) && ++steps < nbuckets) {
+        e.bucket = e.bucket + 1 == nbuckets ? 0 : e.bucket + 1;
+        u64 k4[4];
+        ldBucket(keys + e.bucket * 4, pol, k4);
 #pragma unroll
-    for (int j = 0; j < kJPer; ++j) {
-      const int64_t r = w0 + j * 32 + lane;
-      long long k;
-      const bool valid = r < n && joinKeyStream(key, base + r, k);
-      // outer join: a NULL-key probe row matches nothing; it is emitted once, in pass 0
-      jStage(out, st, fill, out.outer && jp.pass == 0 && r < n && !valid, -1, (int)(base + r), lane);
-      if (valid) {
-        const u64 h = mix64((u64)k);
-        if (jp.mine(h)) {
-#pragma unroll
-          for (int q = 0; q < kJPer; ++q)
-            if (q == nq) qk[q] = (u64)k ^ kJSign, qs[q] = (unsigned)(h & mask), qr[q] = (int)(base + r);
-          ++nq;
-        }
+        for (int s = 0; s < 4; ++s) e.m |= (unsigned)(k4[s] == e.sk) << s;
+        e.flags = (e.flags & 2) | (k4[0] && k4[1] && k4[2] && k4[3] ? 1 : 0);
+      } else {
+        live = false;
+        unmatched = out.outer && !(e.flags & 2);
       }
     }
-    unsigned steps = 0;
-    bool headHit = false;  // the key at the head of the queue has matched
-    while (__any_sync(0xffffffffu, nq > 0)) {
-      bool hitA = false, hitB = false, done = true, unmatched = false;
-      int rowA = 0, rowB = 0, pr = 0;
-      if (nq > 0) {
-        const unsigned s0 = qs[0];
-        const unsigned even = s0 & ~1u;
-        ulonglong2 a, b;
-        ldSector(t + even, a, b);
-        pr = qr[0];
-        done = false;
-        // slot `even` counts only when the walk starts there; slot even + 1 always
-        if (s0 == even) {
-          if (a.x == 0) done = true;
-          else if (a.x == qk[0]) hitA = true, rowA = (int)(unsigned)a.y;
-        }
-        if (!done) {
-          if (b.x == 0) done = true;
-          else if (b.x == qk[0]) hitB = true, rowB = (int)(unsigned)b.y;
-        }
-        ++steps;
-        headHit |= hitA || hitB;
-        if (hitA && out.matched) out.matched[rowA - out.rowBase] = 1;
-        if (hitB && out.matched) out.matched[rowB - out.rowBase] = 1;
-        if (!done && steps <= mask) {
-          qs[0] = (even + 2) & mask;
-        } else {
-          unmatched = out.outer && !headHit;
+    jStage(out, st, fill, unmatched, -1, e.probeRow, lane);
+  }
+}
+
+__global__ void __launch_bounds__(kJThreads) kJoinProbe(ws_col_view key, int64_t base, int64_t n, JPass jp,
+                                                        const u64* keys, const int* rows, u64 nbuckets, JOut out) {
+  __shared__ int2 stage[kJWarps][kJStage];
+  __shared__ JRest restQ[kJWarps][kJRestCap];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned full = 0xffffffffu, lower = (1u << lane) - 1u;
+  int2* st = stage[warp];
+  JRest* rq = restQ[warp];
+  int fill = 0, queued = 0;  // warp-uniform
+  const u64 pol = jKeepPolicy();
+  const int64_t wstep = (int64_t)gridDim.x * kJWarps * 32 * kJHashPer;
+  for (int64_t w0 = ((int64_t)blockIdx.x * kJWarps + warp) * 32 * kJHashPer; w0 < n; w0 += wstep) {
+    u64 sk[kJHashPer], bk[kJHashPer], slot[kJHashPer][4];
+    bool act[kJHashPer];
+    // round 1: keys
 #pragma unroll
-          for (int q = 0; q < kJPer - 1; ++q) qk[q] = qk[q + 1], qs[q] = qs[q + 1], qr[q] = qr[q + 1];
-          --nq;
-          steps = 0;
-          headHit = false;
-        }
+    for (int j = 0; j < kJHashPer; ++j) {
+      const int64_t r = w0 + j * 32 + lane;
+      long long k = 0;
+      const bool valid = r < n && joinKeyStream(key, base + r, k);
+      // outer join: a NULL-key probe row matches nothing; it is emitted once, in pass 0
+      if (out.outer) jStage(out, st, fill, jp.pass == 0 && r < n && !valid, -1, (int)(base + r), lane);
+      const u64 h = mix64((u64)k);
+      act[j] = valid && jp.mine(h);
+      sk[j] = (u64)k ^ kJSign;
+      bk[j] = jBucket(h, nbuckets);
+    }
+    // round 2: first buckets
+#pragma unroll
+    for (int j = 0; j < kJHashPer; ++j)
+      if (act[j]) ldBucket(keys + bk[j] * 4, pol, slot[j]);
+    // round 3: the build row of each key's first matching slot
+    unsigned m[kJHashPer];
+    bool more[kJHashPer];
+    int row[kJHashPer];
+#pragma unroll
+    for (int j = 0; j < kJHashPer; ++j) {
+      m[j] = 0;
+      more[j] = false;
+      if (act[j]) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) m[j] |= (unsigned)(slot[j][q] == sk[j]) << q;
+        more[j] = slot[j][0] && slot[j][1] && slot[j][2] && slot[j][3];  // full: the run may go on
       }
-      jStage(out, st, fill, hitA, rowA, pr, lane);
-      jStage(out, st, fill, hitB, rowB, pr, lane);
-      jStage(out, st, fill, unmatched, -1, pr, lane);
+      row[j] = m[j] ? __ldg(rows + bk[j] * 4 + (__ffs(m[j]) - 1)) : 0;
+    }
+    // round 4: stage the first matches (and an outer join's unmatched rows whose run ended); queue the rest
+#pragma unroll
+    for (int j = 0; j < kJHashPer; ++j) {
+      const int pr = (int)(base + w0 + j * 32 + lane);
+      const bool hit = m[j] != 0;
+      if (hit && out.matched) out.matched[row[j] - out.rowBase] = 1;
+      const bool unmatched = out.outer && act[j] && !hit && !more[j];
+      jStage(out, st, fill, hit || unmatched, hit ? row[j] : -1, pr, lane);
+      if (hit) m[j] &= m[j] - 1;
+      const bool rest = m[j] != 0 || more[j];
+      const unsigned rb = __ballot_sync(full, rest);
+      if (!rb) continue;
+      if (queued + __popc(rb) > kJRestCap) {  // walk a batch first
+        __syncwarp();
+        const int cnt = min(queued, 32);
+        jWalk(out, st, fill, rq + queued - cnt, cnt, keys, rows, nbuckets, pol, lane);
+        queued -= cnt;
+        __syncwarp();
+      }
+      if (rest) rq[queued + __popc(rb & lower)] = JRest{sk[j], bk[j], pr, m[j], (more[j] ? 1 : 0) | (hit ? 2 : 0)};
+      queued += __popc(rb);
+      if (queued >= 32) {
+        __syncwarp();
+        jWalk(out, st, fill, rq + queued - 32, 32, keys, rows, nbuckets, pol, lane);
+        queued -= 32;
+        __syncwarp();
+      }
     }
   }
   __syncwarp();
+  while (queued > 0) {
+    const int cnt = min(queued, 32);
+    jWalk(out, st, fill, rq + queued - cnt, cnt, keys, rows, nbuckets, pol, lane);
+    queued -= cnt;
+    __syncwarp();
+  }
   jFlush(out, st, fill, lane);
 }
 
@@ -413,26 +495,19 @@ int64_t joinTableBudget() {
 }
 
 
-int64_t pow2AtLeast(int64_t x) {
-  int64_t c = 2;
-  while (c < x) c <<= 1;
-  return c;
-}
 
-// Hash join table slots for `keys` build keys and `probes` probe rows: the next power of two of 4 x
-// keys (load <= 1/4, shorter clusters: 7.5M x 60M measured 2.48 against 2.66 ms) when the probe side
-// has at least 8 rows per key and the table stays within 2 GiB, else of 2 x keys (a smaller probe side
-// does not repay clearing the larger table: 7.5M x 8M measured 0.90 against 0.85 ms);
+// Hash join table slots for `keys` build keys: 2 per key (load 1/2: a bucket of 4 is full for about
+// 1 key in 7), a multiple of the 4-slot bucket with at least one spare bucket;
 // WARPSTORE_B200_JOIN_SLOTS_PER_KEY = 2..16 fixes the factor.
-int64_t joinTableSlots(int64_t keys, int64_t probes) {
+constexpr int64_t kJSlotBytes = 8 + 4;  // key + build row
+int64_t joinTableSlots(int64_t keys) {
   static const int64_t fixed = [] {
     const char* e = getenv("WARPSTORE_B200_JOIN_SLOTS_PER_KEY");
     const long long v = e ? atoll(e) : 0;
     return v >= 2 && v <= 16 ? (int64_t)v : (int64_t)0;
   }();
-  if (fixed) return pow2AtLeast(fixed * keys);
-  const int64_t c = pow2AtLeast(4 * keys);
-  return probes >= 8 * keys && c * (int64_t)sizeof(JSlot) <= ((int64_t)2 << 30) ? c : pow2AtLeast(2 * keys);
+  const int64_t per = fixed ? fixed : 2;
+  return ((per * keys + 3) / 4 + 1) * 4;
 }
 
 }  // namespace
@@ -698,8 +773,8 @@ static void joinImpl(ws_col_view build_key, const int64_t* boff, int pb, ws_col_
     for (int q = 0; q < pb; ++q) {
       const int64_t nq = boff[q + 1] - boff[q];
       const int64_t npq = pb == 1 ? np : poff[q + 1] - poff[q];  // probe rows joined with build partition q
-      while (bits[q] < 6 && joinTableSlots((nq >> bits[q]) + 1, npq >> bits[q]) * (int64_t)sizeof(JSlot) > joinTableBudget())
-        ++bits[q];
+      (void)npq;
+      while (bits[q] < 6 && joinTableSlots((nq >> bits[q]) + 1) * kJSlotBytes > joinTableBudget()) ++bits[q];
     }
     // Build-key statistics (non-NULL count, min, max, keys per hash pass) of every partition.
     DBuf<unsigned long long> stats((int64_t)pb * kJStatWords);
@@ -730,14 +805,15 @@ static void joinImpl(ws_col_view build_key, const int64_t* boff, int pb, ws_col_
         continue;
       }
       for (int p = 0; p < (1 << bits[q]); ++p) {
-        const int64_t c = joinTableSlots(bits[q] ? (int64_t)st[3 + p] : keys, (pb == 1 ? np : poff[q + 1] - poff[q]) >> bits[q]);
+        const int64_t c = joinTableSlots(bits[q] ? (int64_t)st[3 + p] : keys);
         cap[q].push_back(c);
         tableSlots = std::max(tableSlots, c);
       }
     }
     bool anyDense = false, anyHash = false;
     for (int q = 0; q < pb; ++q) anyDense |= dense[q] != 0, anyHash |= !cap[q].empty();
-    DBuf<JSlot> table(anyHash ? tableSlots : 1);
+    DBuf<u64> tkeys(anyHash ? tableSlots : 4);
+    DBuf<int> trows(anyHash ? tableSlots : 4);
     DBuf<int> dtable(anyDense ? denseSlots : 1), next(anyDense ? nextRows : 1);
     DBuf<int> flags(2);  // [0] hash table full, [1] duplicate dense keys
     WS_CK(cudaMemsetAsync(flags.p, 0, 8, stream()));
@@ -773,8 +849,9 @@ static void joinImpl(ws_col_view build_key, const int64_t* boff, int pb, ws_col_
             WS_LAUNCH(kJoinDenseBuild, gridFor(nbq), 256, 0, build_key, boff[q], nbq, dtable.p, kmin[q], next.p,
                       flags.p + 1);
           } else {
-            WS_CK(cudaMemsetAsync(table.p, 0, sizeof(JSlot) * c, stream()));
-            WS_LAUNCH(kJoinBuild, gridFor(nbq), 256, 0, build_key, boff[q], nbq, jp, table.p, (u64)(c - 1), flags.p);
+            WS_CK(cudaMemsetAsync(tkeys.p, 0, 8 * c, stream()));
+            WS_LAUNCH(kJoinBuild, gridFor(nbq), 256, 0, build_key, boff[q], nbq, jp, tkeys.p, trows.p, (u64)(c / 4),
+                      flags.p);
           }
           for (int p = 0; p < pp; ++p) {  // probe partitions joined with build partition q
             if (pb != 1 && p != q) continue;
@@ -782,11 +859,12 @@ static void joinImpl(ws_col_view build_key, const int64_t* boff, int pb, ws_col_
             if (!n) continue;
             const JOut jo{ob.p, op.p, outStart[p], capOut[p], counters.p + p, outer, matched, boff[q]};
             const int grid = gridFor((n + kJPer - 1) / kJPer, kJThreads);
+            const int hgrid = gridFor((n + kJHashPer - 1) / kJHashPer, kJThreads);
             if (dense[q])
               WS_LAUNCH(kJoinDenseProbe, grid, kJThreads, 0, probe_key, poff[p], n, dtable.p, kmin[q], range[q], next.p,
                         boff[q], flags.p + 1, jo);
             else
-              WS_LAUNCH(kJoinProbe, grid, kJThreads, 0, probe_key, poff[p], n, jp, table.p, (unsigned)(c - 1), jo);
+              WS_LAUNCH(kJoinProbe, hgrid, kJThreads, 0, probe_key, poff[p], n, jp, tkeys.p, trows.p, (u64)(c / 4), jo);
           }
         }
       }
