@@ -246,6 +246,16 @@ int ws_eval_at_int(const ws_expr_env* env, int ncols, ws_prog prog, const int32_
  * encoder runs on the host and writes the formats 1-6. */
 int ws_encode_column(const void* src, int t, int64_t n, int enc, void** out, int64_t* bytes, int* enc_used);
 
+/* Table::encodeColumn (src/storage.cu:1138-1192) on the device: a segment column of n values (ptype
+ * WS_PT_I32 / I64 / F64, device memory) in the engine's own formats, by the engine's rule: integers
+ * whose value range fits as uint8 / uint16 (/ uint32 for BIGINT) offsets from the minimum (enc 1 / 2 /
+ * 3); doubles with at most 255 distinct bit patterns as a dictionary (enc 4, entries in order of first
+ * occurrence); other doubles that are exact decimals with at most 4 digits after the point as uint16 /
+ * uint32 offsets (enc 5 / 6, the first scale that holds every value decides); otherwise, and for fewer
+ * than 1024 rows, *enc_used = 0 (keep the column raw, *out = NULL).  *out (ws_tmp_free) receives
+ * *bytes bytes: the 16-byte header, the dictionary (enc 4), the codes and 16 pad bytes. */
+int ws_encode_column_engine(const void* src, int ptype, int64_t n, void** out, int64_t* bytes, int* enc_used);
+
 /* ---- group-count estimation for hash table sizing (no counterpart in the reference, which sizes
  * tables from dictionary sizes and segment min/max: src/engine_select.cpp:1154-1167) */
 /* HyperLogLog sketch (2^p registers, p 4..12) of the GROUP BY key(s) of the rows that pass the plan's

@@ -28,6 +28,7 @@ def lib() -> C.CDLL:
         l.ws_oracle_aggregate_distinct.argtypes = [C.POINTER(abi.ExprEnv), C.POINTER(abi.AggPlan), abi.Prog, C.c_int,
                                                    C.c_int, P, P, P, C.c_int, C.c_int, C.POINTER(P)]
         l.ws_oracle_prog_is_int.argtypes = [C.POINTER(abi.ExprEnv), abi.Prog]
+        l.ws_oracle_encode_column_engine.argtypes = [P, C.c_int, C.c_int64, P, C.c_int64, C.POINTER(C.c_int64)]
         l.ws_oracle_ngroups.restype = C.c_int64
         l.ws_oracle_ngroups.argtypes = [P]
         l.ws_oracle_nkeys.argtypes = [P]
@@ -60,6 +61,17 @@ def prog_is_int(env: abi.ExprEnv, prog: abi.Prog) -> bool:
     if r < 0:
         raise ValueError("malformed expression")
     return bool(r)
+
+
+def encode_column_engine(col: np.ndarray, ptype: int):
+    """(enc, bytes) of the engine's encoding of one segment column (enc 0: kept raw, bytes empty)."""
+    col = np.ascontiguousarray(col)
+    nb = C.c_int64()
+    e = lib().ws_oracle_encode_column_engine(col.ctypes.data, ptype, col.size, None, 0, C.byref(nb))
+    out = np.zeros(max(nb.value, 1), dtype=np.uint8)
+    if e:
+        lib().ws_oracle_encode_column_engine(col.ctypes.data, ptype, col.size, out.ctypes.data, out.size, C.byref(nb))
+    return e, out[:nb.value] if e else out[:0]
 
 
 def _batches(batches: list):

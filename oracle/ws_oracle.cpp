@@ -1,3 +1,4 @@
+#include <climits>
 // CPU oracle of the Warpstore hot-path operators — TEST INFRASTRUCTURE ONLY (see ws_oracle.h).
 //
 // The expression semantics follow the reference's typed code generator (src/jit.cu:113-273), which is
@@ -838,6 +839,96 @@ int runAggregate(const ws_expr_env* env, const ws_agg_plan* plan, const ws_prog*
 }  // namespace
 
 extern "C" {
+
+// Table::encodeColumn (src/storage.cu:1093-1192) restated: the engine's encoding of one segment column
+// (ptype 0 I32, 1 I64, 2 F64).  Returns enc (0: raw) and, when cap allows, the bytes in out.
+int ws_oracle_encode_column_engine(const void* src, int ptype, int64_t n, uint8_t* out, int64_t cap, int64_t* bytes) {
+  *bytes = 0;
+  if (n < 1024) return 0;
+  std::vector<uint8_t> o;
+  int e = 0;
+  if (ptype == 0 || ptype == 1) {
+    const bool i32 = ptype == 0;
+    const long long nul = i32 ? (long long)WS_NULL_I32 : (long long)WS_NULL_I64;
+    auto at = [&](int64_t i) { return i32 ? (long long)((const int32_t*)src)[i] : (long long)((const int64_t*)src)[i]; };
+    long long mn = LLONG_MAX, mx = LLONG_MIN;
+    for (int64_t i = 0; i < n; ++i) {
+      const long long v = at(i);
+      if (v == nul) continue;
+      mn = std::min(mn, v), mx = std::max(mx, v);
+    }
+    if (mn > mx) mn = mx = 0;
+    const unsigned long long range = (unsigned long long)mx - (unsigned long long)mn;
+    e = range < 0xFFull ? 1 : range < 0xFFFFull ? 2 : (!i32 && range < 0xFFFFFFFFull) ? 3 : 0;
+    if (!e) return 0;
+    const int w = e == 1 ? 1 : e == 2 ? 2 : 4;
+    o.assign(16 + (size_t)n * w + 16, 0);
+    memcpy(o.data(), &mn, 8);
+    for (int64_t i = 0; i < n; ++i) {
+      const long long v = at(i);
+      const unsigned long long c = v == nul ? ~0ull : (unsigned long long)v - (unsigned long long)mn;
+      if (w == 1) o[16 + i] = (uint8_t)c;
+      else if (w == 2) { const uint16_t c2 = (uint16_t)c; memcpy(&o[16 + 2 * i], &c2, 2); }
+      else { const uint32_t c4 = (uint32_t)c; memcpy(&o[16 + 4 * i], &c4, 4); }
+    }
+  } else if (ptype == 2) {
+    const double* x = (const double*)src;
+    std::unordered_map<uint64_t, uint8_t> dict;
+    std::vector<double> vals;
+    bool many = false;
+    for (int64_t i = 0; i < n && !many; ++i) {
+      uint64_t b;
+      memcpy(&b, &x[i], 8);
+      if (dict.count(b)) continue;
+      if (dict.size() == 255) { many = true; break; }
+      dict.emplace(b, (uint8_t)dict.size());
+      vals.push_back(x[i]);
+    }
+    if (!many) {
+      e = 4;
+      o.assign(16 + 256 * 8 + (size_t)n + 16, 0);
+      memcpy(o.data() + 16, vals.data(), vals.size() * 8);
+      for (int64_t i = 0; i < n; ++i) {
+        uint64_t b;
+        memcpy(&b, &x[i], 8);
+        o[16 + 256 * 8 + i] = dict[b];
+      }
+    } else {
+      double p = 1.0;
+      for (int s = 0; s <= 4; ++s, p *= 10.0) {
+        long long mn = LLONG_MAX, mx = LLONG_MIN;
+        bool ok = true;
+        for (int64_t i = 0; i < n && ok; ++i) {
+          if (x[i] != x[i]) continue;
+          const double y = x[i] * p;
+          if (!(std::fabs(y) < 4e15)) { ok = false; break; }
+          const long long k = std::llround(y);
+          if ((double)k / p != x[i]) { ok = false; break; }
+          mn = std::min(mn, k), mx = std::max(mx, k);
+        }
+        if (!ok) continue;
+        if (mn > mx) mn = mx = 0;
+        const unsigned long long range = (unsigned long long)(mx - mn);
+        e = range < 0xFFFFull ? 5 : range < 0xFFFFFFFFull ? 6 : 0;
+        if (!e) return 0;
+        const int w = e == 5 ? 2 : 4;
+        o.assign(16 + (size_t)n * w + 16, 0);
+        memcpy(o.data(), &mn, 8);
+        memcpy(o.data() + 8, &p, 8);
+        for (int64_t i = 0; i < n; ++i) {
+          const unsigned long long c = x[i] != x[i] ? ~0ull : (unsigned long long)(std::llround(x[i] * p) - mn);
+          if (w == 2) { const uint16_t c2 = (uint16_t)c; memcpy(&o[16 + 2 * i], &c2, 2); }
+          else { const uint32_t c4 = (uint32_t)c; memcpy(&o[16 + 4 * i], &c4, 4); }
+        }
+        break;
+      }
+      if (!e) return 0;
+    }
+  }
+  *bytes = (int64_t)o.size();
+  if (out && cap >= (int64_t)o.size()) memcpy(out, o.data(), o.size());
+  return e;
+}
 
 // Static type of an expression (1 = int64, 0 = double), as buildTree types it; -1 when malformed.
 int ws_oracle_prog_is_int(const ws_expr_env* env, ws_prog p) {

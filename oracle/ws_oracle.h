@@ -23,6 +23,8 @@ typedef struct ws_oracle_result ws_oracle_result;
  * int64 in *ival with *is_int = 1.  *ovf is set when checked int64 arithmetic overflowed. */
 /* Static type of an expression: 1 int64, 0 double, -1 malformed. */
 int ws_oracle_prog_is_int(const ws_expr_env* env, ws_prog p);
+/* The engine's segment encoding (Table::encodeColumn): enc (0 raw) and the bytes (when cap allows). */
+int ws_oracle_encode_column_engine(const void* src, int ptype, int64_t n, uint8_t* out, int64_t cap, int64_t* bytes);
 double ws_oracle_eval(const ws_expr_env* env, const ws_col_view* cols, ws_prog prog, int64_t row, int64_t* ival,
                       int* is_int, int* ovf);
 

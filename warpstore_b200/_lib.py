@@ -59,6 +59,7 @@ SIGNATURES = {
     "ws_sort_perm_host": (C.c_int, [P, C.c_int, C.c_int64, P]),
     "ws_jit_plan_text": (C.c_int, [C.c_int, C.c_int, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     "ws_jit_last_query_plans": (C.c_int, [P, C.c_int, C.POINTER(C.c_int)]),
+    "ws_encode_column_engine": (C.c_int, [P, C.c_int, C.c_int64, C.POINTER(P), I64P, C.POINTER(C.c_int)]),
     "ws_agg_create": (C.c_int, [C.POINTER(abi.AggPlan), C.c_int64, C.POINTER(abi.DenseSpec), C.POINTER(P)]),
     "ws_agg_destroy": (None, [P]),
     "ws_agg_add_batch": (C.c_int, [P, C.POINTER(abi.ExprEnv), C.c_int, C.c_int64, P]),

@@ -452,6 +452,14 @@ def encode_column(src_ptr: int, t: int, n: int, enc: int = 0):
     return out.value, nb.value, used.value
 
 
+def encode_column_engine(src_ptr: int, ptype: int, n: int):
+    """(device ptr or None, bytes, enc) of a segment column in the engine's formats (enc 1-6, 0 = raw);
+    free the pointer with tmp_free."""
+    out, nb, used = P(), C.c_int64(), C.c_int()
+    check(lib().ws_encode_column_engine(src_ptr, ptype, n, C.byref(out), C.byref(nb), C.byref(used)))
+    return out.value, nb.value, used.value
+
+
 def map_rank(keys_ptr: int, rank_ptr: int, m: int):
     check(lib().ws_map_rank(keys_ptr, rank_ptr, m))
 
@@ -548,4 +556,4 @@ __all__ = ["DeviceBuffer", "Executor", "GpuAggregator", "WsError", "agg_nokeys_n
            "key_bitmap", "map_rank", "remap_codes", "select_multi", "set_bits", "sort_perm", "sync", "tmp_free",
            "set_vram_limit", "vram_used", "place_column", "release_column", "vram_acquire", "vram_release", "host_map",
            "host_unmap", "patch_column", "update_column", "distinct_ints", "bits_from_column", "temp_column",
-           "sort_perm_host"]
+           "sort_perm_host", "encode_column_engine"]
