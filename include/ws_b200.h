@@ -118,6 +118,13 @@ int ws_agg_add_batches(ws_aggregator* agg, int ncols, int nb, const int64_t* bn,
                        const ws_col_view* bcols);
 int ws_agg_run(ws_aggregator* agg, const ws_expr_env* env, const ws_jit_program* jit);
 int ws_agg_run_window(ws_aggregator* agg, const ws_expr_env* env, const ws_jit_program* jit);
+/* Several aggregations in ONE kernel launch (no counterpart in the reference, which launches each
+ * query on its own): aggs[i] over its batches with envs[i]'s constants, all of one scan kind (no GROUP
+ * BY, dense private rows, or hash GROUP BY) and one compiled plan `jit` (null: all interpreted, which
+ * lets queries of different expressions share the launch).  The SMs' resident CTAs are shared out by
+ * the queries' tiles; each query's results are then read as after ws_agg_run.  Aggregators without
+ * batches are skipped.  WS_ERR_ARG when the queries need different kernels. */
+int ws_agg_run_many(ws_aggregator* const* aggs, const ws_expr_env* const* envs, const ws_jit_program* jit, int n);
 int ws_agg_batches(const ws_aggregator* agg);
 int ws_agg_windows(const ws_aggregator* agg);
 int64_t ws_agg_rows_in(const ws_aggregator* agg);

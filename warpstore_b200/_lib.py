@@ -65,6 +65,7 @@ SIGNATURES = {
     "ws_agg_add_batch": (C.c_int, [P, C.POINTER(abi.ExprEnv), C.c_int, C.c_int64, P]),
     "ws_agg_add_batches": (C.c_int, [P, C.c_int, C.c_int, P, P, P]),
     "ws_agg_run": (C.c_int, [P, C.POINTER(abi.ExprEnv), P]),
+    "ws_agg_run_many": (C.c_int, [P, P, P, C.c_int]),
     "ws_agg_run_window": (C.c_int, [P, C.POINTER(abi.ExprEnv), P]),
     "ws_agg_batches": (C.c_int, [P]),
     "ws_agg_windows": (C.c_int, [P]),

@@ -441,9 +441,11 @@ namespace {
 // kernels each plan kind compiles (prefix wsq)
 const char* kindKernels(int fnKind) {
   switch (fnKind) {
-    case WS_JF_NOKEYS: return "WS_K_NOKEYS(QEv, wsq)\n";
-    case WS_JF_GROUPED: return "WS_K_HASH(QEv, wsq)\n";
-    case WS_JF_DENSE: return "WS_K_DENSE_PRIV(QEv, wsq)\nWS_K_DENSE_SHARED(QEv, wsq)\nWS_K_DENSE_GLOBAL(QEv, wsq)\n";
+    case WS_JF_NOKEYS: return "WS_K_NOKEYS(QEv, wsq)\nWS_K_MULTI_NOKEYS(QEv, wsq)\n";
+    case WS_JF_GROUPED: return "WS_K_HASH(QEv, wsq)\nWS_K_MULTI_HASH(QEv, wsq)\n";
+    case WS_JF_DENSE:
+      return "WS_K_DENSE_PRIV(QEv, wsq)\nWS_K_DENSE_SHARED(QEv, wsq)\nWS_K_DENSE_GLOBAL(QEv, wsq)\n"
+             "WS_K_MULTI_DENSE_PRIV(QEv, wsq)\n";
     default: return "WS_K_SELECT_COUNT(QEv, wsq)\nWS_K_SELECT_WRITE(QEv, wsq)\n";
   }
 }
@@ -586,7 +588,8 @@ void compileProgram(ws_jit_program& p) {
   p.fromDisk = disk;
   static const char* names[K_COUNT_] = {"wsq_nokeys", "wsq_dense_shared", "wsq_dense_global", "wsq_hash",
                                         "wsq_select_count", "wsq_select_write", "wsq_dense_priv",
-                                        "wsq_dense_priv_staged"};
+                                        "wsq_dense_priv_staged", "wsq_multi_nokeys", "wsq_multi_dense_priv",
+                                        "wsq_multi_hash"};
   for (int k = 0; k < K_COUNT_; ++k) {
     CUfunction f = nullptr;
     if (drv().moduleGetFunction(&f, p.module, names[k]) == CUDA_SUCCESS) p.kernels.fn[k] = f;

@@ -638,6 +638,9 @@ struct Launch {
   int sumShift;               // integer SUM words need no overflow test while (argument magnitude >> sumShift)
                               // is 0 (set at launch from the rows a thread adds; -1: always test)
   int waitLog2;               // staged scans: a wait for a tile stage gives up after 2^waitLog2 SM cycles
+  // A launch serving several queries gives each its own range of CTAs: this query's first CTA and its
+  // CTA count (0: the whole grid).  Bodies use ctaIndex / ctaCount, never blockIdx / gridDim.
+  int ctaBase, ctaGrid;
   // aggregation outputs
   u64* part;                  // per-CTA partial rows
   u64* rows;                  // result rows
@@ -658,6 +661,17 @@ struct Launch {
   // selection
   i64* tileCount;             // [ntiles] selected rows per tile (count pass) / exclusive offsets (write pass)
   int32_t* outIdx;
+};
+
+WS_DI unsigned ctaIndex(const Launch& L) { return blockIdx.x - (unsigned)L.ctaBase; }
+WS_DI unsigned ctaCount(const Launch& L) { return L.ctaGrid ? (unsigned)L.ctaGrid : gridDim.x; }
+
+// One launch of a scan kernel over several queries of the same compiled plan: query q's launch
+// descriptor q[q] and CTAs [ctaStart[q], ctaStart[q + 1]).
+struct MultiLaunch {
+  const Launch* q;
+  const int* ctaStart;  // [nq + 1]
+  int nq;
 };
 
 }  // namespace ws

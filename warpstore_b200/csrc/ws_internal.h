@@ -146,7 +146,7 @@ EnvK envK(const ws_expr_env& env);
 // K_DENSE_PRIV_STAGED: the same body with a producer warp staging tiles by TMA (kStagedThreads).
 enum KernelId {
   K_NOKEYS = 0, K_DENSE_SHARED, K_DENSE_GLOBAL, K_HASH, K_SELECT_COUNT, K_SELECT_WRITE, K_DENSE_PRIV,
-  K_DENSE_PRIV_STAGED, K_COUNT_
+  K_DENSE_PRIV_STAGED, K_MULTI_NOKEYS, K_MULTI_DENSE_PRIV, K_MULTI_HASH, K_COUNT_
 };
 struct KernelSet {
   CUfunction fn[K_COUNT_] = {};

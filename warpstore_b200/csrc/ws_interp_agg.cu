@@ -6,11 +6,13 @@
 WS_K_NOKEYS(ws::InterpEv, wsi)
 WS_K_DENSE_SHARED(ws::InterpEv, wsi)
 WS_K_DENSE_GLOBAL(ws::InterpEv, wsi)
+WS_K_MULTI_NOKEYS(ws::InterpEv, wsi)
 
 namespace ws {
 void interpSyms_agg(const void** s) {
   s[K_NOKEYS] = (const void*)wsi_nokeys;
   s[K_DENSE_SHARED] = (const void*)wsi_dense_shared;
   s[K_DENSE_GLOBAL] = (const void*)wsi_dense_global;
+  s[K_MULTI_NOKEYS] = (const void*)wsi_multi_nokeys;
 }
 }  // namespace ws

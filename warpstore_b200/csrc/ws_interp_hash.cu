@@ -4,9 +4,11 @@
 #include "ws_interp.cuh"
 
 WS_K_HASH(ws::InterpEv, wsi)
+WS_K_MULTI_HASH(ws::InterpEv, wsi)
 
 namespace ws {
 void interpSyms_hash(const void** s) {
   s[K_HASH] = (const void*)wsi_hash;
+  s[K_MULTI_HASH] = (const void*)wsi_multi_hash;
 }
 }  // namespace ws

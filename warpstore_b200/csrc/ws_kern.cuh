@@ -58,16 +58,16 @@ WS_DI int batchOfTile(const Launch& L, i64 t) {
 }
 
 // Walks the tiles this CTA owns: the contiguous range [T c / G, T (c + 1) / G) of the launch's T tiles
-// (c = blockIdx.x, G = gridDim.x), batch by batch.  A CTA crosses one or two batches, so the batch's
+// (c = ctaIndex, G = ctaCount), batch by batch.  A CTA crosses one or two batches, so the batch's
 // size, bitmap and column views (and an encoded column's header) are read once or twice per CTA
 // rather than once per batch of the launch.  tile(t, b, r0, n, del) is called by every thread of the
 // CTA for each tile t of batch b (r0 = the thread's first row in the batch, n = the batch's rows,
 // del = its deleted bitmap); it returns true to end the walk (the same value in every thread).
 template <class Ev, class F>
 WS_DI void forEachOwnedTile(const Launch& L, Ev& ev, F&& tile) {
-  const i64 T = L.ntiles, G = gridDim.x;
-  i64 t = T * (i64)blockIdx.x / G;
-  const i64 tEnd = T * ((i64)blockIdx.x + 1) / G;
+  const i64 T = L.ntiles, G = ctaCount(L), c = ctaIndex(L);
+  i64 t = T * c / G;
+  const i64 tEnd = T * (c + 1) / G;
   if (t >= tEnd) return;
   for (int b = batchOfTile(L, t); t < tEnd && b < L.nb; ++b) {
     const i64 bs = __ldg(L.tileStart + b), bend = __ldg(L.tileStart + b + 1), be = bend < tEnd ? bend : tEnd;
@@ -144,8 +144,8 @@ WS_DI void forEachRowStaged(const Launch& L, Ev& ev, unsigned char* stages, int 
   }
   __syncthreads();
   // this CTA's tiles: the contiguous range [tFirst, tFirst + K) (as forEachOwnedTile)
-  const i64 tFirst = L.ntiles * (i64)blockIdx.x / gridDim.x;
-  const i64 K = L.ntiles * ((i64)blockIdx.x + 1) / gridDim.x - tFirst;
+  const i64 tFirst = L.ntiles * (i64)ctaIndex(L) / ctaCount(L);
+  const i64 K = L.ntiles * ((i64)ctaIndex(L) + 1) / ctaCount(L) - tFirst;
   if (warp == kConsumerWarps) {  // ---- producer warp (one elected lane)
     if (lane == 0) {
       int pb = K > 0 ? batchOfTile(L, tFirst) : 0, pbatch = -1;
@@ -496,7 +496,7 @@ WS_DI void lastCtaReduce(const Launch& L, const Ev& ev, int nrows, u64* sred) {
   __shared__ bool amLast;
   __threadfence();
   __syncthreads();
-  if (threadIdx.x == 0) amLast = atomicAdd(L.ticket, 1u) == gridDim.x - 1;
+  if (threadIdx.x == 0) amLast = atomicAdd(L.ticket, 1u) == ctaCount(L) - 1;
   __syncthreads();
   if (!amLast) return;
   __threadfence();
@@ -504,7 +504,7 @@ WS_DI void lastCtaReduce(const Launch& L, const Ev& ev, int nrows, u64* sred) {
   for (int g = 0; g < nrows; ++g) {
     u64 w[RW];
     rowIdentity(ev, w);
-    for (unsigned c = threadIdx.x; c < gridDim.x; c += blockDim.x) {
+    for (unsigned c = threadIdx.x; c < ctaCount(L); c += blockDim.x) {
       const u64* p = L.part + ((size_t)c * nrows + g) * rw;
       u64 x[RW];
 #pragma unroll
@@ -552,7 +552,7 @@ __device__ void aggNoKeys(const Launch& L) {
   if (threadIdx.x == 0) {
     for (int a = 0; a < ev.na(); ++a)
       if (ev.kind(a) == SK_ISUM) add128w(w[ev.woff(a)], *(i64*)&w[ev.woff(a) + 1], spill[2 * a], (i64)spill[2 * a + 1]);
-    for (int j = 1; j < rw; ++j) L.part[(size_t)blockIdx.x * rw + j] = w[j];
+    for (int j = 1; j < rw; ++j) L.part[(size_t)ctaIndex(L) * rw + j] = w[j];
   }
   lastCtaReduce<Ev, RW>(L, ev, 1, sred);
 }
@@ -662,7 +662,7 @@ __device__ void aggDensePriv(const Launch& L) {
       const u64* sp = spill + (size_t)g * 2 * Ev::NA;
       for (int a = 0; a < ev.na(); ++a)
         if (ev.kind(a) == SK_ISUM) add128w(w[ev.woff(a)], *(i64*)&w[ev.woff(a) + 1], sp[2 * a], (i64)sp[2 * a + 1]);
-      for (int j = 1; j < rw; ++j) L.part[((size_t)blockIdx.x * G + g) * rw + j] = w[j];
+      for (int j = 1; j < rw; ++j) L.part[((size_t)ctaIndex(L) * G + g) * rw + j] = w[j];
     }
   }
   lastCtaReduce<Ev, RW>(L, ev, G, sred);
@@ -963,6 +963,28 @@ __device__ void selectWrite(const Launch& L) {
     BODY(L);                                                                                                 \
   }
 #define WS_K_ENTRY(PREFIX, NAME, BODY) WS_K_ENTRY_B(PREFIX, NAME, BODY, ws::kStagedThreads, 1)
+// The same body serving several queries in one launch: each CTA finds its query (binary search of the
+// CTA ranges) and runs the body on a shared-memory copy of that query's descriptor with its CTA range.
+#define WS_K_MULTI_B(PREFIX, NAME, BODY, THREADS, MINB)                                                       \
+  extern "C" __global__ void __launch_bounds__(THREADS, MINB) PREFIX##_multi_##NAME(const __grid_constant__ ws::MultiLaunch M) { \
+    __shared__ __align__(16) ws::Launch Lq;                                                                 \
+    int lo = 0, hi = M.nq - 1;                                                                               \
+    while (lo < hi) {                                                                                        \
+      const int mid = (lo + hi + 1) >> 1;                                                                    \
+      if (M.ctaStart[mid] <= (int)blockIdx.x) lo = mid;                                                      \
+      else hi = mid - 1;                                                                                     \
+    }                                                                                                        \
+    const unsigned long long* src = (const unsigned long long*)(M.q + lo);                                  \
+    for (int w = threadIdx.x; w < (int)(sizeof(ws::Launch) / 8); w += blockDim.x) ((unsigned long long*)&Lq)[w] = src[w]; \
+    __syncthreads();                                                                                         \
+    if (threadIdx.x == 0) Lq.ctaBase = M.ctaStart[lo], Lq.ctaGrid = M.ctaStart[lo + 1] - M.ctaStart[lo];    \
+    __syncthreads();                                                                                         \
+    BODY(Lq);                                                                                                \
+  }
+#define WS_K_MULTI_NOKEYS(EV, PREFIX) WS_K_MULTI_B(PREFIX, nokeys, ws::aggNoKeys<EV>, ws::kStagedThreads, 1)
+#define WS_K_MULTI_DENSE_PRIV(EV, PREFIX) \
+  WS_K_MULTI_B(PREFIX, dense_priv, (ws::aggDensePriv<EV, false>), ws::kThreads, EV::PRIV_MIN_BLOCKS)
+#define WS_K_MULTI_HASH(EV, PREFIX) WS_K_MULTI_B(PREFIX, hash, ws::aggHash<EV>, ws::kStagedThreads, 1)
 #define WS_K_NOKEYS(EV, PREFIX) WS_K_ENTRY(PREFIX, nokeys, ws::aggNoKeys<EV>)
 #define WS_K_DENSE_SHARED(EV, PREFIX) WS_K_ENTRY(PREFIX, dense_shared, ws::aggDenseShared<EV>)
 #define WS_K_DENSE_GLOBAL(EV, PREFIX) WS_K_ENTRY(PREFIX, dense_global, ws::aggDenseGlobal<EV>)

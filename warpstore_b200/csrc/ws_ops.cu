@@ -879,6 +879,71 @@ int ws_agg_run(ws_aggregator* A, const ws_expr_env* env, const ws_jit_program* j
   return guardedCall([&] { aggRun(*A, *env, jit); });
 }
 
+int ws_agg_run_many(ws_aggregator* const* aggs, const ws_expr_env* const* envs, const ws_jit_program* jit, int n) {
+  return guardedCall([&] {
+    if (n < 1 || n > 1024 || !aggs || !envs) throw Error("ws_agg_run_many: 1..1024 aggregators", WS_ERR_ARG);
+    // each query prepared as for its own launch (descriptor uploaded, kernel and shape chosen)
+    std::vector<PreparedScan> preps((size_t)n);
+    for (int i = 0; i < n; ++i) aggRun(*aggs[i], *envs[i], jit, &preps[(size_t)i]);
+    const KernelSet* ks = nullptr;
+    int multi = -1;
+    size_t smem = 0;
+    int threads = 0;
+    int64_t tiles = 0;
+    std::vector<int> live;
+    for (int i = 0; i < n; ++i) {
+      const PreparedScan& p = preps[(size_t)i];
+      if (!p.ready) continue;  // no tiles: nothing to scan
+      const KernelSet& k = p.compiled ? jit->kernels : interpKernels();
+      const int m = p.f == k.fn[K_NOKEYS] ? K_MULTI_NOKEYS : p.f == k.fn[K_DENSE_PRIV] ? K_MULTI_DENSE_PRIV
+                  : p.f == k.fn[K_HASH] ? K_MULTI_HASH : -1;
+      if (m < 0 || !k.fn[m])
+        throw Error("ws_agg_run_many: a query's scan has no multi-query form (dense shared / global rows, staged tiles)",
+                    WS_ERR_ARG);
+      if (multi >= 0 && (m != multi || &k != ks))
+        throw Error("ws_agg_run_many: the queries need one scan kind and one plan (or all interpreted)", WS_ERR_ARG);
+      ks = &k, multi = m;
+      smem = std::max(smem, p.smem);
+      threads = p.threads;
+      tiles += p.L.ntiles;
+      live.push_back(i);
+    }
+    if (live.empty()) return;
+    CUfunction f = ks->fn[multi];
+    // the launch's resident CTAs, shared out by the queries' tiles (each at least one CTA, at most its
+    // own persistent grid, which its partial rows were sized for)
+    const unsigned total = persistentGrid(f, smem, std::max<int64_t>(tiles, (int64_t)live.size()), threads);
+    std::vector<int> start(live.size() + 1, 0);
+    for (size_t j = 0; j < live.size(); ++j) {
+      const PreparedScan& p = preps[(size_t)live[j]];
+      int64_t share = (int64_t)((double)total * (double)p.L.ntiles / (double)tiles);
+      share = std::max<int64_t>(1, std::min<int64_t>(share, std::min<int64_t>(p.grid, p.L.ntiles)));
+      start[j + 1] = start[j] + (int)share;
+    }
+    const size_t nl = live.size();
+    const size_t launchBytes = nl * sizeof(Launch), startBytes = (nl + 1) * sizeof(int);
+    uint8_t* st = pinnedStage(launchBytes + startBytes);
+    for (size_t j = 0; j < nl; ++j) {
+      Launch L = preps[(size_t)live[j]].L;
+      L.sumShift = sumShiftFor(L.ntiles, (unsigned)(start[j + 1] - start[j]));
+      L.waitLog2 = stagedWaitLog2();
+      L.ctaBase = L.ctaGrid = 0;  // set per CTA by the kernel
+      memcpy(st + j * sizeof(Launch), &L, sizeof(Launch));
+      if (L.ticket) WS_CK(cudaMemsetAsync(L.ticket, 0, 4, stream()));
+    }
+    memcpy(st + launchBytes, start.data(), startBytes);
+    DBuf<uint8_t> dl((int64_t)(launchBytes + startBytes));
+    h2dAsync(dl.p, st, launchBytes + startBytes);
+    stageCopied();
+    MultiLaunch M{(const Launch*)dl.p, (const int*)(dl.p + launchBytes), (int)nl};
+    if (smem > 0) WS_CKD(drv().funcSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)smem));
+    void* args[] = {(void*)&M};
+    WS_CKD(drv().launchKernel(f, (unsigned)start[nl], 1, 1, (unsigned)threads, 1, 1, (unsigned)smem, (CUstream)stream(),
+                              args, nullptr));
+    countLaunch();
+  });
+}
+
 int ws_agg_run_window(ws_aggregator* A, const ws_expr_env* env, const ws_jit_program* jit) {
   return guardedCall([&] {
     if (A->bn.empty()) return;

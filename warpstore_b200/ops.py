@@ -318,6 +318,14 @@ class GpuAggregator:
         return k.value, a.value, g.value
 
 
+def agg_run_many(aggs: list, envs: list, jit: int | None = None):
+    """One launch aggregating every aggregator over its batches (ws_agg_run_many)."""
+    n = len(aggs)
+    ha = (P * n)(*[a.h for a in aggs])
+    he = (P * n)(*[C.addressof(e) for e in envs])
+    check(lib().ws_agg_run_many(ha, he, jit, n))
+
+
 def agg_nokeys_noalloc(env: abi.ExprEnv, ncols: int, plan: abi.AggPlan, batches: list, jit: int | None = None):
     """Filter + aggregate without GROUP BY through ws_agg_nokeys_noalloc (no memory is allocated: the
     library's fixed scratch array is used).  batches: [(n, deleted_ptr, [ColView])].  Returns the exact
@@ -556,4 +564,4 @@ __all__ = ["DeviceBuffer", "Executor", "GpuAggregator", "WsError", "agg_nokeys_n
            "key_bitmap", "map_rank", "remap_codes", "select_multi", "set_bits", "sort_perm", "sync", "tmp_free",
            "set_vram_limit", "vram_used", "place_column", "release_column", "vram_acquire", "vram_release", "host_map",
            "host_unmap", "patch_column", "update_column", "distinct_ints", "bits_from_column", "temp_column",
-           "sort_perm_host", "encode_column_engine"]
+           "sort_perm_host", "encode_column_engine", "agg_run_many"]
