@@ -353,6 +353,9 @@ typedef struct ws_serve_options {
   int one_sync;                     /* the one-sync form (see above) */
   int64_t arena_bytes;              /* per worker, for queries without result arrays (0: none) */
   int checksum;                     /* digest every delivered group (checksum, fsum) */
+  int batch;                        /* up to this many arrived queries of one plan share a launch
+                                       (ws_agg_run_many) before their groups are delivered one by one;
+                                       0 or 1: a launch per query */
 } ws_serve_options;
 int ws_serve(ws_serve_query* queries, int n, const ws_serve_options* opt, double* wall_s);
 

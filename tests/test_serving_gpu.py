@@ -60,6 +60,18 @@ def test_results_alone_equal_results_in_the_mix():
                 assert abs(r.fsum - f) <= 1e-9 * max(abs(f), 1e-300)
             print(f"\n[serving] native loop, {mode}, results to per-worker buffers: {st.qps:.0f} QPS, "
                   f"p50 {st.p50_ms:.2f} ms, p99 {st.p99_ms:.2f} ms")
+        # arrived queries of one plan sharing a scan launch (ws_agg_run_many): compiled plans (queries of
+        # the same shape only) and interpreted ones (any queries of the hash kind), all arriving at once
+        import dataclasses
+        burst = [dataclasses.replace(p, qr=dataclasses.replace(p.qr, arrival=0.0)) for p in prepared]
+        interp = [dataclasses.replace(p, prog=None) for p in burst]
+        for name, prep in (("compiled", burst), ("interpreted", interp)):
+            st = S.run_native(tables, prep, arrays, "batched", result_rows=rows, batch=8)
+            assert st.completed == len(queries)
+            for p in prep:
+                r = st.results[p.qr.qid]
+                same(*alone[p.qr.qid], r.keys, r.exact)
+            print(f"\n[serving] native loop, batched, {name} plans, up to 8 queries per launch: {st.qps:.0f} QPS")
     finally:
         ops.jit_set_mode(-1)
         for t in tables:

@@ -101,7 +101,7 @@ class ServeQuery(C.Structure):
 class ServeOptions(C.Structure):
     """ws_serve_options (include/ws_b200.h)."""
     _fields_ = [("slots", C.c_int), ("hbm_budget", C.c_int64), ("est", C.c_void_p), ("one_sync", C.c_int),
-                ("arena_bytes", C.c_int64), ("checksum", C.c_int)]
+                ("arena_bytes", C.c_int64), ("checksum", C.c_int), ("batch", C.c_int)]
 
 
 class FetchStatus(C.Structure):

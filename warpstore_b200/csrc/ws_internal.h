@@ -45,6 +45,7 @@ struct DriverApi {
   CUresult (*occupancy)(int*, CUfunction, int, size_t);
   CUresult (*getErrorString)(CUresult, const char**);
   CUresult (*graphExecKernelNodeSetParams)(CUgraphExec, CUgraphNode, const CUDA_KERNEL_NODE_PARAMS*);
+  CUresult (*funcGetAttribute)(int*, CUfunction_attribute, CUfunction);
 };
 const DriverApi& drv();
 void ensureInit();
@@ -153,6 +154,8 @@ struct KernelSet {
   bool interp = true;
 };
 const KernelSet& interpKernels();
+// Raises f's dynamic shared memory allowance to smem (never lowers it; safe across threads).
+void allowDynamicSmem(CUfunction f, size_t smem);
 // Launch.sumShift of a scan of ntiles tiles on `grid` CTAs (the integer SUM bound of ws_kern.cuh).
 int sumShiftFor(int64_t ntiles, unsigned grid);
 // Launch.waitLog2: the staged scans' wait limit (WARPSTORE_B200_WAIT_LIMIT_LOG2, default 32).

@@ -936,7 +936,7 @@ int ws_agg_run_many(ws_aggregator* const* aggs, const ws_expr_env* const* envs, 
     h2dAsync(dl.p, st, launchBytes + startBytes);
     stageCopied();
     MultiLaunch M{(const Launch*)dl.p, (const int*)(dl.p + launchBytes), (int)nl};
-    if (smem > 0) WS_CKD(drv().funcSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)smem));
+    allowDynamicSmem(f, smem);
     void* args[] = {(void*)&M};
     WS_CKD(drv().launchKernel(f, (unsigned)start[nl], 1, 1, (unsigned)threads, 1, 1, (unsigned)smem, (CUstream)stream(),
                               args, nullptr));
@@ -1173,8 +1173,7 @@ int ws_exec_create(const ws_agg_plan* plan, int64_t capacity, const ws_dense_spe
       X->kernels = 1;
       if (X->ps.ready) {
         const PreparedScan& p = X->ps;
-        if (p.smem > 0)
-          WS_CKD(drv().funcSetAttribute(p.f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)p.smem));
+        allowDynamicSmem(p.f, p.smem);
         void* args[] = {(void*)&X->ps.L};
         WS_CKD(drv().launchKernel(p.f, p.grid, 1, 1, (unsigned)p.threads, 1, 1, (unsigned)p.smem, (CUstream)cs, args,
                                   nullptr));

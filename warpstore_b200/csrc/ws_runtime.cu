@@ -77,6 +77,7 @@ const DriverApi& drv() {
     get("cuOccupancyMaxActiveBlocksPerMultiprocessor", (void**)&a.occupancy);
     get("cuGetErrorString", (void**)&a.getErrorString);
     get("cuGraphExecKernelNodeSetParams", (void**)&a.graphExecKernelNodeSetParams);
+    get("cuFuncGetAttribute", (void**)&a.funcGetAttribute);
     return a;
   }();
   return api;
@@ -270,8 +271,21 @@ int sumShiftFor(int64_t ntiles, unsigned grid) {
   return k <= 31 ? 31 - k : -1;
 }
 
+void allowDynamicSmem(CUfunction f, size_t smem) {
+  // The attribute is per function and shared by every thread that launches it: it only ever grows
+  // (under a lock), so that a thread asking for less never lowers it below another thread's launch.
+  if (!smem) return;
+  static std::mutex mu;
+  static std::map<CUfunction, size_t> allowed;
+  std::lock_guard<std::mutex> g(mu);
+  size_t& cur = allowed[f];
+  if (smem <= cur) return;
+  WS_CKD(drv().funcSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)smem));
+  cur = smem;
+}
+
 void launchScan(CUfunction f, unsigned grid, size_t smem, const Launch& Lin, int threads) {
-  if (smem > 0) WS_CKD(drv().funcSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)smem));
+  allowDynamicSmem(f, smem);
   Launch L = Lin;
   L.sumShift = sumShiftFor(L.ntiles, grid);
   L.waitLog2 = stagedWaitLog2();
@@ -281,10 +295,21 @@ void launchScan(CUfunction f, unsigned grid, size_t smem, const Launch& Lin, int
 }
 
 unsigned persistentGrid(CUfunction f, size_t smem, int64_t ntiles, int threads) {
-  if (smem > 0) WS_CKD(drv().funcSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)smem));
+  allowDynamicSmem(f, smem);
   int per = 0;
   WS_CKD(drv().occupancy(&per, f, threads, smem));
-  if (per < 1) throw Error("scan kernel does not fit on an SM (shared memory " + std::to_string(smem) + " B)", WS_ERR_INTERNAL);
+  if (per < 1) {
+    int regs = 0, stat = 0, local = 0, maxThreads = 0;
+    drv().funcGetAttribute(&regs, CU_FUNC_ATTRIBUTE_NUM_REGS, f);
+    drv().funcGetAttribute(&stat, CU_FUNC_ATTRIBUTE_SHARED_SIZE_BYTES, f);
+    drv().funcGetAttribute(&local, CU_FUNC_ATTRIBUTE_LOCAL_SIZE_BYTES, f);
+    drv().funcGetAttribute(&maxThreads, CU_FUNC_ATTRIBUTE_MAX_THREADS_PER_BLOCK, f);
+    throw Error("scan kernel does not fit on an SM (" + std::to_string(threads) + " threads, dynamic shared memory " +
+                    std::to_string(smem) + " B, static " + std::to_string(stat) + " B, " + std::to_string(regs) +
+                    " registers, local " + std::to_string(local) + " B, at most " + std::to_string(maxThreads) +
+                    " threads)",
+                WS_ERR_INTERNAL);
+  }
   int64_t g = (int64_t)per * smCount();
   if (g > ntiles) g = ntiles;
   return (unsigned)(g < 1 ? 1 : g);

@@ -132,7 +132,8 @@ void growTo(std::vector<uint8_t>& v, size_t bytes) {
 //    memory are queued back to back and the thread waits once per run (per range for results larger
 //    than the arena);
 //  otherwise the engine's sequence: overflow check, group count, compaction, copies, each a wait.
-void serveOne(ws_serve_query& q, const ws_serve_options& o, ws_fetch_status* st, Arena& ar) {
+// The query's first hash table capacity: the plain rule's, or for a large table the learned estimate.
+int64_t initialCap(const ws_serve_query& q, const ws_serve_options& o) {
   const ws_estimator_weights* w = o.est;
   int64_t cap = q.cap_plain;
   if (w && cap > (1 << 16)) {
@@ -148,6 +149,13 @@ void serveOne(ws_serve_query& q, const ws_serve_options& o, ws_fetch_status* st,
     const double pred = std::exp2((double)x[8] + (double)y) - 1;
     cap = std::min(cap, pow2AtLeast(2 * pred * w->margin, 1024));
   }
+  return cap;
+}
+
+// pre: an aggregator of capacity cap already run for this query (rc: its run's status), as a launch
+// shared with other queries leaves it; null: the query's first run happens here.
+void serveOne(ws_serve_query& q, const ws_serve_options& o, ws_fetch_status* st, Arena& ar, int64_t cap,
+              ws_aggregator* pre = nullptr, int preRc = 0) {
   const int nk = q.plan->nkeys, na = q.plan->naggs;
   const int64_t rowBytes = 8 * (nk + 2 * na);
   const bool arena = !q.keys && !q.accs && !q.exact && o.arena_bytes > 0;
@@ -156,10 +164,15 @@ void serveOne(ws_serve_query& q, const ws_serve_options& o, ws_fetch_status* st,
   q.fsum = 0;
   for (;;) {
     ++q.runs;
-    ws_aggregator* a = nullptr;
-    checkRc(ws_agg_create(q.plan, cap, nullptr, &a));
-    int rc = ws_agg_add_batches(a, q.ncols, q.nb, q.bn, q.bdel, q.bcols);
-    if (!rc) rc = ws_agg_run(a, q.env, q.jit);
+    ws_aggregator* a = pre;
+    int rc = preRc;
+    if (pre) {
+      pre = nullptr;
+    } else {
+      checkRc(ws_agg_create(q.plan, cap, nullptr, &a));
+      rc = ws_agg_add_batches(a, q.ncols, q.nb, q.bn, q.bdel, q.bcols);
+      if (!rc) rc = ws_agg_run(a, q.env, q.jit);
+    }
     if (st) {
       // destination: the caller's arrays, or the arena range by range
       const int64_t per = arena ? std::max<int64_t>(1, ar.bytes / rowBytes) : q.max_groups;
@@ -280,21 +293,69 @@ int ws_serve(ws_serve_query* queries, int n, const ws_serve_options* opt, double
           inFlight += q.footprint;
         }
         q.start_s = nowS() - t0;
+        // batch: the queries after this one that have arrived, use the same plan (one compiled program,
+        // or all interpreted) and fit the budget join its launch (ws_agg_run_many)
+        std::vector<int> grp{i};
+        while (o.batch > 1 && (int)grp.size() < o.batch && !failed) {
+          int j = next.load();
+          if (j >= n) break;
+          ws_serve_query& c = queries[j];
+          if (c.arrival_s > nowS() - t0 || c.jit != q.jit || (c.plan->nkeys == 0) != (q.plan->nkeys == 0)) break;
+          std::lock_guard<std::mutex> l(mu);
+          if (inFlight + c.footprint > o.hbm_budget) break;
+          if (!next.compare_exchange_strong(j, j + 1)) continue;
+          inFlight += c.footprint;
+          c.start_s = nowS() - t0;
+          grp.push_back(j);
+        }
+        auto oneSyncFor = [&](const ws_serve_query& x) {
+          const bool arrays = x.keys || x.accs || x.exact;
+          return o.one_sync && (arrays ? (x.keys || !x.plan->nkeys) && x.exact && !x.accs && pinnedHost(x.exact) &&
+                                             (!x.keys || pinnedHost(x.keys))
+                                       : o.arena_bytes > 0);
+        };
+        std::vector<ws_aggregator*> pre(grp.size(), nullptr);
+        std::vector<int64_t> caps(grp.size(), 0);
+        int preRc = 0;
         try {
-          const bool arrays = q.keys || q.accs || q.exact;
-          const bool oneSync = o.one_sync && (arrays ? (q.keys || !q.plan->nkeys) && q.exact && !q.accs &&
-                                                           pinnedHost(q.exact) && (!q.keys || pinnedHost(q.keys))
-                                                     : o.arena_bytes > 0);
-          serveOne(q, o, oneSync ? stat[k] : nullptr, arenas[k]);
+          if (grp.size() > 1) {  // the first runs of the group in one launch
+            std::vector<const ws_expr_env*> envs;
+            for (size_t g = 0; g < grp.size(); ++g) {
+              ws_serve_query& x = queries[grp[g]];
+              caps[g] = initialCap(x, o);
+              checkRc(ws_agg_create(x.plan, caps[g], nullptr, &pre[g]));
+              checkRc(ws_agg_add_batches(pre[g], x.ncols, x.nb, x.bn, x.bdel, x.bcols));
+              envs.push_back(x.env);
+            }
+            preRc = ws_agg_run_many(pre.data(), envs.data(), q.jit, (int)grp.size());
+          } else {
+            caps[0] = initialCap(q, o);
+          }
         } catch (const ws::Error& e) {
           fail(e.what(), e.code);
+          for (auto& a : pre)
+            if (a) ws_agg_destroy(a), a = nullptr;
         }
-        q.finish_s = nowS() - t0;
-        {
-          std::lock_guard<std::mutex> l(mu);
-          inFlight -= q.footprint;
+        for (size_t g = 0; g < grp.size(); ++g) {
+          ws_serve_query& x = queries[grp[g]];
+          ws_aggregator* mine = pre[g];  // serveOne takes it over (and destroys it on every path)
+          pre[g] = nullptr;
+          try {
+            if (failed) {
+              if (mine) ws_agg_destroy(mine);
+            } else {
+              serveOne(x, o, oneSyncFor(x) ? stat[k] : nullptr, arenas[k], caps[g], mine, preRc);
+            }
+          } catch (const ws::Error& e) {
+            fail(e.what(), e.code);
+          }
+          x.finish_s = nowS() - t0;
+          {
+            std::lock_guard<std::mutex> l(mu);
+            inFlight -= x.footprint;
+          }
+          cv.notify_all();
         }
-        cv.notify_all();
       }
       ws_set_stream(nullptr);
     };

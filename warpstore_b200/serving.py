@@ -281,7 +281,7 @@ def run_alone(p: Prepared, arrays: list, learned: bool):
 
 def run_native(tables: list, prepared: list, arrays: list, mode: str = "batched", slots: int | None = None,
                hbm_budget: int = 8 << 30, keep_results: bool = True, result_rows: dict | None = None,
-               pinned: bool | None = None, arena_bytes: int = 0, checksum: bool = False) -> Stats:
+               pinned: bool | None = None, arena_bytes: int = 0, checksum: bool = False, batch: int = 0) -> Stats:
     """The same serving loop in the library (ws_serve): C++ worker threads with a CUDA stream each,
     no Python on the per-query path; the prepared queries' arrival times are honoured.
 
@@ -289,6 +289,7 @@ def run_native(tables: list, prepared: list, arrays: list, mode: str = "batched"
     rows each when given, else the key ranges' bound.  Otherwise, with arena_bytes, every worker
     receives its queries' groups in a buffer of its own (reused query after query, as a server's send
     buffer; checksum: each query's groups are digested as they arrive), else they stay on the device.
+    batch > 1: arrived queries of one plan share a scan launch, up to `batch` at a time.
     pinned (default: the batched form) selects the one-sync form: result arrays / arenas are pinned
     host memory and the GPU writes the groups into them; plain: pageable memory and the engine's fetch
     sequence."""
@@ -333,7 +334,7 @@ def run_native(tables: list, prepared: list, arrays: list, mode: str = "batched"
                                  hold[6].ctypes.data, 2.0 ** float(m.meta.get("val_p90_log2_err", 0.0)))
     wall = C.c_double()
     opt = abi.ServeOptions(nslots, hbm_budget, C.addressof(w) if w else None, int(bool(pinned)),
-                           0 if keep_results else int(arena_bytes), int(bool(checksum)))
+                           0 if keep_results else int(arena_bytes), int(bool(checksum)), int(batch))
     ops.check(ops.lib().ws_serve(qs, len(prepared), C.byref(opt), C.byref(wall)))
     lat = np.array([(q.finish_s - q.arrival_s) * 1e3 for q in qs])
     span = max(q.finish_s for q in qs) - min(q.arrival_s for q in qs)
