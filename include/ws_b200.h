@@ -213,6 +213,11 @@ int ws_hash_join_parts(ws_col_view build_key, const int64_t* boff, int nbparts, 
                        int64_t* m);
 int ws_hash_join(ws_col_view build_key, int64_t nb, ws_col_view probe_key, int64_t np, int32_t** out_build,
                  int32_t** out_probe, int64_t* m);
+/* ws_hash_join with the pair buffers' first capacity chosen by the caller (a predicted pair count, for
+ * instance) instead of the probe rows: a join that emits more pairs runs a second time with exact sizes,
+ * so only the memory held and *attempts (1 or 2) depend on it, never the pairs. */
+int ws_hash_join_sized(ws_col_view build_key, int64_t nb, ws_col_view probe_key, int64_t np, int64_t first_capacity,
+                       int32_t** out_build, int32_t** out_probe, int64_t* m, int* attempts);
 /* gpuHashJoinOuter (src/gpu.h:187-188): every probe row appears, with build row -1 when it matched
  * nothing (NULL keys never match); full != 0 also appends each build row that matched nothing, with
  * probe row -1.  Pairs are freed with ws_tmp_free. */
@@ -269,7 +274,8 @@ int ws_encode_column_engine(const void* src, int ptype, int64_t n, void** out, i
  * filter, over the global rows k * stride of the batches (stride = max(1, rows / sample_rows)):
  * register j = max over sampled hashes h = mix64(key bits) with top p bits j of (leading zeros of
  * h << p) + 1.  regs_out: host array of 2^p words; *sampled / *passing: sampled rows (not deleted) and
- * those that pass the filter. */
+ * those that pass the filter.  A plan without keys only counts (the registers stay 0): the sampled
+ * selectivity of its filter. */
 int ws_hll_sketch(const ws_expr_env* env, int ncols, const ws_agg_plan* plan, int nb, const int64_t* bn,
                   const uint32_t* const* bdel, const ws_col_view* bcols, int p, int64_t sample_rows, uint32_t* regs_out,
                   int64_t* sampled, int64_t* passing);
@@ -332,8 +338,9 @@ typedef struct ws_serve_query {
                                        exact words (DOUBLE SUM slots excluded) -- order-independent */
   double fsum;                      /* with `checksum`: the sum of the DOUBLE SUM slots over the groups */
 } ws_serve_query;
-/* Learned sizing (est may be null for the plain rule): the estimator's MLP (9 features, `hidden`
- * units, BF16 weight bits), its input normalisation and the capacity margin (2^(p90 log2 error)). */
+/* Learned sizing (est may be null for the plain rule): the estimator's group-count MLP (9 features,
+ * `hidden` units, BF16 weight bits), its input normalisation, the capacity margin (2^(p90 of the log2
+ * underestimates)) and the gate of its correction. */
 typedef struct ws_estimator_weights {
   int hidden;
   const uint16_t* w1;
@@ -345,6 +352,7 @@ typedef struct ws_estimator_weights {
   const float* mean;
   const float* std;
   double margin;
+  float gate;                       /* the correction applies only where |correction| > gate (log2) */
 } ws_estimator_weights;
 typedef struct ws_serve_options {
   int slots;                        /* worker threads (queries in flight), 1..256 */

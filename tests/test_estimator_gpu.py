@@ -1,11 +1,16 @@
 """The estimator on the GPU: the sketch kernel's registers and counts equal the host definition on the
-same sampled rows; the MLP kernel equals the FP32 forward pass over the BF16 weights; learned sizing of
-COUNT(DISTINCT)'s phase-1 table gives the plain sizing's result in fewer (or as many) runs."""
+same sampled rows (and, without keys, it counts); the MLP kernel equals the FP32 forward pass over the
+BF16 weights; learned sizing of COUNT(DISTINCT)'s phase-1 table gives the plain sizing's result in fewer
+(or as many) runs; the selectivity and join-size predictions land within a factor 2; a join sized by
+its prediction, or a sparse key range moved to the hash path, gives the same pairs / groups."""
+import ctypes
+
 import numpy as np
 import pytest
 
 from warpstore_b200 import abi, ops
 from warpstore_b200 import estimator as E
+from warpstore_b200 import query as q
 from warpstore_b200 import workloads as W
 
 pytestmark = pytest.mark.gpu
@@ -52,3 +57,126 @@ def test_learned_sizing_same_result_fewer_runs(table):
     assert np.array_equal(kp[op], kl[ol])
     assert np.array_equal(plain[1][op].view(np.int64), learned[1][ol].view(np.int64))
     print(f"\n[estimator] distinct pairs {plain[3]}: phase-1 runs plain {plain[2]}, learned {learned[2]}")
+
+
+def test_sketch_counts_without_keys(table):
+    """A plan without keys only counts: the filter's sampled selectivity, registers all 0."""
+    cut = W.high_cardinality_cut(9)
+    e, aq, _ = W.high_cardinality_query(table, cut)
+    counting = abi.AggPlan()
+    ctypes.memmove(ctypes.addressof(counting), ctypes.addressof(aq.plan), ctypes.sizeof(aq.plan))
+    counting.nkeys = 0
+    regs, sampled, passing = E.sketch(e.env, e.ncols, counting, table.batches(True), 1 << 16)
+    rows = E.sample_rows_of(table.n, 1 << 16)
+    assert not regs.any()
+    assert sampled == rows.size and passing == int((table.cols[1].data[rows] < cut).sum())
+
+
+def sorted_table(n=3_000_000):
+    rng = np.random.default_rng(4)
+    t = W.Table(n, seg_rows=1 << 18)
+    t.add("day", abi.T_I32, np.sort(rng.integers(0, 3650, n)).astype(np.int32))  # arrival order
+    t.add("v", abi.T_I64, rng.integers(0, 1000, n, dtype=np.int64))
+    return t
+
+
+@pytest.mark.parametrize("lo_day,with_v", [(3640, False), (1000, True), (3649, True)])
+def test_estimate_rows_with_zone_maps(lo_day, with_v):
+    """The selectivity prediction (sampled count + zone maps over the sorted column + MLP) stays within
+    a factor 2 of the rows that pass, also where the sample holds a handful of them."""
+    t = sorted_table()
+    t.to_device()
+    try:
+        e = W.env_for(t)
+        where = q.col(0).ge(lo_day)
+        if with_v:
+            where = q.and_(where, q.col(1).lt(100))
+        aq = q.AggQuery(e, where, [], [q.Agg("COUNT")])
+        mm = {0: [(int(t.cols[0].data[s * t.seg_rows:(s + 1) * t.seg_rows].min()),
+                   int(t.cols[0].data[s * t.seg_rows:(s + 1) * t.seg_rows].max())) for s in range(t.nseg)]}
+        pred = E.estimate_rows(e.env, e.ncols, aq.plan, where, t.batches(True), mm, sample_rows=1 << 14)
+        truth = int(((t.cols[0].data >= lo_day) & ((t.cols[1].data < 100) | (not with_v))).sum())
+        assert truth / 2 <= pred <= truth * 2, (pred, truth)
+    finally:
+        t.free_device()
+
+
+@pytest.mark.parametrize("dup", [False, True], ids=["unique-build", "many-to-many"])
+def test_sized_join_same_pairs_and_prediction(dup):
+    """ws_hash_join_sized gives the pairs of ws_hash_join for any first capacity (a short one costs a
+    second attempt); the predicted pair count sizes a many-to-many join in one attempt, where the
+    plain first capacity (the probe rows) takes two."""
+    rng = np.random.default_rng(8 + dup)
+    nb, np_ = 400_000, 2_000_000
+    bk = (rng.integers(0, 100_000, nb) if dup else rng.permutation(1 << 22)[:nb]).astype(np.int64)
+    pk = rng.integers(0, 1 << 22 if not dup else 150_000, np_).astype(np.int64)
+    mul = np.uint64(0x9E3779B97F4A7C15)
+    bk, pk = (bk.astype(np.uint64) * mul).view(np.int64), (pk.astype(np.uint64) * mul).view(np.int64)
+    db, dp = ops.DeviceBuffer.from_array(bk), ops.DeviceBuffer.from_array(pk)
+    bv, pv = abi.ColView(db.ptr, abi.T_I64N, 0, 0, 0), abi.ColView(dp.ptr, abi.T_I64N, 0, 0, 0)
+
+    def pairs(ob, op, m):
+        gb, gp = ops.device_to_array(ob, np.int32, m), ops.device_to_array(op, np.int32, m)
+        ops.tmp_free(ob)
+        ops.tmp_free(op)
+        o = np.lexsort((gb, gp))
+        return gb[o], gp[o]
+
+    ob, op, m = ops.hash_join(bv, nb, pv, np_)
+    want = pairs(ob, op, m)
+    for first in (1, m // 3, m, 3 * m):
+        ob, op, m2, att = ops.hash_join_sized(bv, nb, pv, np_, first)
+        got = pairs(ob, op, m2)
+        assert m2 == m and np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+        assert att == (1 if first >= m else 2)
+    pred = E.estimate_pairs(bv, nb, pv, np_)
+    assert m / 2 <= pred <= 2 * m, (pred, m)
+    cap = E.learned_pair_capacity(pred)
+    _, _, _, att = (lambda r: (ops.tmp_free(r[0]), ops.tmp_free(r[1]), r[2], r[3]))(
+        ops.hash_join_sized(bv, nb, pv, np_, cap))
+    plain = 1 if m <= np_ else 2
+    print(f"\n[estimator] join pairs {m}: predicted {pred:.0f}, first capacity {cap} -> {att} attempt(s); "
+          f"probe rows {np_} -> {plain}")
+    if dup:  # ~2.7 pairs per probe row: the plain capacity reruns, the predicted one does not
+        assert plain == 2 and att == 1
+    else:  # ~10 % of the probe rows match: the predicted buffers hold a fraction of the plain ones
+        assert cap <= np_ // 4
+
+
+def test_sparse_key_range_takes_hash_path_same_result():
+    """choose_grouping leaves a dense global table over a sparse key range (2^22 slots, 5,000 groups)
+    for the hash path, sized by the group-count prediction; the groups equal the dense table's."""
+    rng = np.random.default_rng(6)
+    n, G = 2_000_000, 1 << 22
+    vals = np.sort(rng.choice(G, 5_000, replace=False)).astype(np.int32)
+    vals[0], vals[-1] = 0, G - 1
+    t = W.Table(n)
+    t.add("k", abi.T_I32, vals[rng.integers(0, vals.size, n)])
+    t.add("v", abi.T_I64, rng.integers(-1000, 1000, n, dtype=np.int64))
+    t.to_device()
+    ops.jit_set_mode(abi.JIT_SYNC)
+    try:
+        e = W.env_for(t)
+        out = []
+        for learned in (False, True):
+            aq = q.AggQuery(e, None, [(q.col(0), True)], [q.Agg("COUNT"), q.Agg("SUM", q.col(1), "BIGINT", True)])
+            pred = E.estimate_groups(e.env, e.ncols, aq.plan, t.batches(True), key_range=G) if learned else None
+            ds = E.choose_grouping(aq.plan, [(0, G - 1)], n, pred)
+            assert (ds is None) == learned
+            cap = E.learned_capacity(pred) if learned else 1024
+            fn = abi.JF_DENSE if ds is not None else abi.JF_GROUPED
+            prog = ops.jit_get(e.env, e.ncols, aq.plan, fn, "sparse range")
+            agg = ops.GpuAggregator(aq.plan, cap, ds)
+            agg.add_batches(e.ncols, t.batches(True))
+            agg.run(e.env, prog)
+            assert not agg.overflowed()
+            k, _, ex = agg.fetch()
+            agg.close()
+            kk = np.ascontiguousarray(k).view(np.int64)[:, 0]
+            o = np.argsort(kk)
+            out.append((kk[o], ex[o]))
+        assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+        assert out[0][0].size == vals.size
+    finally:
+        ops.jit_set_mode(-1)
+        t.free_device()

@@ -49,7 +49,7 @@ def test_tuned_shapes_give_the_oracle_result(tuning):
     kinds = sorted({k.split(":")[0] for k in tab})
     assert kinds == ["dense_priv", "hash", "nokeys"], tab
     assert any(k.split(":")[1].startswith("i") for k in tab)  # the interpreter's own entry
-    assert all(us > 0 for _, _, us in tab.values())
+    assert all(us > 0 for _, _, _, us in tab.values())
     # recorded: the same runs tune nothing more
     n = len(tab)
     run_and_check(t, e, aq.plan, ds)
@@ -62,5 +62,6 @@ def test_tuned_shapes_give_the_oracle_result(tuning):
     ops.tune_clear()
     ops.jit_set_cache_dir(str(tuning))
     assert set(ops.tune_table()) == set(tab)
-    print("\n[tune] " + "; ".join(f"{k.split(':')[0]}: ctas/SM {c or 'max'}, smem {m or 'default'} KB, {us:.0f} us"
-                                  for k, (c, m, us) in sorted(tab.items())))
+    print("\n[tune] " + "; ".join(f"{k.split(':')[0]}: ctas/SM {c or 'max'}, smem {m or 'default'} KB, "
+                                  f"stages {'default' if st < 0 else st}, {us:.0f} us"
+                                  for k, (c, m, st, us) in sorted(tab.items())))

@@ -93,6 +93,8 @@ SIGNATURES = {
     "ws_hash_join_parts": (C.c_int, [abi.ColView, P, C.c_int, abi.ColView, P, C.c_int, C.POINTER(P), C.POINTER(P),
                                      P, I64P]),
     "ws_hash_join": (C.c_int, [abi.ColView, C.c_int64, abi.ColView, C.c_int64, C.POINTER(P), C.POINTER(P), I64P]),
+    "ws_hash_join_sized": (C.c_int, [abi.ColView, C.c_int64, abi.ColView, C.c_int64, C.c_int64, C.POINTER(P),
+                                     C.POINTER(P), I64P, C.POINTER(C.c_int)]),
     "ws_hash_join_outer": (C.c_int, [abi.ColView, C.c_int64, abi.ColView, C.c_int64, C.c_int, C.POINTER(P),
                                      C.POINTER(P), I64P]),
     "ws_cross_join": (C.c_int, [C.c_int64, C.c_int64, C.POINTER(P), C.POINTER(P), I64P]),

@@ -127,4 +127,4 @@ class EstimatorWeights(C.Structure):
     """ws_estimator_weights (include/ws_b200.h)."""
     _fields_ = [("hidden", C.c_int), ("w1", C.c_void_p), ("b1", C.c_void_p), ("w2", C.c_void_p), ("b2", C.c_void_p),
                 ("w3", C.c_void_p), ("b3", C.c_float), ("mean", C.c_void_p), ("std", C.c_void_p),
-                ("margin", C.c_double)]
+                ("margin", C.c_double), ("gate", C.c_float)]

@@ -69,6 +69,7 @@ __global__ void kHllSketch(const __grid_constant__ SketchSpec s, const __grid_co
       if (!(s.whereInt ? w.i != 0 : truthy(w.d))) continue;
     }
     ++passing;
+    if (!s.nkeys) continue;  // counting only: the filter's sampled selectivity
     const u64 h = sketchHash(s, cv, r, env);
     const unsigned j = (unsigned)(h >> (64 - s.p));
     const u64 rest = h << s.p;
@@ -126,7 +127,7 @@ int ws_hll_sketch(const ws_expr_env* env, int ncols, const ws_agg_plan* plan, in
   return guardedCall([&] {
     if (ncols < 0 || ncols > WS_MAX_COLS || nb < 0) throw Error("sketch: bad column or batch count", WS_ERR_ARG);
     if (p < 4 || p > kHllMaxP) throw Error("sketch: precision must be 4..12", WS_ERR_ARG);
-    if (plan->nkeys < 1 || plan->nkeys > WS_INTERP_KEYS) throw Error("sketch: 1 to 4 GROUP BY keys", WS_ERR_ARG);
+    if (plan->nkeys < 0 || plan->nkeys > WS_INTERP_KEYS) throw Error("sketch: 0 to 4 GROUP BY keys", WS_ERR_ARG);
     std::unique_ptr<TProgs> tp(new TProgs);
     buildTProgs(*env, ncols, *plan, plan->hasWhere != 0, *tp);
     SketchSpec s{};

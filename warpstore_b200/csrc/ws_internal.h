@@ -65,6 +65,7 @@ void countLaunch(int n = 1);     // kernels launched by this library (ws_kernel_
 struct TuneChoice {
   int ctasPerSm = 0;
   int smemKB = 0;
+  int stages = -1;  // shared-memory tile stages of a compiled scan (0: direct loads; -1: the default)
   bool found = false;
 };
 int tuneMode();  // WS_TUNE_USE / WS_TUNE_ON / WS_TUNE_OFF

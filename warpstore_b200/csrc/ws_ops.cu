@@ -536,6 +536,7 @@ static size_t hashSmemSlots(const ws_aggregator& A, size_t budget) {
 // A scan prepared for launching elsewhere (a captured graph): kernel, shape, launch descriptor and the
 // device buffers the descriptor points to.
 struct PreparedScan {
+  bool direct = false;    // in: direct loads only (a multi-query launch has no staged form)
   bool ready = false;     // false: the batches hold no tiles (nothing to launch)
   bool compiled = false;  // the plan's generated kernels (not the interpreter)
   CUfunction f = nullptr;
@@ -580,7 +581,6 @@ static void aggRun(ws_aggregator& A, const ws_expr_env& env, const ws_jit_progra
     return e ? std::max(0, std::min(8, atoi(e))) : 0;
   }();
   const int S = stageBytes > 0 ? (int)std::min<int64_t>(maxStages, (200 * 1024) / stageBytes) : 0;
-  const size_t stageSmem = S >= 2 ? (size_t)S * stageBytes : 0;
   // The scan's launch shape as a function of a tuning choice: kernel, shared memory, block size and
   // the launch fields the shape changes.  Per-CTA partial rows (`part`: no-key and private-row scans)
   // are sized by the grid.
@@ -598,16 +598,30 @@ static void aggRun(ws_aggregator& A, const ws_expr_env& env, const ws_jit_progra
     t.ctasPerSm = c;
     return t;
   };
+  auto staged = [](int st) {
+    TuneChoice t;
+    t.stages = st;
+    return t;
+  };
+  Launch* lp = &L;
   if (A.plan.nkeys == 0) {
     CUfunction f = ks.fn[K_NOKEYS];
     if (!f) throw Error("compiled plan has no aggregation kernel", WS_ERR_INTERNAL);
-    L.stages = S >= 2 ? S : 0;
-    const int threads = L.stages ? kStagedThreads : kThreads;
-    shapeOf = [=](const TuneChoice&) { return Shape{f, stageSmem, threads}; };
+    shapeOf = [=](const TuneChoice& c) {
+      // stage count: the choice's, else the default; within 200 KB of tile stages
+      int st = c.stages >= 0 ? c.stages : S;
+      if (stageBytes > 0) st = (int)std::min<int64_t>(st, (200 * 1024) / stageBytes);
+      if (st < 2 || stageBytes <= 0) st = 0;
+      lp->stages = st;
+      return Shape{f, (size_t)st * stageBytes, st ? kStagedThreads : kThreads};
+    };
     name = "nokeys";
     partRows = 1;
     cands.push_back(ctas(2));
     cands.push_back(ctas(1));
+    if (stageBytes > 0)
+      for (int st : {0, 2, 3})
+        if (st != (S >= 2 ? S : 0)) cands.push_back(staged(st));
   } else if (A.isDense) {
     for (int k = 0; k < A.plan.nkeys; ++k) {
       L.kmin[k] = A.dense.kmin[k];
@@ -622,17 +636,23 @@ static void aggRun(ws_aggregator& A, const ws_expr_env& env, const ws_jit_progra
     const size_t privBytes = (size_t)G * A.lay.frw * kThreads * 8 + (size_t)G * naEv * 16;
     const size_t sharedSmem = (size_t)G * A.lay.rw * 8;
     if (G * A.lay.frw <= 48 && ks.fn[K_DENSE_PRIV]) {
-      const size_t budget = 220 * 1024;
-      int S2 = stageBytes > 0 ? (int)std::min<int64_t>(maxStages, (int64_t)(budget - privBytes) / stageBytes) : 0;
-      if (S2 < 2 || !ks.fn[K_DENSE_PRIV_STAGED]) S2 = 0;
-      CUfunction f = S2 ? ks.fn[K_DENSE_PRIV_STAGED] : ks.fn[K_DENSE_PRIV];
-      L.stages = S2;
-      const int threads = S2 ? kStagedThreads : kThreads;
-      const size_t smem = (size_t)S2 * stageBytes + privBytes;
-      shapeOf = [=](const TuneChoice&) { return Shape{f, smem, threads}; };
+      // tile stages fit beside the private rows within 220 KB; the staged body is its own entry
+      const int64_t room = std::max<int64_t>(0, (int64_t)(220 * 1024) - (int64_t)privBytes);
+      const int fitStages = stageBytes > 0 ? (int)std::min<int64_t>(8, room / stageBytes) : 0;
+      CUfunction direct = ks.fn[K_DENSE_PRIV], stagedFn = ks.fn[K_DENSE_PRIV_STAGED];
+      shapeOf = [=](const TuneChoice& c) {
+        int st = std::min(c.stages >= 0 ? c.stages : maxStages, fitStages);
+        if (st < 2 || !stagedFn) st = 0;
+        lp->stages = st;
+        return Shape{st ? stagedFn : direct, (size_t)st * stageBytes + privBytes, st ? kStagedThreads : kThreads};
+      };
       name = "dense_priv";
       partRows = G;
       cands.push_back(ctas(1));
+      if (stagedFn && fitStages >= 2)
+        for (int st : {0, 2, 3})
+          if (st <= fitStages && st != (std::min(maxStages, fitStages) >= 2 ? std::min(maxStages, fitStages) : 0))
+            cands.push_back(staged(st));
     } else if (sharedSmem <= 96 * 1024 && ks.fn[K_DENSE_SHARED]) {
       CUfunction f = ks.fn[K_DENSE_SHARED];
       shapeOf = [=](const TuneChoice&) { return Shape{f, sharedSmem, kThreads}; };
@@ -658,7 +678,6 @@ static void aggRun(ws_aggregator& A, const ws_expr_env& env, const ws_jit_progra
     const size_t per = (size_t)A.lay.rw * 8 + (A.plan.nkeys > 1 ? (size_t)A.plan.nkeys * 8 : 0);
     // spill buffer: up to a tile's rows, within 40 KB
     L.spillRows = (int)std::min<size_t>(kTile, (40 * 1024) / per);
-    Launch* lp = &L;
     ws_aggregator* ap = &A;
     shapeOf = [=](const TuneChoice& c) {
       // per-CTA table: up to 4096 slots within the budget (default 64 KB)
@@ -692,8 +711,16 @@ static void aggRun(ws_aggregator& A, const ws_expr_env& env, const ws_jit_progra
   };
   const std::string key = tuneKey(name, useJit ? jit : nullptr, A.plan, d.ntiles);
   TuneChoice choice;
+  if (prep && prep->direct) {  // tuned without staged candidates: a multi-query launch loads directly
+    std::vector<TuneChoice> directOnly;
+    for (const TuneChoice& c : cands)
+      if (c.stages <= 0) directOnly.push_back(c);
+    for (TuneChoice& c : directOnly) c.stages = 0;
+    cands.swap(directOnly);
+  }
   if (!tuneLookup(key, choice) && tuneMode() == WS_TUNE_ON && A.windows == 0 && A.rowsDone == 0)
     choice = tuneScan(A, key, cands, launchOnce);
+  if (prep && prep->direct) choice.stages = 0;
   if (prep) {
     const Shape sh = shapeOf(choice);
     unsigned grid = persistentGrid(sh.f, sh.smem, d.ntiles, sh.threads);
@@ -884,7 +911,10 @@ int ws_agg_run_many(ws_aggregator* const* aggs, const ws_expr_env* const* envs, 
     if (n < 1 || n > 1024 || !aggs || !envs) throw Error("ws_agg_run_many: 1..1024 aggregators", WS_ERR_ARG);
     // each query prepared as for its own launch (descriptor uploaded, kernel and shape chosen)
     std::vector<PreparedScan> preps((size_t)n);
-    for (int i = 0; i < n; ++i) aggRun(*aggs[i], *envs[i], jit, &preps[(size_t)i]);
+    for (int i = 0; i < n; ++i) {
+      preps[(size_t)i].direct = true;
+      aggRun(*aggs[i], *envs[i], jit, &preps[(size_t)i]);
+    }
     const KernelSet* ks = nullptr;
     int multi = -1;
     size_t smem = 0;
@@ -897,7 +927,7 @@ int ws_agg_run_many(ws_aggregator* const* aggs, const ws_expr_env* const* envs, 
       const KernelSet& k = p.compiled ? jit->kernels : interpKernels();
       const int m = p.f == k.fn[K_NOKEYS] ? K_MULTI_NOKEYS : p.f == k.fn[K_DENSE_PRIV] ? K_MULTI_DENSE_PRIV
                   : p.f == k.fn[K_HASH] ? K_MULTI_HASH : -1;
-      if (m < 0 || !k.fn[m])
+      if (m < 0 || !k.fn[m] || p.L.stages)
         throw Error("ws_agg_run_many: a query's scan has no multi-query form (dense shared / global rows, staged tiles)",
                     WS_ERR_ARG);
       if (multi >= 0 && (m != multi || &k != ks))

@@ -740,9 +740,11 @@ __global__ void kCross(int64_t na, int64_t nb, int32_t* oa, int32_t* ob) {
 
 // Inner (outer = 0) or outer equi join over build / probe partitions; see ws_hash_join_parts and
 // ws_hash_join_outer.  full: also the build rows that matched nothing, paired with probe row -1.
-static void joinImpl(ws_col_view build_key, const int64_t* boff, int pb, ws_col_view probe_key, const int64_t* poff,
-                     int pp, int outer, bool full, int32_t** out_build, int32_t** out_probe, int64_t* out_off,
-                     int64_t* m_out) {
+// firstCap > 0 (an inner join of one partition): the pair buffers' capacity of the first attempt
+// instead of the probe rows.  Returns the attempts made (a second one when the first capacity was short).
+static int joinImpl(ws_col_view build_key, const int64_t* boff, int pb, ws_col_view probe_key, const int64_t* poff,
+                    int pp, int outer, bool full, int32_t** out_build, int32_t** out_probe, int64_t* out_off,
+                    int64_t* m_out, int64_t firstCap = 0) {
   {
     *out_build = *out_probe = nullptr;
     if (pb < 1 || pp < 1 || (pb != 1 && pb != pp)) throw Error("internal: partition count mismatch in join", WS_ERR_INTERNAL);
@@ -763,7 +765,7 @@ static void joinImpl(ws_col_view build_key, const int64_t* boff, int pb, ws_col_
       *out_build = ob.release();
       *out_probe = op.release();
       *m_out = m;
-      return;
+      return 1;
     }
     DBuf<uint8_t> matchedBuf(full ? nb : 1);
     uint8_t* matched = full ? matchedBuf.p : nullptr;
@@ -822,6 +824,7 @@ static void joinImpl(ws_col_view build_key, const int64_t* boff, int pb, ws_col_
     std::vector<int64_t> capOut(pp), outStart(pp + 1, 0);
     for (int p = 0; p < pp; ++p) {
       capOut[p] = poff[p + 1] - poff[p];
+      if (firstCap > 0 && !outer && pp == 1) capOut[p] = std::min<int64_t>(firstCap, INT32_MAX);
       outStart[p + 1] = outStart[p] + capOut[p];
     }
     DBuf<unsigned long long> counters(pp);
@@ -897,7 +900,7 @@ static void joinImpl(ws_col_view build_key, const int64_t* boff, int pb, ws_col_
         *out_build = cb.release();
         *out_probe = cp.release();
         *m_out = m + extra;
-        return;
+        return attempt + 1;
       }
       if (fits) {
         // make the partitions' pairs contiguous
@@ -919,7 +922,7 @@ static void joinImpl(ws_col_view build_key, const int64_t* boff, int pb, ws_col_
         if (out_off)
           for (int p = 0; p <= pp; ++p) out_off[p] = dst[p];
         *m_out = m;
-        return;
+        return attempt + 1;
       }
       for (int p = 0; p < pp; ++p) {  // exact sizes for the second attempt
         capOut[p] = (int64_t)cnt[p];
@@ -946,6 +949,16 @@ int ws_hash_join(ws_col_view build_key, int64_t nb, ws_col_view probe_key, int64
                  int32_t** out_probe, int64_t* m) {
   const int64_t bo[2] = {0, nb}, po[2] = {0, np};
   return ws_hash_join_parts(build_key, bo, 1, probe_key, po, 1, out_build, out_probe, nullptr, m);
+}
+
+int ws_hash_join_sized(ws_col_view build_key, int64_t nb, ws_col_view probe_key, int64_t np, int64_t first_capacity,
+                       int32_t** out_build, int32_t** out_probe, int64_t* m, int* attempts) {
+  return guardedCall([&] {
+    const int64_t bo[2] = {0, nb}, po[2] = {0, np};
+    const int a = joinImpl(build_key, bo, 1, probe_key, po, 1, 0, false, out_build, out_probe, nullptr, m,
+                           std::max<int64_t>(first_capacity, 1));
+    if (attempts) *attempts = a;
+  });
 }
 
 int ws_hash_join_outer(ws_col_view build_key, int64_t nb, ws_col_view probe_key, int64_t np, int full,

@@ -4,6 +4,7 @@
 // estimator weights, a query whose plain-rule table is large is sized from the learned estimate (GPU
 // sketch + GPU MLP); the plain rule's overflow retry stays the fallback.  No counterpart in the
 // reference, whose connections each run their query synchronously (src/server.cpp).
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
@@ -146,7 +147,10 @@ int64_t initialCap(const ws_serve_query& q, const ws_serve_options& o) {
     features(regs, sampled, passing, total, q.key_range, x);
     for (int i = 0; i < 9; ++i) xn[i] = (x[i] - w->mean[i]) / w->std[i];
     checkRc(ws_mlp_infer(xn, 1, 9, w->hidden, w->w1, w->b1, w->w2, w->b2, w->w3, w->b3, &y));
-    const double pred = std::exp2((double)x[8] + (double)y) - 1;
+    // log2(1 + groups) floored at log2(1 + 1024), the smallest capacity (as estimator.Model.gated)
+    const double floorLog2 = std::log2(1025.0);
+    const double corr = std::fabs(y) > w->gate ? (double)y : 0.0;
+    const double pred = std::exp2(std::max(std::max((double)x[8], floorLog2) + corr, floorLog2)) - 1;
     cap = std::min(cap, pow2AtLeast(2 * pred * w->margin, 1024));
   }
   return cap;

@@ -1,18 +1,21 @@
 // Launch-shape autotuner for the aggregation scans.  The choices are kept per key = (scan kernel,
 // plan, size class): the plan is a 64-bit FNV-1a digest of the compiled evaluator's source (the
 // interpreter: of the plan's shape), the size class log2 of the scan's tiles.  A choice is the CTAs
-// per SM of the persistent grid (0: as many as fit) and, for the hash scan, the shared-memory budget of
-// the per-CTA table in KB (0: the default 64).  In tuning mode a key seen for the first time is tuned
-// on the query's own batches (aggRun in ws_ops.cu times each candidate and keeps the fastest); the
-// table lives in memory and, once a plan-cache directory is set, in <dir>/wsb200_tune.txt (one line
-// per key: `key ctas smem_kb microseconds`), read back when the directory is set.  No counterpart in
-// the reference, whose launch shapes are fixed (src/gpu.cu:393-653).
+// per SM of the persistent grid (0: as many as fit), for the hash scan the shared-memory budget of the
+// per-CTA table in KB (0: the default), and for compiled no-key and private-row scans the depth of the
+// TMA tile staging (0: direct loads, 2..4 stages, -1: the default).  In tuning mode a key seen for the
+// first time is tuned on the query's own batches (aggRun in ws_ops.cu times each candidate and keeps
+// the fastest); the table lives in memory and, once a plan-cache directory is set, in
+// <dir>/wsb200_tune.txt (one line per key: `key ctas smem_kb stages microseconds`; lines without the
+// stages field are read with the default), read back when the directory is set.  No counterpart in the
+// reference, whose launch shapes are fixed (src/gpu.cu:393-653).
 #include <cstdio>
 #include <cstring>
 #include <fstream>
 #include <map>
 #include <mutex>
 #include <sstream>
+#include <vector>
 
 #include "ws_b200.h"
 #include "ws_internal.h"
@@ -38,20 +41,25 @@ uint64_t fnv1a(const void* p, size_t n, uint64_t h = 0xcbf29ce484222325ull) {
 
 bool parseLine(const std::string& line, std::string& key, Entry& e) {
   std::istringstream in(line);
-  int ctas = -1, smem = -1;
-  double us = 0;
-  if (!(in >> key >> ctas >> smem >> us)) return false;
-  if (ctas < 0 || ctas > 64 || smem < 0 || smem > 228) return false;
+  if (!(in >> key)) return false;
+  std::vector<double> v;
+  double x;
+  while (in >> x) v.push_back(x);
+  if (!in.eof() || (v.size() != 3 && v.size() != 4)) return false;
+  const int ctas = (int)v[0], smem = (int)v[1], stages = v.size() == 4 ? (int)v[2] : -1;
+  if (v[0] != ctas || v[1] != smem || ctas < 0 || ctas > 64 || smem < 0 || smem > 228) return false;
+  if (stages != -1 && stages != 0 && (stages < 2 || stages > 4)) return false;
   e.c.ctasPerSm = ctas;
   e.c.smemKB = smem;
+  e.c.stages = stages;
   e.c.found = true;
-  e.us = us;
+  e.us = v.back();
   return true;
 }
 
 std::string formatLine(const std::string& key, const Entry& e) {
-  char b[64];
-  std::snprintf(b, sizeof(b), " %d %d %.1f\n", e.c.ctasPerSm, e.c.smemKB, e.us);
+  char b[80];
+  std::snprintf(b, sizeof(b), " %d %d %d %.1f\n", e.c.ctasPerSm, e.c.smemKB, e.c.stages, e.us);
   return key + b;
 }
 

@@ -85,15 +85,16 @@ def tune_set_mode(mode: int):
 
 
 def tune_table() -> dict:
-    """{key: (ctas per SM, shared KB, microseconds)} of the autotuner's table."""
+    """{key: (ctas per SM, shared KB, tile stages, microseconds)} of the autotuner's table (stages -1:
+    the default)."""
     need = C.c_size_t()
     lib().ws_tune_table(None, 0, C.byref(need))
     buf = C.create_string_buffer(need.value)
     check(lib().ws_tune_table(buf, need.value, C.byref(need)))
     out = {}
     for line in buf.value.decode().splitlines():
-        k, c, m, us = line.split()
-        out[k] = (int(c), int(m), float(us))
+        k, c, m, st, us = line.split()
+        out[k] = (int(c), int(m), int(st), float(us))
     return out
 
 
@@ -390,6 +391,15 @@ def hash_join_parts(build_key: abi.ColView, boff: list, probe_key: abi.ColView, 
 
 def hash_join(build_key: abi.ColView, nb: int, probe_key: abi.ColView, np_: int):
     return hash_join_parts(build_key, [0, nb], probe_key, [0, np_])[:3]
+
+
+def hash_join_sized(build_key: abi.ColView, nb: int, probe_key: abi.ColView, np_: int, first_capacity: int):
+    """(build idx ptr, probe idx ptr, m, attempts) of the inner join whose pair buffers first hold
+    first_capacity pairs (a second attempt with exact sizes when the join emits more)."""
+    b, p, m, a = P(), P(), C.c_int64(), C.c_int()
+    check(lib().ws_hash_join_sized(build_key, nb, probe_key, np_, int(first_capacity), C.byref(b), C.byref(p),
+                                   C.byref(m), C.byref(a)))
+    return b.value, p.value, m.value, a.value
 
 
 def hash_join_outer(build_key: abi.ColView, nb: int, probe_key: abi.ColView, np_: int, full: bool = False):

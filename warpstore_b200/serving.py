@@ -331,7 +331,7 @@ def run_native(tables: list, prepared: list, arrays: list, mode: str = "batched"
         keep.append(hold)
         w = abi.EstimatorWeights(estimator.HIDDEN, hold[0].ctypes.data, hold[1].ctypes.data, hold[2].ctypes.data,
                                  hold[3].ctypes.data, hold[4].ctypes.data, float(m.b3), hold[5].ctypes.data,
-                                 hold[6].ctypes.data, 2.0 ** float(m.meta.get("val_p90_log2_err", 0.0)))
+                                 hold[6].ctypes.data, m.margin(), m.gate)
     wall = C.c_double()
     opt = abi.ServeOptions(nslots, hbm_budget, C.addressof(w) if w else None, int(bool(pinned)),
                            0 if keep_results else int(arena_bytes), int(bool(checksum)), int(batch))
