@@ -338,7 +338,7 @@ typedef struct ws_serve_query {
                                        exact words (DOUBLE SUM slots excluded) -- order-independent */
   double fsum;                      /* with `checksum`: the sum of the DOUBLE SUM slots over the groups */
 } ws_serve_query;
-/* Learned sizing (est may be null for the plain rule): the estimator's group-count MLP (9 features,
+/* Learned sizing (est may be null for the plain rule): the estimator's group-count MLP (10 features,
  * `hidden` units, BF16 weight bits), its input normalisation, the capacity margin (2^(p90 of the log2
  * underestimates)) and the gate of its correction. */
 typedef struct ws_estimator_weights {

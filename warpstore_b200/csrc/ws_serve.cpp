@@ -36,13 +36,30 @@ double hllEstimate(const std::vector<uint32_t>& regs) {
   return e;
 }
 
-// The estimator's nine inputs (the same definition as the Python package's features())
+// The distinct values D of a population of equally frequent values whose sample of s rows shows d:
+// the root of D (1 - exp(-s / D)) = d by bisection on log D; infinite when d is within 5 % of s (the
+// sketch's error cannot tell such a sample from one of distinct rows).
+double uniformDistinct(double d, double s) {
+  if (d <= 0) return 0;
+  if (d >= 0.95 * s) return HUGE_VAL;
+  double lo = d, hi = d * std::ldexp(1.0, 60);
+  for (int i = 0; i < 100; ++i) {
+    const double mid = std::sqrt(lo * hi);
+    if (mid * -std::expm1(-s / mid) < d) lo = mid;
+    else hi = mid;
+  }
+  return hi;
+}
+
+// The estimator's ten inputs (the same definition as the Python package's features())
+constexpr int kGroupFeatures = 10;
 void features(const std::vector<uint32_t>& regs, int64_t sampled, int64_t passing, int64_t total, double keyRange,
               float* x) {
   const double est = hllEstimate(regs);
   const double scale = (double)total / (double)std::max<int64_t>(sampled, 1);
   const double kr = keyRange > 0 ? keyRange : std::ldexp(1.0, 63);
-  const double naive = std::min({est * scale, (double)passing * scale, kr});
+  const double scaled = std::min({est * scale, (double)passing * scale, kr});
+  const double naive = std::min(uniformDistinct(est, (double)passing), scaled);
   int zeros = 0;
   for (uint32_t r : regs) zeros += r == 0;
   x[0] = (float)std::log2(1 + est);
@@ -53,7 +70,8 @@ void features(const std::vector<uint32_t>& regs, int64_t sampled, int64_t passin
   x[5] = (float)(est / (double)std::max<int64_t>(passing, 1));
   x[6] = (float)((double)passing / (double)std::max<int64_t>(sampled, 1));
   x[7] = (float)((double)zeros / (double)regs.size());
-  x[8] = (float)std::log2(1 + naive);
+  x[8] = (float)std::log2(1 + scaled);
+  x[9] = (float)std::log2(1 + naive);
 }
 
 int64_t pow2AtLeast(double x, int64_t lo) {
@@ -143,14 +161,14 @@ int64_t initialCap(const ws_serve_query& q, const ws_serve_options& o) {
     for (int b = 0; b < q.nb; ++b) total += q.bn[b];
     checkRc(ws_hll_sketch(q.env, q.ncols, q.plan, q.nb, q.bn, q.bdel, q.bcols, 12, 1 << 18, regs.data(), &sampled,
                           &passing));
-    float x[9], xn[9], y = 0;
+    float x[kGroupFeatures], xn[kGroupFeatures], y = 0;
     features(regs, sampled, passing, total, q.key_range, x);
-    for (int i = 0; i < 9; ++i) xn[i] = (x[i] - w->mean[i]) / w->std[i];
-    checkRc(ws_mlp_infer(xn, 1, 9, w->hidden, w->w1, w->b1, w->w2, w->b2, w->w3, w->b3, &y));
+    for (int i = 0; i < kGroupFeatures; ++i) xn[i] = (x[i] - w->mean[i]) / w->std[i];
+    checkRc(ws_mlp_infer(xn, 1, kGroupFeatures, w->hidden, w->w1, w->b1, w->w2, w->b2, w->w3, w->b3, &y));
     // log2(1 + groups) floored at log2(1 + 1024), the smallest capacity (as estimator.Model.gated)
     const double floorLog2 = std::log2(1025.0);
     const double corr = std::fabs(y) > w->gate ? (double)y : 0.0;
-    const double pred = std::exp2(std::max(std::max((double)x[8], floorLog2) + corr, floorLog2)) - 1;
+    const double pred = std::exp2(std::max(std::max((double)x[kGroupFeatures - 1], floorLog2) + corr, floorLog2)) - 1;
     cap = std::min(cap, pow2AtLeast(2 * pred * w->margin, 1024));
   }
   return cap;

@@ -6,7 +6,8 @@ corrects a plain statistical estimate in the log2 domain:
 
 * ``groups`` -- the group count of a GROUP BY, to size its hash table: a HyperLogLog sketch (2^12
   registers) of a strided sample of the rows that pass the filter (`ws_hll_sketch`), the row counts
-  and the keys' value range; the plain estimate is the sample's distinct count scaled up.
+  and the keys' value range; the plain estimate extrapolates the sample's distinct count as if the
+  values were equally frequent.
 * ``rows`` -- the rows a filter passes, to size a selection's index buffer or a join's build side: the
   same sampled pass (without keys it only counts), plus zone maps -- each segment's min / max of the
   columns the filter compares with constants (``col < c``, ``col >= c``, ``col = c`` ...) bound and
@@ -35,7 +36,7 @@ import os
 import numpy as np
 
 HLL_P = 12
-NFEATURES = 9  # the group-count model's inputs
+NFEATURES = 10  # the group-count model's inputs
 # Every capacity the estimates size starts at 1024 entries, so counts below that are the same to it:
 # predictions, labels and errors are taken in log2(1 + max(count, 1024)).
 FLOOR_LOG2 = math.log2(1 + 1024)
@@ -103,18 +104,40 @@ def hll_estimate(regs: np.ndarray) -> float:
 
 
 # ---------------------------------------------------------------- features: group counts
+def uniform_distinct(d: float, s: float) -> float:
+    """The distinct values D of a population with equally frequent values whose sample of s rows shows d
+    of them: the root of D (1 - exp(-s / D)) = d (increasing in D from 0 towards s), by bisection on
+    log D.  Infinite (nothing bounds D) when d is within 5 % of s: the sketch's error (1.6 % at 2^12
+    registers) cannot tell such a sample from one whose rows are all distinct."""
+    if d <= 0:
+        return 0.0
+    if d >= 0.95 * s:
+        return math.inf
+    lo, hi = d, d * 2.0 ** 60
+    for _ in range(100):
+        mid = math.sqrt(lo * hi)
+        if mid * -math.expm1(-s / mid) < d:
+            lo = mid
+        else:
+            hi = mid
+    return hi
+
+
 def features(regs: np.ndarray, sampled: int, passing: int, total_rows: int, key_range: float | None) -> np.ndarray:
-    """The group-count model's inputs (log2 domain where counts are concerned); the last one is the
-    plain estimate, the sample's distinct count scaled up (capped by the passing rows and the key range)."""
+    """The group-count model's inputs (log2 domain where counts are concerned).  The last one is the
+    plain estimate: the sample's distinct count d extrapolated as if the values were equally frequent
+    (uniform_distinct; a saturated sample, whose d barely grows with more rows, stays near d), at most d
+    scaled up by the sampling rate, the passing rows and the key range."""
     est = hll_estimate(regs)
     scale = total_rows / max(sampled, 1)
     kr = float(key_range) if key_range else 2.0 ** 63
-    naive = min(est * scale, passing * scale, kr)
+    scaled = min(est * scale, passing * scale, kr)
+    naive = min(uniform_distinct(est, passing), scaled)
     zeros = float(np.mean(regs == 0))
     return np.array([
         math.log2(1 + est), math.log2(1 + passing), math.log2(1 + sampled), math.log2(1 + total_rows),
         min(math.log2(1 + kr), 64.0), est / max(passing, 1), passing / max(sampled, 1), zeros,
-        math.log2(1 + naive)], dtype=np.float32)
+        math.log2(1 + scaled), math.log2(1 + naive)], dtype=np.float32)
 
 
 # ---------------------------------------------------------------- features: filter selectivity

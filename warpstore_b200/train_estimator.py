@@ -23,6 +23,7 @@ gate: of "never", the corrections' quantiles and 0, the one that minimises media
 underestimates, the capacity margin).
 
     python -m warpstore_b200.train_estimator [--tables 400] [--seed 0] [--only groups,rows,pairs]
+    python -m warpstore_b200.train_estimator --evaluate 200      # the error table on fresh tables
 """
 from __future__ import annotations
 
@@ -233,14 +234,43 @@ def fit(target: str, xs: np.ndarray, ys: np.ndarray, epochs: int, seed: int, ext
     return {pre + k: v for k, v in out.items()}
 
 
+def evaluate(n: int, seed: int) -> str:
+    """A markdown table of |log2 error| (median / 90th percentile, floored at 1024) on n fresh tables per
+    target: the naive rule (groups: the sample's distinct count scaled up; rows: the sample's passing
+    fraction scaled up; pairs: the probe rows, the join's plain first capacity), the plain estimate
+    (the model's base) and the model."""
+    rng = np.random.default_rng(seed)
+    lines = ["| target | tables | naive rule | plain estimate | learned (gated) | gate |", "|---|---|---|---|---|---|"]
+    for target in E.TARGETS:
+        m = E.Model(target=target)
+        if target == "groups":
+            data = [make_example(rng) for _ in range(n)]
+            naive = np.array([d[0][8] for d in data])
+        elif target == "rows":
+            data = [make_rows_example(rng) for _ in range(n)]
+            naive = np.array([d[0][-1] for d in data])
+        else:
+            data = [make_pairs_example(rng) for _ in range(n)]
+            naive = np.array([math.log2(1 + d[2]) for d in data])
+        xs = np.stack([d[0] for d in data]).astype(np.float32)
+        ys = np.array([d[1] for d in data])
+        cells = [errors(v, ys) for v in (naive, xs[:, -1].astype(np.float64), m.predict_log2_np(xs))]
+        lines.append(f"| {target} | {n} | " + " | ".join(f"{a:.3f} / {b:.3f}" for a, b in cells) + f" | {m.gate:.3g} |")
+    return "\n".join(lines)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--tables", type=int, default=400)
+    ap.add_argument("--evaluate", type=int, default=0, help="only print the error table on this many fresh tables")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--epochs", type=int, default=4000)
     ap.add_argument("--only", default="groups,rows,pairs", help="targets to retrain (others are kept)")
     ap.add_argument("--out", default=E.WEIGHTS)
     a = ap.parse_args()
+    if a.evaluate:
+        print(evaluate(a.evaluate, a.seed + 777))
+        return
     keep = {}
     if os.path.exists(a.out):
         d = np.load(a.out)
