@@ -330,8 +330,8 @@ def run_ours(args, ws, rank, local):
         if prev is not None:
             finish_step(prev)
         prev = cur
+    s1.record(stream)               # after the last query's work, before its host-side check
     finish_step(prev, verify=True)  # the last step is verified in every mode
-    s1.record(stream)
     s1.synchronize()
     launches = ops.kernel_launches() - launches0
     total_ms = s0.elapsed_time(s1)

@@ -83,10 +83,13 @@ def test_choose_grouping():
     e.column(abi.T_I64)
     aq = q.AggQuery(e, None, [(q.col(0), True)], [q.Agg("COUNT"), q.Agg("SUM", q.col(1), "BIGINT", True)])
     G = 1 << 22  # a global table of 4M slots (the engine keeps dense tables within 512 MB)
-    ds = E.choose_grouping(aq.plan, [(0, G - 1)], 10_000_000, None)  # no prediction: the engine's rule
+    rows = 1 << 20  # a quarter of the slots: the fewest rows the engine's rule takes a dense table for
+    ds = E.choose_grouping(aq.plan, [(0, G - 1)], rows, None)  # no prediction: the engine's rule
     assert ds is not None and ds.G == G and not ds.priv and not ds.copies
-    assert E.choose_grouping(aq.plan, [(0, G - 1)], 10_000_000, 5_000.0) is None and aq.plan.densePriv == 0
-    ds = E.choose_grouping(aq.plan, [(0, G - 1)], 10_000_000, 4_000_000.0)  # dense enough: kept
+    assert E.choose_grouping(aq.plan, [(0, G - 1)], rows, 5_000.0) is None and aq.plan.densePriv == 0
+    ds = E.choose_grouping(aq.plan, [(0, G - 1)], rows, 400_000.0)  # groups a tenth of the slots: kept
+    assert ds is not None and ds.G == G
+    ds = E.choose_grouping(aq.plan, [(0, G - 1)], 10_000_000, 5_000.0)  # more rows than slots: kept
     assert ds is not None and ds.G == G
     ds = E.choose_grouping(aq.plan, [(0, 9)], 10_000_000, 3.0)  # private rows: never second-guessed
     assert ds is not None and ds.priv

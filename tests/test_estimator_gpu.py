@@ -146,10 +146,10 @@ def test_sized_join_same_pairs_and_prediction(dup):
 
 
 def test_sparse_key_range_takes_hash_path_same_result():
-    """choose_grouping leaves a dense global table over a sparse key range (2^22 slots, 5,000 groups)
-    for the hash path, sized by the group-count prediction; the groups equal the dense table's."""
+    """choose_grouping leaves a dense global table over a sparse key range (2^22 slots, 2^20 rows, 5,000
+    groups) for the hash path, sized by the group-count prediction; the groups equal the dense table's."""
     rng = np.random.default_rng(6)
-    n, G = 2_000_000, 1 << 22
+    n, G = 1 << 20, 1 << 22
     vals = np.sort(rng.choice(G, 5_000, replace=False)).astype(np.int32)
     vals[0], vals[-1] = 0, G - 1
     t = W.Table(n)
