@@ -371,6 +371,8 @@ def main():
     ap.add_argument("--repeats", type=int, default=2)
     ap.add_argument("--arena-mb", type=int, default=256, help="per-worker result buffer")
     ap.add_argument("--hbm-gb", type=float, default=8.0, help="admission budget")
+    ap.add_argument("--batch", type=int, default=8,
+                    help="a third form: batched, with up to this many arrived queries of one plan per launch (<= 1: none)")
     a = ap.parse_args()
     t0 = time.perf_counter()
     tables = make_tables(a.tables, int(a.min_rows), int(a.max_rows), seed=5)
@@ -387,9 +389,9 @@ def main():
         run_native(tables, prepared[:200], arrays, "plain", **kw)
         ref = None
         for rep in range(a.repeats):
-            for mode in ("plain", "batched"):
+            for mode, batch in [("plain", 1), ("batched", 1)] + ([("batched", a.batch)] if a.batch > 1 else []):
                 torch.cuda.synchronize()
-                st = run_native(tables, prepared, arrays, mode, **kw)
+                st = run_native(tables, prepared, arrays, mode, batch=batch, **kw)
                 dig = {qid: (r.checksum, r.fsum, r.cap) for qid, r in st.results.items()}
                 same = None
                 if ref is not None:
@@ -397,7 +399,8 @@ def main():
                                for q in ref)
                 else:
                     ref = dig
-                print(json.dumps({"form": mode, "repeat": rep, "qps": round(st.qps, 1), "p50_ms": round(st.p50_ms, 3),
+                print(json.dumps({"form": mode, "batch": batch, "repeat": rep, "qps": round(st.qps, 1),
+                                  "p50_ms": round(st.p50_ms, 3),
                                   "p99_ms": round(st.p99_ms, 3), "completed": st.completed,
                                   "overflow_reruns": st.overflow_reruns,
                                   "groups": int(sum(r.groups for r in st.results.values())),
