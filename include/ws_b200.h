@@ -171,6 +171,19 @@ int ws_exec_create(const ws_agg_plan* plan, int64_t capacity, const ws_dense_spe
 int ws_exec_run(ws_executor* ex, const ws_expr_env* env);
 int ws_exec_results(ws_executor* ex, const double** keys, const int64_t** exact, const ws_fetch_status** status);
 void ws_exec_destroy(ws_executor* ex);
+/* Several prepared queries run as one (no counterpart in the reference): one CUDA graph that resets
+ * every query's result rows, runs ONE multi-query scan over all of them (as ws_agg_run_many) and then
+ * delivers each query's groups and status into its own executor's pinned memory (read them with
+ * ws_exec_results).  The executors must share one compiled plan (`jit`) and a scan kind with a
+ * multi-query form (hash, dense private rows, no keys; direct loads): WS_ERR_ARG otherwise.
+ * ws_exec_group_run takes one env per executor, in the order given at creation, each with the
+ * expressions of its executor's; it first waits until the group's previous run has read its
+ * constants.  While a group runs, its executors must not run on their own; destroy the group before
+ * its executors, from the thread whose stream ran it. */
+typedef struct ws_exec_group ws_exec_group;
+int ws_exec_group_create(ws_executor* const* exs, int n, const ws_jit_program* jit, ws_exec_group** out);
+int ws_exec_group_run(ws_exec_group* g, const ws_expr_env* const* envs);
+void ws_exec_group_destroy(ws_exec_group* g);
 
 /* Without GROUP BY: which slots hold exact int64 bits (GpuAggregator::sumBitsSlots) and the high 64 bits
  * of the exact integer sums (GpuAggregator::sumHigh; valid after ws_agg_fetch). */

@@ -1,7 +1,9 @@
 """Prepared queries (ws_exec_*): a query built once with a CUDA graph and run with new constants each
 time gives exactly the groups of the ordinary path (create / add / run / fetch) for the same
 constants — hash, dense and no-key plans; overflow is reported in the status; other expressions are
-refused.  Prints the per-query latency of the three forms on the 1M-row filter + GROUP BY."""
+refused.  Prints the per-query latency of the three forms on the 1M-row filter + GROUP BY.  A group of
+prepared queries of one plan (one graph, one multi-query scan) gives each query's groups as alone."""
+import ctypes
 import struct
 import time
 
@@ -173,3 +175,91 @@ def test_latency_of_the_three_forms(fg):
             b.close()
     finally:
         ops.jit_set_mode(-1)
+
+
+@pytest.mark.parametrize("kind", ["hash", "dense", "nokeys"])
+def test_group_of_prepared_queries_equals_each_alone(kind):
+    """Prepared queries of one compiled plan over tables of uneven size, run as one group (one graph,
+    one multi-query scan): every query's groups equal the ordinary path's for its own constants, on two
+    runs with different constants; other expressions are refused.  Prints the latency of 6 queries run
+    one by one against the group."""
+    tables = []
+    for n, seed in ((1 << 20, 0), (300_001, 1), (2_500_000, 2), (70_000, 3), (1_200_000, 4), (1 << 20, 5)):
+        t = W.pricing_summary(n, seed=seed) if kind != "hash" else W.filter_groupby_1m(n, seed=seed)
+        t.to_device()
+        tables.append(t)
+    ops.jit_set_mode(abi.JIT_SYNC)
+    exs, group = [], None
+    try:
+        qs = []
+        for t in tables:
+            if kind == "hash":
+                e, aq = W.filter_groupby_1m_query(t)
+                ds, cap, c0 = None, 1024, 500_000
+            elif kind == "dense":
+                e, aq, ds = W.pricing_summary_query(t)
+                cap, c0 = 1024, 2467
+            else:
+                e = W.env_for(t)
+                aq = q.AggQuery(e, q.col(0).le(2467), [],
+                                [q.Agg("COUNT"), q.Agg("SUM", q.col(2) * (q.ilit(100) - q.col(3)), "BIGINT", False),
+                                 q.Agg("MIN", q.col(2), "BIGINT", True)])
+                ds, cap, c0 = None, 1, 2467
+            qs.append((t, e, aq, ds, cap, const_index(e.env, c0), E.batch_arrays(t.batches(True))))
+        fn = {"hash": abi.JF_GROUPED, "dense": abi.JF_DENSE, "nokeys": abi.JF_NOKEYS}[kind]
+        e0, aq0 = qs[0][1], qs[0][2]
+        prog = ops.jit_get(e0.env, e0.ncols, aq0.plan, fn, "exec group")
+        assert prog
+        exs = [ops.Executor(aq.plan, cap, ds, e.env, e.ncols, arrays, prog, 64) for _, e, aq, ds, cap, _, arrays in qs]
+        group = ops.ExecGroup(exs, prog)
+        if kind == "hash":
+            cuts = ([500_000, 1, 999_999, 250_000, 0, 777_777], [3, 600_000, 500_000, 999_999, 120_000, 1])
+        else:
+            cuts = ([2467, 100, 2556, 1500, 2000, 0], [1, 2467, 800, 2556, 2300, 1200])
+        for rnd in cuts:
+            for (t, e, aq, ds, cap, ci, arrays), c in zip(qs, rnd):
+                set_int_const(e.env, ci, c)
+            group.run([e.env for _, e, *_ in qs])
+            ops.sync()
+            for ex, (t, e, aq, ds, cap, ci, arrays) in zip(exs, qs):
+                k, x, st = ex.results()
+                ovf, rk, rx = ordinary(aq.plan, cap, ds, e.env, e.ncols, arrays, prog)
+                assert not ovf and st["overflow"] == 0 and st["error"] == 0
+                assert st["groups"] == rk.shape[0]
+                same_groups(aq.plan, k, x, rk, rx)
+        # other expressions are refused
+        bad = abi.ExprEnv()
+        ctypes.memmove(ctypes.addressof(bad), ctypes.addressof(qs[0][1].env), ctypes.sizeof(bad))
+        bad.code[0].op = (bad.code[0].op + 1) % 250
+        with pytest.raises(ops.WsError) as ei:
+            group.run([bad] + [e.env for _, e, *_ in qs[1:]])
+        assert ei.value.code == 1210
+        # latency: the six queries one by one, against the group
+        n = 50
+
+        def alone():
+            for ex, (_, e, *_r) in zip(exs, qs):
+                ex.run(e.env)
+            ops.sync()
+
+        def together():
+            group.run([e.env for _, e, *_ in qs])
+            ops.sync()
+
+        out = {}
+        for name, f in (("one by one", alone), ("group", together)):
+            for _ in range(5):
+                f()
+            t0 = time.perf_counter()
+            for _ in range(n):
+                f()
+            out[name] = (time.perf_counter() - t0) / n * 1e6
+        print(f"\n[exec] {kind}: 6 prepared queries " + ", ".join(f"{k} {v:.0f} us" for k, v in out.items()))
+    finally:
+        if group is not None:
+            group.close()
+        for ex in exs:
+            ex.close()
+        ops.jit_set_mode(-1)
+        for t in tables:
+            t.free_device()

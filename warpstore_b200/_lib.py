@@ -80,6 +80,9 @@ SIGNATURES = {
     "ws_exec_run": (C.c_int, [P, P]),
     "ws_exec_results": (C.c_int, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P)]),
     "ws_exec_destroy": (None, [P]),
+    "ws_exec_group_create": (C.c_int, [P, C.c_int, P, C.POINTER(P)]),
+    "ws_exec_group_run": (C.c_int, [P, P]),
+    "ws_exec_group_destroy": (None, [P]),
     "ws_agg_sum_bits_slots": (C.c_int, [P, P]),
     "ws_agg_sum_high": (C.c_int, [P, P]),
     "ws_agg_compact": (C.c_int, [P, C.POINTER(P), C.POINTER(P), I64P]),

@@ -847,6 +847,60 @@ static void checkFlags(ws_aggregator& A, bool* overflow) {
   if (overflow) *overflow = e[1] != 0;
 }
 
+// One multi-query scan over prepared queries (ws_agg_run_many, ws_exec_group_*): the kernel of the
+// queries' common scan kind, its shared memory and block, the queries that have tiles, their CTA
+// starts (the launch's resident CTAs shared out by tiles: each query at least one CTA, at most its own
+// persistent grid, which its partial rows were sized for) and their launch descriptors.
+struct MultiPlan {
+  CUfunction f = nullptr;
+  size_t smem = 0;
+  int threads = 0;
+  std::vector<int> live;    // indices of the queries with tiles
+  std::vector<int> start;   // CTA starts, live.size() + 1
+  std::vector<Launch> L;    // per live query, ctaBase / ctaGrid left for the kernel
+};
+
+static MultiPlan planMulti(const std::vector<const PreparedScan*>& preps, const ws_jit_program* jit, const char* who) {
+  MultiPlan mp;
+  const KernelSet* ks = nullptr;
+  int multi = -1;
+  int64_t tiles = 0;
+  for (size_t i = 0; i < preps.size(); ++i) {
+    const PreparedScan& p = *preps[i];
+    if (!p.ready) continue;  // no tiles: nothing to scan
+    if (p.compiled && !jit) throw Error(std::string(who) + ": compiled queries need their plan", WS_ERR_ARG);
+    const KernelSet& k = p.compiled ? jit->kernels : interpKernels();
+    const int m = p.f == k.fn[K_NOKEYS] ? K_MULTI_NOKEYS : p.f == k.fn[K_DENSE_PRIV] ? K_MULTI_DENSE_PRIV
+                : p.f == k.fn[K_HASH] ? K_MULTI_HASH : -1;
+    if (m < 0 || !k.fn[m] || p.L.stages)
+      throw Error(std::string(who) + ": a query's scan has no multi-query form (dense shared / global rows, staged tiles)",
+                  WS_ERR_ARG);
+    if (multi >= 0 && (m != multi || &k != ks))
+      throw Error(std::string(who) + ": the queries need one scan kind and one plan (or all interpreted)", WS_ERR_ARG);
+    ks = &k, multi = m;
+    mp.smem = std::max(mp.smem, p.smem);
+    mp.threads = p.threads;
+    tiles += p.L.ntiles;
+    mp.live.push_back((int)i);
+  }
+  if (mp.live.empty()) return mp;
+  mp.f = ks->fn[multi];
+  const unsigned total = persistentGrid(mp.f, mp.smem, std::max<int64_t>(tiles, (int64_t)mp.live.size()), mp.threads);
+  mp.start.assign(mp.live.size() + 1, 0);
+  for (size_t j = 0; j < mp.live.size(); ++j) {
+    const PreparedScan& p = *preps[(size_t)mp.live[j]];
+    int64_t share = (int64_t)((double)total * (double)p.L.ntiles / (double)tiles);
+    share = std::max<int64_t>(1, std::min<int64_t>(share, std::min<int64_t>(p.grid, p.L.ntiles)));
+    mp.start[j + 1] = mp.start[j] + (int)share;
+    Launch L = p.L;
+    L.sumShift = sumShiftFor(L.ntiles, (unsigned)share);
+    L.waitLog2 = stagedWaitLog2();
+    L.ctaBase = L.ctaGrid = 0;  // set per CTA by the kernel
+    mp.L.push_back(L);
+  }
+  return mp;
+}
+
 }  // namespace ws
 
 extern "C" {
@@ -915,61 +969,25 @@ int ws_agg_run_many(ws_aggregator* const* aggs, const ws_expr_env* const* envs, 
       preps[(size_t)i].direct = true;
       aggRun(*aggs[i], *envs[i], jit, &preps[(size_t)i]);
     }
-    const KernelSet* ks = nullptr;
-    int multi = -1;
-    size_t smem = 0;
-    int threads = 0;
-    int64_t tiles = 0;
-    std::vector<int> live;
-    for (int i = 0; i < n; ++i) {
-      const PreparedScan& p = preps[(size_t)i];
-      if (!p.ready) continue;  // no tiles: nothing to scan
-      const KernelSet& k = p.compiled ? jit->kernels : interpKernels();
-      const int m = p.f == k.fn[K_NOKEYS] ? K_MULTI_NOKEYS : p.f == k.fn[K_DENSE_PRIV] ? K_MULTI_DENSE_PRIV
-                  : p.f == k.fn[K_HASH] ? K_MULTI_HASH : -1;
-      if (m < 0 || !k.fn[m] || p.L.stages)
-        throw Error("ws_agg_run_many: a query's scan has no multi-query form (dense shared / global rows, staged tiles)",
-                    WS_ERR_ARG);
-      if (multi >= 0 && (m != multi || &k != ks))
-        throw Error("ws_agg_run_many: the queries need one scan kind and one plan (or all interpreted)", WS_ERR_ARG);
-      ks = &k, multi = m;
-      smem = std::max(smem, p.smem);
-      threads = p.threads;
-      tiles += p.L.ntiles;
-      live.push_back(i);
-    }
-    if (live.empty()) return;
-    CUfunction f = ks->fn[multi];
-    // the launch's resident CTAs, shared out by the queries' tiles (each at least one CTA, at most its
-    // own persistent grid, which its partial rows were sized for)
-    const unsigned total = persistentGrid(f, smem, std::max<int64_t>(tiles, (int64_t)live.size()), threads);
-    std::vector<int> start(live.size() + 1, 0);
-    for (size_t j = 0; j < live.size(); ++j) {
-      const PreparedScan& p = preps[(size_t)live[j]];
-      int64_t share = (int64_t)((double)total * (double)p.L.ntiles / (double)tiles);
-      share = std::max<int64_t>(1, std::min<int64_t>(share, std::min<int64_t>(p.grid, p.L.ntiles)));
-      start[j + 1] = start[j] + (int)share;
-    }
-    const size_t nl = live.size();
+    std::vector<const PreparedScan*> pp;
+    for (const PreparedScan& p : preps) pp.push_back(&p);
+    const MultiPlan mp = planMulti(pp, jit, "ws_agg_run_many");
+    if (mp.live.empty()) return;
+    const size_t nl = mp.live.size();
     const size_t launchBytes = nl * sizeof(Launch), startBytes = (nl + 1) * sizeof(int);
     uint8_t* st = pinnedStage(launchBytes + startBytes);
-    for (size_t j = 0; j < nl; ++j) {
-      Launch L = preps[(size_t)live[j]].L;
-      L.sumShift = sumShiftFor(L.ntiles, (unsigned)(start[j + 1] - start[j]));
-      L.waitLog2 = stagedWaitLog2();
-      L.ctaBase = L.ctaGrid = 0;  // set per CTA by the kernel
-      memcpy(st + j * sizeof(Launch), &L, sizeof(Launch));
+    memcpy(st, mp.L.data(), launchBytes);
+    memcpy(st + launchBytes, mp.start.data(), startBytes);
+    for (const Launch& L : mp.L)
       if (L.ticket) WS_CK(cudaMemsetAsync(L.ticket, 0, 4, stream()));
-    }
-    memcpy(st + launchBytes, start.data(), startBytes);
     DBuf<uint8_t> dl((int64_t)(launchBytes + startBytes));
     h2dAsync(dl.p, st, launchBytes + startBytes);
     stageCopied();
     MultiLaunch M{(const Launch*)dl.p, (const int*)(dl.p + launchBytes), (int)nl};
-    allowDynamicSmem(f, smem);
+    allowDynamicSmem(mp.f, mp.smem);
     void* args[] = {(void*)&M};
-    WS_CKD(drv().launchKernel(f, (unsigned)start[nl], 1, 1, (unsigned)threads, 1, 1, (unsigned)smem, (CUstream)stream(),
-                              args, nullptr));
+    WS_CKD(drv().launchKernel(mp.f, (unsigned)mp.start[nl], 1, 1, (unsigned)mp.threads, 1, 1, (unsigned)mp.smem,
+                              (CUstream)stream(), args, nullptr));
     countLaunch();
   });
 }
@@ -1138,6 +1156,29 @@ struct ws_executor {
 };
 
 namespace {
+// Queues on this thread's stream the part of a prepared query after its scan: compaction of the
+// result rows, the status word and the groups written into the executor's pinned memory.
+void queueExecTail(ws_executor& X) {
+  ws_aggregator& A = *X.A;
+  const int nk = A.plan.nkeys, na = A.plan.naggs;
+  double* dk = nullptr;
+  long long* dx = nullptr;
+  ws_fetch_status* dst = nullptr;
+  WS_CK(cudaHostGetDevicePointer((void**)&dk, X.keys, 0));
+  WS_CK(cudaHostGetDevicePointer((void**)&dx, X.exact, 0));
+  WS_CK(cudaHostGetDevicePointer((void**)&dst, X.st, 0));
+  const int64_t nr = A.nrows();
+  const OccSpec o{A.lay.rw, nk == 0 ? 0 : A.isDense ? 1 : 2, A.lay.woff[0], A.cap};
+  const int64_t nchunks = (nr + kOccChunk - 1) / kOccChunk;
+  const int rowBytes = 8 * (nk + 2 * na);
+  const int threads = std::max(32, std::min(256, (32768 / rowBytes) & ~31));
+  WS_LAUNCH(kOccCount, (unsigned)nchunks, 256, 0, A.rows.p, nr, o, X.offs.p);
+  WS_LAUNCH(kScanExclusive, 1, 1024, 0, X.offs.p, nchunks);
+  WS_LAUNCH(kFetchStatus, 1, 1, 0, X.offs.p + nchunks, A.err(), o.mode == 2 ? 1 : 0, dst);
+  WS_LAUNCH(kOccEmitHost, (unsigned)nchunks, threads, (size_t)threads * rowBytes, A.rows.p, nr, o, emitSpec(A), X.offs.p,
+            nchunks, A.err(), (int64_t)0, X.maxGroups, dk, dx);
+}
+
 uint64_t codeDigest(const ws_expr_env& env) {
   uint64_t h = 0xcbf29ce484222325ull;
   const unsigned char* b = (const unsigned char*)env.code;
@@ -1175,19 +1216,7 @@ int ws_exec_create(const ws_agg_plan* plan, int64_t capacity, const ws_dense_spe
     pinned(sizeof(double) * max_groups * std::max(nk, 1), (void**)&X->keys);
     pinned(sizeof(int64_t) * max_groups * na * 2, (void**)&X->exact);
     pinned(sizeof(ws_fetch_status), (void**)&X->st);
-    double* dk = nullptr;
-    long long* dx = nullptr;
-    ws_fetch_status* dst = nullptr;
-    WS_CK(cudaHostGetDevicePointer((void**)&dk, X->keys, 0));
-    WS_CK(cudaHostGetDevicePointer((void**)&dx, X->exact, 0));
-    WS_CK(cudaHostGetDevicePointer((void**)&dst, X->st, 0));
-    const int64_t nr = A.nrows();
-    const OccSpec o{A.lay.rw, nk == 0 ? 0 : A.isDense ? 1 : 2, A.lay.woff[0], A.cap};
-    const int64_t nchunks = (nr + kOccChunk - 1) / kOccChunk;
-    X->offs = DBuf<int64_t>(nchunks + 1);
-    const int rowBytes = 8 * (nk + 2 * na);
-    const int threads = std::max(32, std::min(256, (32768 / rowBytes) & ~31));
-    const EmitSpec es = emitSpec(A);
+    X->offs = DBuf<int64_t>((A.nrows() + kOccChunk - 1) / kOccChunk + 1);
     sync();  // the preparation's copies and allocations are done before the capture starts
     // capture on a private stream (nothing else of this thread's work joins the graph)
     cudaStream_t cs = nullptr;
@@ -1216,11 +1245,7 @@ int ws_exec_create(const ws_agg_plan* plan, int64_t capacity, const ws_dense_spe
         X->scanNode = deps[0];
         ++X->kernels;
       }
-      WS_LAUNCH(kOccCount, (unsigned)nchunks, 256, 0, A.rows.p, nr, o, X->offs.p);
-      WS_LAUNCH(kScanExclusive, 1, 1024, 0, X->offs.p, nchunks);
-      WS_LAUNCH(kFetchStatus, 1, 1, 0, X->offs.p + nchunks, A.err(), o.mode == 2 ? 1 : 0, dst);
-      WS_LAUNCH(kOccEmitHost, (unsigned)nchunks, threads, (size_t)threads * rowBytes, A.rows.p, nr, o, es, X->offs.p,
-                nchunks, A.err(), (int64_t)0, max_groups, dk, dx);
+      queueExecTail(*X);
       X->kernels += 4;
       capturing = false;
       WS_CK(cudaStreamEndCapture(cs, &X->graph));
@@ -1272,6 +1297,131 @@ int ws_exec_results(ws_executor* X, const double** keys, const int64_t** exact, 
 }
 
 void ws_exec_destroy(ws_executor* X) { delete X; }
+
+}  // extern "C"
+
+// Prepared queries of one plan run together (ws_exec_group_*): one CUDA graph that resets every
+// query's result rows, copies the queries' launch descriptors from pinned memory (each run writes the
+// new constants there first), runs ONE multi-query scan over all of them and then each query's
+// compaction and delivery into its own executor's pinned memory.
+struct ws_exec_group {
+  std::vector<ws_executor*> xs;
+  ws::MultiPlan mp;
+  uint8_t* stage = nullptr;  // pinned: [Launch per live query][CTA starts]
+  size_t stageBytes = 0;
+  ws::DBuf<uint8_t> dl;      // the device copy the scan reads
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t done = nullptr;  // the last run's end: its copy of `stage` has been made
+  int kernels = 0;
+  ~ws_exec_group() {
+    if (done) cudaEventSynchronize(done);
+    cudaStreamSynchronize(ws::stream());
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (done) cudaEventDestroy(done);
+    if (stage) cudaFreeHost(stage);
+  }
+};
+
+extern "C" {
+
+int ws_exec_group_create(ws_executor* const* xs, int n, const ws_jit_program* jit, ws_exec_group** out) {
+  return guardedCall([&] {
+    *out = nullptr;
+    if (n < 1 || n > 1024 || !xs) throw Error("exec group: 1..1024 prepared queries", WS_ERR_ARG);
+    std::unique_ptr<ws_exec_group> G(new ws_exec_group);
+    std::vector<const PreparedScan*> pp;
+    for (int i = 0; i < n; ++i) {
+      if (!xs[i]) throw Error("exec group: a null prepared query", WS_ERR_ARG);
+      for (int j = 0; j < i; ++j)
+        if (xs[j] == xs[i]) throw Error("exec group: a prepared query given twice", WS_ERR_ARG);
+      G->xs.push_back(xs[i]);
+      pp.push_back(&xs[i]->ps);
+    }
+    G->mp = planMulti(pp, jit, "exec group");
+    const MultiPlan& mp = G->mp;
+    const size_t nl = mp.live.size();
+    const size_t launchBytes = nl * sizeof(Launch), startBytes = (nl + 1) * sizeof(int);
+    G->stageBytes = launchBytes + startBytes;
+    if (cudaHostAlloc((void**)&G->stage, std::max<size_t>(G->stageBytes, 8), cudaHostAllocDefault) != cudaSuccess) {
+      cudaGetLastError();
+      G->stage = nullptr;
+      throw Error("exec group: pinned descriptor buffer", WS_ERR_OOM);
+    }
+    if (nl) {
+      memcpy(G->stage, mp.L.data(), launchBytes);
+      memcpy(G->stage + launchBytes, mp.start.data(), startBytes);
+      G->dl = DBuf<uint8_t>((int64_t)G->stageBytes);
+    }
+    WS_CK(cudaEventCreateWithFlags(&G->done, cudaEventDisableTiming));
+    sync();  // allocations done before the capture starts
+    cudaStream_t cs = nullptr;
+    WS_CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaStream_t prev = stream();
+    auto restore = [&] { ws_set_stream(prev == cudaStreamPerThread ? nullptr : (void*)prev); };
+    ws_set_stream(cs);
+    const int64_t launches0 = ws_kernel_launches();
+    bool capturing = false;
+    try {
+      WS_CK(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+      capturing = true;
+      for (ws_executor* X : G->xs) aggResetRows(*X->A);
+      if (nl) {
+        WS_CK(cudaMemcpyAsync(G->dl.p, G->stage, G->stageBytes, cudaMemcpyHostToDevice, cs));
+        for (const Launch& L : mp.L)
+          if (L.ticket) WS_CK(cudaMemsetAsync(L.ticket, 0, 4, cs));
+        MultiLaunch M{(const Launch*)G->dl.p, (const int*)(G->dl.p + launchBytes), (int)nl};
+        allowDynamicSmem(mp.f, mp.smem);
+        void* args[] = {(void*)&M};
+        WS_CKD(drv().launchKernel(mp.f, (unsigned)mp.start[nl], 1, 1, (unsigned)mp.threads, 1, 1, (unsigned)mp.smem,
+                                  (CUstream)cs, args, nullptr));
+        countLaunch();
+      }
+      for (ws_executor* X : G->xs) queueExecTail(*X);
+      capturing = false;
+      WS_CK(cudaStreamEndCapture(cs, &G->graph));
+      WS_CK(cudaGraphInstantiate(&G->exec, G->graph, 0));
+    } catch (...) {
+      if (capturing) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(cs, &g);
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+      }
+      restore();
+      cudaStreamDestroy(cs);
+      throw;
+    }
+    G->kernels = (int)(ws_kernel_launches() - launches0);
+    countLaunch(-G->kernels);  // captured, not launched
+    restore();
+    WS_CK(cudaStreamDestroy(cs));
+    *out = G.release();
+  });
+}
+
+int ws_exec_group_run(ws_exec_group* G, const ws_expr_env* const* envs) {
+  return guardedCall([&] {
+    if (!envs) throw Error("exec group: no constants", WS_ERR_ARG);
+    for (size_t i = 0; i < G->xs.size(); ++i)
+      if (!envs[i] || codeDigest(*envs[i]) != G->xs[i]->code)
+        throw Error("exec group: query " + std::to_string(i) + "'s expressions differ from its prepared query's",
+                    WS_ERR_ARG);
+    // the previous run's graph copies `stage` when it runs: wait for it before overwriting
+    WS_CK(cudaEventSynchronize(G->done));
+    for (size_t j = 0; j < G->mp.live.size(); ++j) {
+      Launch L = G->mp.L[j];
+      L.env = envK(*envs[(size_t)G->mp.live[j]]);
+      memcpy(G->stage + j * sizeof(Launch), &L, sizeof(Launch));
+    }
+    WS_CK(cudaGraphLaunch(G->exec, stream()));
+    WS_CK(cudaEventRecord(G->done, stream()));
+    countLaunch(G->kernels);
+  });
+}
+
+void ws_exec_group_destroy(ws_exec_group* G) { delete G; }
 
 int ws_host_alloc(size_t bytes, void** out) {
   return guardedCall([&] {

@@ -219,6 +219,35 @@ class Executor:
             pass
 
 
+class ExecGroup:
+    """Prepared queries of one compiled plan run as one graph with one multi-query scan
+    (ws_exec_group_*): run(envs) queues them with one env each; each Executor's results() reads its
+    groups after sync().  Close the group before its executors."""
+
+    def __init__(self, executors: list, jit: int):
+        self.executors = list(executors)
+        self.h = None
+        arr = (P * len(self.executors))(*[x.h for x in self.executors])
+        h = P()
+        check(lib().ws_exec_group_create(arr, len(self.executors), jit, C.byref(h)))
+        self.h = h.value
+
+    def run(self, envs: list):
+        arr = (P * len(envs))(*[C.addressof(e) for e in envs])
+        check(lib().ws_exec_group_run(self.h, arr))
+
+    def close(self):
+        if self.h:
+            lib().ws_exec_group_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class GpuAggregator:
     """GPU aggregation state of one query (src/gpu.h:84-130)."""
 
