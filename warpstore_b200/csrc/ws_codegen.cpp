@@ -264,6 +264,7 @@ std::string genEvaluator(const ws_expr_env& env, int ncols, const ws_agg_plan& p
     return v >= 1 && v <= 4 ? v : 2;
   }();
   o << "  static constexpr int PRIV_MIN_BLOCKS = " << privMinBlocks << ";\n";
+  o << "  static constexpr int HASH_MULTI_MIN_BLOCKS = 3;\n";  // the multi-query hash scan's register bound
   o << "  static constexpr int NSC = " << std::max<size_t>(staged.size(), 1) << ", STAGE_BYTES = " << stageBytes << ";\n";
   o << "  struct Stage { const unsigned char* d[NSC]; int w[NSC]; unsigned bytes; int ok; };\n";
   o << "  __device__ static void stageBind(const ws::Launch& l, int b, Stage& st) {\n";

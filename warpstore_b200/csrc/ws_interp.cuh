@@ -172,6 +172,7 @@ static __device__ __noinline__ Word vmRun(const TInstr* code, int start, int len
 struct InterpEv {
   static constexpr int NK = WS_INTERP_KEYS, NA = WS_INTERP_AGGS, RW = 1 + 2 * WS_INTERP_AGGS, FRW = WS_INTERP_AGGS;
   static constexpr int PRIV_MIN_BLOCKS = 1;  // the VM needs its registers
+  static constexpr int HASH_MULTI_MIN_BLOCKS = 1;
   static constexpr bool STAGED = false;
   static constexpr int STAGE_BYTES = 0;
   const Launch& L;

@@ -984,7 +984,12 @@ __device__ void selectWrite(const Launch& L) {
 #define WS_K_MULTI_NOKEYS(EV, PREFIX) WS_K_MULTI_B(PREFIX, nokeys, ws::aggNoKeys<EV>, ws::kStagedThreads, 1)
 #define WS_K_MULTI_DENSE_PRIV(EV, PREFIX) \
   WS_K_MULTI_B(PREFIX, dense_priv, (ws::aggDensePriv<EV, false>), ws::kThreads, EV::PRIV_MIN_BLOCKS)
-#define WS_K_MULTI_HASH(EV, PREFIX) WS_K_MULTI_B(PREFIX, hash, ws::aggHash<EV>, ws::kStagedThreads, 1)
+// The hash scan launches kThreads.  For generated plans EV::HASH_MULTI_MIN_BLOCKS = 3 resident CTAs
+// (the shared table allows them) bound the registers: reading the launch descriptor from shared
+// memory took the kernel from 72 to 82 registers, two CTAs per SM and 20 % more time than the
+// single-query scan; bounded it needs 80, without spills.
+#define WS_K_MULTI_HASH(EV, PREFIX) \
+  WS_K_MULTI_B(PREFIX, hash, ws::aggHash<EV>, ws::kThreads, EV::HASH_MULTI_MIN_BLOCKS)
 #define WS_K_NOKEYS(EV, PREFIX) WS_K_ENTRY(PREFIX, nokeys, ws::aggNoKeys<EV>)
 #define WS_K_DENSE_SHARED(EV, PREFIX) WS_K_ENTRY(PREFIX, dense_shared, ws::aggDenseShared<EV>)
 #define WS_K_DENSE_GLOBAL(EV, PREFIX) WS_K_ENTRY(PREFIX, dense_global, ws::aggDenseGlobal<EV>)
