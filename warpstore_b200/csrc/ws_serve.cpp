@@ -168,7 +168,11 @@ int64_t initialCap(const ws_serve_query& q, const ws_serve_options& o) {
     // log2(1 + groups) floored at log2(1 + 1024), the smallest capacity (as estimator.Model.gated)
     const double floorLog2 = std::log2(1025.0);
     const double corr = std::fabs(y) > w->gate ? (double)y : 0.0;
-    const double pred = std::exp2(std::max(std::max((double)x[kGroupFeatures - 1], floorLog2) + corr, floorLog2)) - 1;
+    // at most the passing rows (the sample's fraction of the table) and the key range, as estimator.Model
+    const double upper = std::min(std::log2(1 + (double)passing * (double)total / (double)std::max<int64_t>(sampled, 1)),
+                                  (double)x[4]);
+    const double pred =
+        std::exp2(std::max(std::min(std::max((double)x[kGroupFeatures - 1], floorLog2) + corr, upper), floorLog2)) - 1;
     cap = std::min(cap, pow2AtLeast(2 * pred * w->margin, 1024));
   }
   return cap;

@@ -286,14 +286,27 @@ class Model:
         h = np.maximum(h @ from_bf16(self.w2) + self.b2, 0)
         return h @ from_bf16(self.w3) + np.float32(self.b3)
 
+    def upper_log2(self, x: np.ndarray) -> np.ndarray:
+        """What the count cannot exceed, from the features: a GROUP BY has at most as many groups as
+        rows pass (the sample's passing fraction of the table) and as key values (the key range); a
+        filter passes at most the table's rows."""
+        x = x.astype(np.float64)
+        if self.target == "groups":
+            passing, sampled, total = np.exp2(x[:, 1]) - 1, np.exp2(x[:, 2]) - 1, np.exp2(x[:, 3]) - 1
+            return np.minimum(np.log2(1 + passing * total / np.maximum(sampled, 1)), x[:, 4])
+        if self.target == "rows":
+            return x[:, 8]
+        return np.full(x.shape[0], np.inf)
+
     def gated(self, x: np.ndarray, corr: np.ndarray) -> np.ndarray:
         corr = np.asarray(corr, dtype=np.float64)
         base = np.maximum(x[:, -1].astype(np.float64), FLOOR_LOG2)
-        return np.maximum(base + np.where(np.abs(corr) > self.gate, corr, 0.0), FLOOR_LOG2)
+        pred = np.minimum(base + np.where(np.abs(corr) > self.gate, corr, 0.0), self.upper_log2(x))
+        return np.maximum(pred, FLOOR_LOG2)
 
     def predict_log2_np(self, x: np.ndarray) -> np.ndarray:
         """log2(1 + count), floored at 1024: the plain estimate (last feature) plus the gated MLP
-        correction."""
+        correction, at most upper_log2."""
         x = np.atleast_2d(x)
         return self.gated(x, self.forward_np(x))
 
