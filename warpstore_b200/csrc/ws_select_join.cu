@@ -117,11 +117,16 @@ __device__ __forceinline__ bool joinKeyStream(const ws_col_view& c, int64_t r, l
   return d == d;
 }
 
-// Hash table: buckets of 4 keys, one 32-byte sector each (key ^ 2^63; 0 = empty), and the build row of
-// slot i in a parallel int32 array read only when slot i matched.  The bucket of a key is the low 32
-// bits of its hash scaled to the bucket count (any count: the table is sized to the keys, not to a
-// power of two); a full bucket overflows into the next one, so a probe walks buckets from the key's
-// own until one has an empty slot.  A probe costs one 256-bit load when its bucket is not full.
+// Hash table: buckets of 64 bytes, each 4 keys in its first 32-byte sector (key ^ 2^63; 0 = empty) and
+// their 4 build rows (int32) in the second, read only when a slot matched.  A random DRAM access brings
+// 64 bytes whatever is asked for, so the rows beside the keys arrive with them: a match's row is an L2
+// hit instead of a second random DRAM access (rows in a separate array cost ~117 DRAM bytes per probe).
+// The bucket of a key is the low 32 bits of its hash scaled to the bucket count (any count: the table
+// is sized to the keys, not to a power of two); a full bucket overflows into the next one, so a probe
+// walks buckets from the key's own until one has an empty slot.  A probe costs one 256-bit load when
+// its bucket is not full.
+constexpr u64 kJBucketWords = 8;  // u64 words per bucket: keys [0, 4), rows as int32 in [4, 6)
+constexpr u64 kJRowStride = 16;   // int32 per bucket, for the rows' view of the table (starting at word 4)
 __device__ __forceinline__ u64 jBucket(u64 h, u64 nbuckets) {
   return nbuckets <= 0xffffffffull ? (u64)__umulhi((unsigned)h, (unsigned)nbuckets)
                                    : ((h & 0xffffffffull) * nbuckets) >> 32;
@@ -211,7 +216,7 @@ __global__ void kJoinBuild(ws_col_view key, int64_t base, int64_t n, JPass jp, u
     u64 b = jBucket(h, nbuckets);
     bool done = false;
     for (u64 step = 0; step < nbuckets && !done; ++step) {
-      u64* bk = keys + b * 4;
+      u64* bk = keys + b * kJBucketWords;
       // the bucket through L2 (other threads' inserts are visible there); a slot seen empty may have been
       // taken since: the CAS decides, and a lost CAS moves on to the next slot
       const ulonglong2 lo = __ldcg((const ulonglong2*)bk), hi = __ldcg((const ulonglong2*)bk + 1);
@@ -220,7 +225,7 @@ __global__ void kJoinBuild(ws_col_view key, int64_t base, int64_t n, JPass jp, u
       for (int q = 0; q < 4; ++q) {
         if (done || seen[q] != 0ull) continue;
         if (atomicCAS((unsigned long long*)(bk + q), 0ull, sk) == 0ull) {
-          rows[b * 4 + q] = (int)(base + i);
+          rows[b * kJRowStride + q] = (int)(base + i);
           done = true;
         }
       }
@@ -375,7 +380,7 @@ __device__ __forceinline__ void jWalk(const JOut& out, int2* st, int& fill, cons
       if (has) {
         const int s = __ffs(e.m) - 1;
         e.m &= e.m - 1;
-        r = __ldg(rows + e.bucket * 4 + s);
+        r = __ldg(rows + e.bucket * kJRowStride + s);
         e.flags |= 2;
         if (out.matched) out.matched[r - out.rowBase] = 1;
       }
@@ -386,7 +391,7 @@ __device__ __forceinline__ void jWalk(const JOut& out, int2* st, int& fill, cons
       if ((e.flags & 1) && ++steps < nbuckets) {
         e.bucket = e.bucket + 1 == nbuckets ? 0 : e.bucket + 1;
         u64 k4[4];
-        ldBucket(keys + e.bucket * 4, pol, k4);
+        ldBucket(keys + e.bucket * kJBucketWords, pol, k4);
 #pragma unroll
         for (int s = 0; s < 4; ++s) e.m |= (unsigned)(k4[s] == e.sk) << s;
         e.flags = (e.flags & 2) | (k4[0] && k4[1] && k4[2] && k4[3] ? 1 : 0);
@@ -429,7 +434,7 @@ __global__ void __launch_bounds__(kJThreads) kJoinProbe(ws_col_view key, int64_t
     // round 2: first buckets
 #pragma unroll
     for (int j = 0; j < kJHashPer; ++j)
-      if (act[j]) ldBucket(keys + bk[j] * 4, pol, slot[j]);
+      if (act[j]) ldBucket(keys + bk[j] * kJBucketWords, pol, slot[j]);
     // round 3: the build row of each key's first matching slot
     unsigned m[kJHashPer];
     bool more[kJHashPer];
@@ -443,7 +448,7 @@ __global__ void __launch_bounds__(kJThreads) kJoinProbe(ws_col_view key, int64_t
         for (int q = 0; q < 4; ++q) m[j] |= (unsigned)(slot[j][q] == sk[j]) << q;
         more[j] = slot[j][0] && slot[j][1] && slot[j][2] && slot[j][3];  // full: the run may go on
       }
-      row[j] = m[j] ? __ldg(rows + bk[j] * 4 + (__ffs(m[j]) - 1)) : 0;
+      row[j] = m[j] ? __ldg(rows + bk[j] * kJRowStride + (__ffs(m[j]) - 1)) : 0;
     }
     // round 4: stage the first matches (and an outer join's unmatched rows whose run ended); queue the rest
 #pragma unroll
@@ -499,7 +504,7 @@ int64_t joinTableBudget() {
 // Hash join table slots for `keys` build keys: 2 per key (load 1/2: a bucket of 4 is full for about
 // 1 key in 7), a multiple of the 4-slot bucket with at least one spare bucket;
 // WARPSTORE_B200_JOIN_SLOTS_PER_KEY = 2..16 fixes the factor.
-constexpr int64_t kJSlotBytes = 8 + 4;  // key + build row
+constexpr int64_t kJSlotBytes = 16;  // a 64-byte bucket of 4 slots
 int64_t joinTableSlots(int64_t keys) {
   static const int64_t fixed = [] {
     const char* e = getenv("WARPSTORE_B200_JOIN_SLOTS_PER_KEY");
@@ -814,8 +819,10 @@ static int joinImpl(ws_col_view build_key, const int64_t* boff, int pb, ws_col_v
     }
     bool anyDense = false, anyHash = false;
     for (int q = 0; q < pb; ++q) anyDense |= dense[q] != 0, anyHash |= !cap[q].empty();
-    DBuf<u64> tkeys(anyHash ? tableSlots : 4);
-    DBuf<int> trows(anyHash ? tableSlots : 4);
+    // one table of 64-byte buckets (keys, then rows: kJBucketWords)
+    DBuf<u64> table(anyHash ? tableSlots / 4 * kJBucketWords : kJBucketWords);
+    u64* tkeys = table.p;
+    int* trows = (int*)(table.p + 4);
     DBuf<int> dtable(anyDense ? denseSlots : 1), next(anyDense ? nextRows : 1);
     DBuf<int> flags(2);  // [0] hash table full, [1] duplicate dense keys
     WS_CK(cudaMemsetAsync(flags.p, 0, 8, stream()));
@@ -852,8 +859,8 @@ static int joinImpl(ws_col_view build_key, const int64_t* boff, int pb, ws_col_v
             WS_LAUNCH(kJoinDenseBuild, gridFor(nbq), 256, 0, build_key, boff[q], nbq, dtable.p, kmin[q], next.p,
                       flags.p + 1);
           } else {
-            WS_CK(cudaMemsetAsync(tkeys.p, 0, 8 * c, stream()));
-            WS_LAUNCH(kJoinBuild, gridFor(nbq), 256, 0, build_key, boff[q], nbq, jp, tkeys.p, trows.p, (u64)(c / 4),
+            WS_CK(cudaMemsetAsync(tkeys, 0, 8 * kJBucketWords * (c / 4), stream()));
+            WS_LAUNCH(kJoinBuild, gridFor(nbq), 256, 0, build_key, boff[q], nbq, jp, tkeys, trows, (u64)(c / 4),
                       flags.p);
           }
           for (int p = 0; p < pp; ++p) {  // probe partitions joined with build partition q
@@ -867,7 +874,7 @@ static int joinImpl(ws_col_view build_key, const int64_t* boff, int pb, ws_col_v
               WS_LAUNCH(kJoinDenseProbe, grid, kJThreads, 0, probe_key, poff[p], n, dtable.p, kmin[q], range[q], next.p,
                         boff[q], flags.p + 1, jo);
             else
-              WS_LAUNCH(kJoinProbe, hgrid, kJThreads, 0, probe_key, poff[p], n, jp, tkeys.p, trows.p, (u64)(c / 4), jo);
+              WS_LAUNCH(kJoinProbe, hgrid, kJThreads, 0, probe_key, poff[p], n, jp, tkeys, trows, (u64)(c / 4), jo);
           }
         }
       }
