@@ -228,7 +228,10 @@ int ws_hash_join(ws_col_view build_key, int64_t nb, ws_col_view probe_key, int64
                  int32_t** out_probe, int64_t* m);
 /* ws_hash_join with the pair buffers' first capacity chosen by the caller (a predicted pair count, for
  * instance) instead of the probe rows: a join that emits more pairs runs a second time with exact sizes,
- * so only the memory held and *attempts (1 or 2) depend on it, never the pairs. */
+ * so only the memory held and *attempts (1 or 2) depend on it, never the pairs.  A first capacity below
+ * 0.35 x the probe rows also says that most probe rows find no match: a hash-table join of 2^20 build
+ * keys or more then builds a key filter (16 bits per key, held by L2) that spares those rows their
+ * table access. */
 int ws_hash_join_sized(ws_col_view build_key, int64_t nb, ws_col_view probe_key, int64_t np, int64_t first_capacity,
                        int32_t** out_build, int32_t** out_probe, int64_t* m, int* attempts);
 /* gpuHashJoinOuter (src/gpu.h:187-188): every probe row appears, with build row -1 when it matched

@@ -168,6 +168,61 @@ def test_hash_join_multipass_matches_single_pass():
     assert int(r.stdout.strip().splitlines()[-1]) > 0
 
 
+FILTER_CASES = r"""
+from tests.test_select_join_gpu import join_case, check_join
+out = []
+for nb, np_, space, dup, nulls, i32 in [(1000, 5000, 1000, False, False, False),
+                                       (100_000, 1_000_000, 400_000, False, False, False),
+                                       (50_000, 200_000, 10_000, True, True, False),
+                                       (30_000, 100_000, 30_000, False, True, True), (1, 1, 1, False, False, False),
+                                       (200_000, 600_000, 200_000, False, False, False)]:
+    bk, pk = join_case(nb, np_, space, nb + np_, dup, nulls, i32, True)
+    out.append(check_join(bk, pk, i32))
+print(" ".join(map(str, out)))
+"""
+
+
+def test_hash_join_key_filter_matches_oracle():
+    """The inner hash join's key filter (a blocked Bloom filter of the build keys that lets probes with
+    no match skip their bucket), forced on for every size: the sparse-key cases above (duplicates, NULLs,
+    int32 keys, every probe key matching) give the oracle's pairs.  A child process: the switch is read
+    once per process."""
+    import os
+    import subprocess
+    import sys
+    env = dict(os.environ, WARPSTORE_B200_JOIN_FILTER="1")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", FILTER_CASES], env=env, cwd=root, capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-3000:]
+    counts = [int(x) for x in r.stdout.strip().splitlines()[-1].split()]
+    assert len(counts) == 6 and all(c > 0 for c in counts)
+
+
+def test_sized_selective_join_uses_key_filter_same_pairs():
+    """A first pair capacity well below the probe rows (a selective join: ~10 % of 3M probe rows match
+    1.2M sparse build keys) turns the key filter on; the pairs equal the unfiltered join's."""
+    rng = np.random.default_rng(17)
+    mul = np.uint64(0x9E3779B97F4A7C15)
+    bk = (rng.permutation(12_000_000)[:1_200_000].astype(np.uint64) * mul).view(np.int64)
+    pk = (rng.integers(0, 12_000_000, 3_000_000).astype(np.uint64) * mul).view(np.int64)
+    db, dp = ops.DeviceBuffer.from_array(bk), ops.DeviceBuffer.from_array(pk)
+    bv, pv = abi.ColView(db.ptr, abi.T_I64, 0, 0, 0), abi.ColView(dp.ptr, abi.T_I64, 0, 0, 0)
+
+    def pairs(ob, op, m):
+        gb, gp = ops.device_to_array(ob, np.int32, m), ops.device_to_array(op, np.int32, m)
+        ops.tmp_free(ob)
+        ops.tmp_free(op)
+        o = np.lexsort((gb, gp))
+        return gb[o], gp[o]
+
+    want = pairs(*ops.hash_join(bv, len(bk), pv, len(pk)))
+    ob, op, m, att = ops.hash_join_sized(bv, len(bk), pv, len(pk), 400_000)
+    got = pairs(ob, op, m)
+    assert att == 1 and m == want[0].size == int(np.isin(pk, bk).sum())
+    assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+
+
 def test_hash_join_partitions():
     rng = np.random.default_rng(4)
     P = 4
