@@ -295,6 +295,12 @@ int ws_encode_column_engine(const void* src, int ptype, int64_t n, void** out, i
 int ws_hll_sketch(const ws_expr_env* env, int ncols, const ws_agg_plan* plan, int nb, const int64_t* bn,
                   const uint32_t* const* bdel, const ws_col_view* bcols, int p, int64_t sample_rows, uint32_t* regs_out,
                   int64_t* sampled, int64_t* passing);
+/* Coordinated sample of a join key column (device view of n rows; keys as the joins read them, NULLs
+ * skipped): the hashes mix64(key) below tau, copied to the host array out[0, min(count, cap)) in no
+ * order; *count = every qualifying key.  Two sides sampled with one tau keep exactly the keys of both
+ * whose hash is below it, so the join of the samples holds every pair of those keys (the estimator's
+ * join-size feature; no counterpart in the reference). */
+int ws_join_key_sample(ws_col_view key, int64_t n, uint64_t tau, uint64_t* out, int64_t cap, int64_t* count);
 /* y[r] of a 3-layer MLP over host feature rows x[rows][features]: relu(x W1 + b1) -> relu(. W2 + b2) ->
  * . W3 + b3, weights as BF16 bits (W1 [features][hidden], W2 [hidden][hidden], W3 [hidden]), biases and
  * accumulation FP32; features <= 64, hidden a multiple of 32 up to 128. */

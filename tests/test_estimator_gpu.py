@@ -2,7 +2,8 @@
 same sampled rows (and, without keys, it counts); the MLP kernel equals the FP32 forward pass over the
 BF16 weights; learned sizing of COUNT(DISTINCT)'s phase-1 table gives the plain sizing's result in fewer
 (or as many) runs; the selectivity and join-size predictions land within a factor 2; a join sized by
-its prediction, or a sparse key range moved to the hash path, gives the same pairs / groups."""
+its prediction, or a sparse key range moved to the hash path, gives the same pairs / groups; the
+coordinated join-key sample keeps exactly the keys the host definition keeps."""
 import ctypes
 
 import numpy as np
@@ -182,3 +183,33 @@ def test_sparse_key_range_takes_hash_path_same_result():
     finally:
         ops.jit_set_mode(-1)
         t.free_device()
+
+
+@pytest.mark.parametrize("i32", [False, True], ids=["int64", "int32"])
+def test_join_key_sample_matches_host_definition(i32):
+    """ws_join_key_sample keeps exactly the non-NULL keys whose hash mix64(key) is below tau (the same
+    key reading as the joins: int32 keys widened), whatever the output capacity (count reports them all)."""
+    rng = np.random.default_rng(12 + i32)
+    n = 1_500_000
+    if i32:
+        k = rng.integers(-2**31 + 1, 2**31 - 1, n).astype(np.int32)
+        k[rng.random(n) < 0.05] = abi.NULL_I32
+        t, wide = abi.T_I32N, k.astype(np.int64)
+        valid = k != abi.NULL_I32
+    else:
+        k = rng.integers(-2**62, 2**62, n).astype(np.int64)
+        k[rng.random(n) < 0.05] = abi.NULL_I64
+        t, wide = abi.T_I64N, k
+        valid = k != abi.NULL_I64
+    d = ops.DeviceBuffer.from_array(k)
+    tau = E.sample_tau(n, n, 1 << 14)
+    h = E.mix64(wide.view(np.uint64))
+    want = np.sort(h[valid & (h < np.uint64(tau))])
+    got = np.sort(E.key_sample(abi.ColView(d.ptr, t, 0, 0, 0), n, tau))
+    assert np.array_equal(got, want) and 10_000 < got.size < 20_000
+    # a capacity too small still counts every key
+    out = np.empty(16, dtype=np.uint64)
+    cnt = ctypes.c_int64()
+    ops.check(ops.lib().ws_join_key_sample(abi.ColView(d.ptr, t, 0, 0, 0), n, ctypes.c_uint64(tau), out.ctypes.data,
+                                           16, ctypes.byref(cnt)))
+    assert cnt.value == want.size and np.isin(out, want).all()

@@ -115,6 +115,7 @@ SIGNATURES = {
     "ws_encode_column": (C.c_int, [P, C.c_int, C.c_int64, C.c_int, C.POINTER(P), I64P, C.POINTER(C.c_int)]),
     "ws_hll_sketch": (C.c_int, [C.POINTER(abi.ExprEnv), C.c_int, C.POINTER(abi.AggPlan), C.c_int, P, P, P, C.c_int,
                                 C.c_int64, P, I64P, I64P]),
+    "ws_join_key_sample": (C.c_int, [abi.ColView, C.c_int64, C.c_uint64, P, C.c_int64, I64P]),
     "ws_mlp_infer": (C.c_int, [P, C.c_int, C.c_int, C.c_int, P, P, P, P, P, C.c_float, P]),
     "ws_serve": (C.c_int, [P, C.c_int, P, C.POINTER(C.c_double)]),
     "ws_tune_set_mode": (C.c_int, [C.c_int]),

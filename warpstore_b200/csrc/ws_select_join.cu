@@ -217,6 +217,28 @@ __global__ void kJoinStats(ws_col_view key, int64_t base, int64_t n, int bits, u
     if (h[i]) atomicAdd(&st[3 + i], h[i]);
 }
 
+// Coordinated key sample of a join side: the hash mix64(key) of every non-NULL key whose hash is below
+// tau, appended (in no order) to out[0, cap); *count receives every qualifying key, also those past cap.
+// Both sides sampled with one tau keep exactly the keys of both whose hash is below it, so the join of
+// the two samples holds every pair of those keys: a scaled estimate of the join's pairs.
+__global__ void kJoinKeySample(ws_col_view key, int64_t n, u64 tau, u64* out, int64_t cap, unsigned long long* count) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x; i0 < n; i0 += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = i0 + threadIdx.x;
+    long long k = 0;
+    const bool valid = i < n && joinKeyStream(key, i, k);
+    const u64 h = mix64((u64)k);
+    const bool take = valid && h < tau;
+    const unsigned m = __ballot_sync(0xffffffffu, take);
+    if (!m) continue;
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(count, (unsigned long long)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    const int64_t at = (int64_t)base + __popc(m & ((1u << lane) - 1u));
+    if (take && at < cap) out[at] = h;
+  }
+}
+
 // Inserts the pass's build rows of [base, base + n): CAS into the first empty slot of the key's bucket
 // or of the buckets after it.  The table has more slots than the pass's keys, so an insert meets an
 // empty slot within nbuckets steps; err is raised otherwise.  (Measured: giving each thread several
@@ -1029,6 +1051,27 @@ int ws_hash_join_outer(ws_col_view build_key, int64_t nb, ws_col_view probe_key,
   return guardedCall([&] {
     const int64_t bo[2] = {0, nb}, po[2] = {0, np};
     joinImpl(build_key, bo, 1, probe_key, po, 1, 1, full != 0, out_build, out_probe, nullptr, m);
+  });
+}
+
+int ws_join_key_sample(ws_col_view key, int64_t n, uint64_t tau, uint64_t* out, int64_t cap, int64_t* count) {
+  return guardedCall([&] {
+    *count = 0;
+    if (n < 0 || cap < 0) throw Error("join key sample: negative size", WS_ERR_ARG);
+    if (n == 0) return;
+    DBuf<unsigned long long> c(1);
+    DBuf<u64> d(std::max<int64_t>(cap, 1));
+    WS_CK(cudaMemsetAsync(c.p, 0, 8, stream()));
+    WS_LAUNCH(kJoinKeySample, gridFor(n), 256, 0, key, n, (u64)tau, d.p, cap, c.p);
+    unsigned long long hc = 0;
+    WS_CK(cudaMemcpyAsync(&hc, c.p, 8, cudaMemcpyDeviceToHost, stream()));
+    sync();
+    *count = (int64_t)hc;
+    const int64_t got = std::min<int64_t>((int64_t)hc, cap);
+    if (got) {
+      WS_CK(cudaMemcpyAsync(out, d.p, 8 * (size_t)got, cudaMemcpyDeviceToHost, stream()));
+      sync();
+    }
   });
 }
 

@@ -12,10 +12,12 @@ corrects a plain statistical estimate in the log2 domain:
   same sampled pass (without keys it only counts), plus zone maps -- each segment's min / max of the
   columns the filter compares with constants (``col < c``, ``col >= c``, ``col = c`` ...) bound and
   interpolate the fraction of rows that pass; the plain estimate is the sample's fraction scaled up.
-* ``pairs`` -- the pairs an inner equi-join emits, to size its pair buffers: HyperLogLog sketches of
-  the build and the probe keys (their registers' maximum sketches the union, so inclusion-exclusion
-  gives the shared distinct keys); the plain estimate is probe rows x containment x build rows per
-  distinct build key.
+* ``pairs`` -- the pairs an inner equi-join emits, to size its pair buffers: a coordinated sample of
+  both sides (every row whose key hash falls below one threshold, ~2^16 rows of the larger side) whose
+  join, scaled up, is the plain estimate; HyperLogLog sketches of the build and the probe keys (their
+  registers' maximum sketches the union, so inclusion-exclusion gives the shared distinct keys) add
+  probe rows x containment x build rows per distinct key, which stays informative where the sample
+  holds few pairs.
 
 Counts are compared in log2(1 + count) with a floor of 1024 (the smallest capacity any of them sizes).
 The correction is applied only where the MLP moves the estimate by more than a gate chosen on
@@ -234,20 +236,43 @@ def row_features(sampled: int, passing: int, total_rows: int, zones: tuple, opaq
 
 
 # ---------------------------------------------------------------- features: join output size
-def pair_features(build_regs: np.ndarray, probe_regs: np.ndarray, build_rows: int, probe_rows: int) -> np.ndarray:
-    """The join-size model's inputs, from full sketches of the build and probe keys; the last one is the
-    plain estimate: probe rows x the share of distinct probe keys that the build holds (inclusion-exclusion
-    over the union sketch) x build rows per distinct build key."""
+PAIR_SAMPLE_ROWS = 1 << 16  # rows of the larger side that the coordinated sample keeps
+
+
+def sample_tau(build_rows: int, probe_rows: int, rows: int = PAIR_SAMPLE_ROWS) -> int:
+    """The hash threshold of a coordinated sample that keeps about `rows` rows of the larger side."""
+    big = max(build_rows, probe_rows, 1)
+    return min((1 << 64) - 1, int(2.0 ** 64 * min(1.0, rows / big)))
+
+
+def sampled_pairs(build_h: np.ndarray, probe_h: np.ndarray) -> int:
+    """Pairs of the join of two coordinated samples (arrays of key hashes, one per row)."""
+    if build_h.size == 0 or probe_h.size == 0:
+        return 0
+    keys, counts = np.unique(build_h.astype(np.uint64), return_counts=True)
+    at = np.minimum(np.searchsorted(keys, probe_h.astype(np.uint64)), keys.size - 1)
+    hit = keys[at] == probe_h
+    return int(counts[at][hit].sum())
+
+
+def pair_features(build_regs: np.ndarray, probe_regs: np.ndarray, build_rows: int, probe_rows: int,
+                  sample_pairs: int, tau: int) -> np.ndarray:
+    """The join-size model's inputs, from full sketches of the build and probe keys and a coordinated
+    sample of both sides (every row whose key hash is below tau); the last one is the plain estimate,
+    the sample join's pairs scaled by 2^64 / tau.  The sketches give probe rows x the share of distinct
+    probe keys that the build holds (inclusion-exclusion over the union sketch) x build rows per
+    distinct build key, an estimate that stays informative where the sample holds few pairs."""
     db, dp = hll_estimate(build_regs), hll_estimate(probe_regs)
     du = hll_estimate(np.maximum(build_regs, probe_regs))
     inter = min(max(db + dp - du, 0.0), db, dp)
     contain = inter / max(dp, 1.0)
     mult = build_rows / max(db, 1.0)
     formula = probe_rows * contain * mult
+    scaled = sample_pairs * (2.0 ** 64 / max(tau, 1))
     return np.array([
         math.log2(1 + build_rows), math.log2(1 + probe_rows), math.log2(1 + db), math.log2(1 + dp),
         math.log2(1 + du), contain, math.log2(max(mult, 1.0)), db / max(du, 1.0), dp / max(du, 1.0),
-        math.log2(1 + formula)], dtype=np.float32)
+        math.log2(1 + formula), math.log2(1 + sample_pairs), math.log2(1 + scaled)], dtype=np.float32)
 
 
 # ---------------------------------------------------------------- model
@@ -399,10 +424,25 @@ def key_sketch(view, n: int, p: int = HLL_P) -> np.ndarray:
     return regs
 
 
+def key_sample(view, n: int, tau: int) -> np.ndarray:
+    """The coordinated sample of one join key column (a device ColView of n rows): the hashes below tau."""
+    from .ops import check, lib
+    cap = max(1024, int(n * (tau / 2.0 ** 64) * 1.5) + 1024)
+    while True:
+        out = np.empty(cap, dtype=np.uint64)
+        cnt = C.c_int64()
+        check(lib().ws_join_key_sample(view, n, C.c_uint64(tau), out.ctypes.data, cap, C.byref(cnt)))
+        if cnt.value <= cap:
+            return out[:cnt.value]
+        cap = cnt.value
+
+
 def estimate_pairs(build_view, nb: int, probe_view, np_: int) -> float:
-    """Predicted pairs of the inner equi-join of two key columns (device ColViews): sketches of both key
-    columns on the GPU and the join-size MLP on the GPU."""
-    x = pair_features(key_sketch(build_view, nb), key_sketch(probe_view, np_), nb, np_)
+    """Predicted pairs of the inner equi-join of two key columns (device ColViews): sketches and a
+    coordinated sample of both key columns on the GPU, the join-size MLP on the GPU."""
+    tau = sample_tau(nb, np_)
+    sp = sampled_pairs(key_sample(build_view, nb, tau), key_sample(probe_view, np_, tau))
+    x = pair_features(key_sketch(build_view, nb), key_sketch(probe_view, np_), nb, np_, sp, tau)
     return float(2.0 ** model("pairs").predict_log2_gpu(x)[0] - 1)
 
 

@@ -11,7 +11,8 @@ rows -- n rows (2^16 .. 2^23) in segments of 2^15 .. 2^18 rows, 1-3 columns each
   rows.  Label: log2(1 + rows that pass).
 pairs -- build 2^10 .. 2^22 rows with unique keys or 1-8 rows per key, probe 2^12 .. 2^23 rows of which
   a uniform share 0-100 % (uniform or Zipf over the build keys) matches and the rest holds keys absent
-  from the build; sketches of every key of both sides.  Label: log2(1 + the inner join's pairs).
+  from the build; sketches of every key of both sides and their coordinated sample.  Label: log2(1 +
+  the inner join's pairs).
 
 Each model: F -> 64 -> 64 -> 1, ReLU, predicting the correction to its plain estimate (the last
 feature), Adam on the squared log2 error, weights stored rounded to BF16.  Counts, labels and errors
@@ -151,9 +152,12 @@ def make_pairs_example(rng, max_log2_rows: float = 23):
     hit = pids < db
     truth = int(counts[pids[hit]].sum())
     base = np.uint64(rng.integers(1, 1 << 40))
-    breg = E.hll_registers(E.mix64(bids.astype(np.uint64) + base))
-    preg = E.hll_registers(E.mix64(pids.astype(np.uint64) + base))
-    return E.pair_features(breg, preg, nb, npr), math.log2(1 + truth), npr
+    bkeys, pkeys = E.mix64(bids.astype(np.uint64) + base), E.mix64(pids.astype(np.uint64) + base)
+    breg, preg = E.hll_registers(bkeys), E.hll_registers(pkeys)
+    tau = E.sample_tau(nb, npr)
+    bh, ph = E.mix64(bkeys), E.mix64(pkeys)  # the sampler's hash of each key, as the GPU computes it
+    sp = E.sampled_pairs(bh[bh < np.uint64(tau)], ph[ph < np.uint64(tau)])
+    return E.pair_features(breg, preg, nb, npr, sp, tau), math.log2(1 + truth), npr
 
 
 def train(xs, ys, hidden, epochs, seed, decay=1e-4):
