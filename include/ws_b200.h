@@ -203,7 +203,8 @@ int ws_agg_compact(ws_aggregator* agg, double** keys, double** accs, int64_t* ng
  * Limits: the batch descriptor (about nb * (ncols * 16 + 32) bytes, plus 9 KiB interpreted) must fit
  * 1 MiB, else WS_ERR_SIZE.  Every call shares the array and reinitialises it; calls that overlap on
  * the GPU race, so serialise them.  The first call on each device looks up the array's address (do
- * it before any stream capture). */
+ * it before any stream capture) and keeps it for the process: after a cudaDeviceReset of that device
+ * the address no longer holds, so the entry must not be called again. */
 #define WS_NOALLOC_SCRATCH_BYTES (4u << 20)
 int ws_agg_nokeys_noalloc(const ws_expr_env* env, int ncols, const ws_agg_plan* plan, const ws_jit_program* jit,
                           int nb, const int64_t* bn, const uint32_t* const* bdel, const ws_col_view* bcols,
