@@ -310,17 +310,20 @@ int ws_mlp_infer(const float* x, int rows, int features, int hidden, const uint1
 
 /* ---- launch-shape autotuner (no counterpart in the reference, whose launch shapes are fixed,
  * src/gpu.cu:393-653).  Per (scan kernel, plan, size class = log2 of the scan's tiles): the CTAs per
- * SM of the persistent grid and, for the hash scan, the per-CTA shared table's budget.  WS_TUNE_ON: a
- * key seen for the first time is tuned inside ws_agg_run on the query's own batches (each candidate
- * timed on the calling stream after resetting the result rows; the fastest is kept and the final run
- * uses it, so results never depend on tuning); WS_TUNE_USE (default): recorded choices are used,
- * others get the default shape; WS_TUNE_OFF: default shapes.  The table is kept in memory and in the
- * plan-cache directory (ws_jit_set_cache_dir).  Only fresh aggregators (no earlier window) tune. */
+ * SM of the persistent grid, for the hash scan the per-CTA shared table's budget, for compiled no-key
+ * and private-row scans the TMA staging depth; per (log2 build keys, log2 probe rows) of a hash join
+ * with one build and one probe partition and a one-pass table: its slots per build key (2, 3 or 4).
+ * WS_TUNE_ON: a key seen for the first time is tuned on the query's own data (each candidate timed on
+ * the calling stream from reset state; the fastest is kept and the final run uses it, so results never
+ * depend on tuning); WS_TUNE_USE (default): recorded choices are used, others get the default shape;
+ * WS_TUNE_OFF: default shapes.  The table is kept in memory and in the plan-cache directory
+ * (ws_jit_set_cache_dir).  Only fresh aggregators (no earlier window) tune. */
 #define WS_TUNE_USE 0
 #define WS_TUNE_ON 1
 #define WS_TUNE_OFF 2
 int ws_tune_set_mode(int mode);
-/* The table as text, one line per key: `key ctas_per_sm smem_kb microseconds`. */
+/* The table as text, one line per key: `key ctas_per_sm smem_kb stages join_slots_per_key microseconds`
+ * (ws_tune_load also reads lines without the stages and slots fields). */
 int ws_tune_table(char* buf, size_t size, size_t* needed);
 int ws_tune_load(const char* text);   /* adds / replaces entries from such text */
 int ws_tune_clear(void);

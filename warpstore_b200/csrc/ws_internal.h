@@ -66,6 +66,7 @@ struct TuneChoice {
   int ctasPerSm = 0;
   int smemKB = 0;
   int stages = -1;  // shared-memory tile stages of a compiled scan (0: direct loads; -1: the default)
+  int slotsPerKey = 0;  // a hash join's table slots per build key (0: the default)
   bool found = false;
 };
 int tuneMode();  // WS_TUNE_USE / WS_TUNE_ON / WS_TUNE_OFF

@@ -552,17 +552,17 @@ int64_t joinTableBudget() {
 
 
 
-// Hash join table slots for `keys` build keys: 2 per key (load 1/2: a bucket of 4 is full for about
-// 1 key in 7), a multiple of the 4-slot bucket with at least one spare bucket;
-// WARPSTORE_B200_JOIN_SLOTS_PER_KEY = 2..16 fixes the factor.
+// Hash join table slots for `keys` build keys: perKey per key (default 2: load 1/2, a bucket of 4 is
+// full for about 1 key in 7; the tuner may choose another), a multiple of the 4-slot bucket with at
+// least one spare bucket; WARPSTORE_B200_JOIN_SLOTS_PER_KEY = 2..16 fixes the factor.
 constexpr int64_t kJSlotBytes = 16;  // a 64-byte bucket of 4 slots
-int64_t joinTableSlots(int64_t keys) {
+int64_t joinTableSlots(int64_t keys, int perKey = 0) {
   static const int64_t fixed = [] {
     const char* e = getenv("WARPSTORE_B200_JOIN_SLOTS_PER_KEY");
     const long long v = e ? atoll(e) : 0;
     return v >= 2 && v <= 16 ? (int64_t)v : (int64_t)0;
   }();
-  const int64_t per = fixed ? fixed : 2;
+  const int64_t per = fixed ? fixed : perKey >= 2 ? perKey : 2;
   return ((per * keys + 3) / 4 + 1) * 4;
 }
 
@@ -794,6 +794,67 @@ __global__ void kCross(int64_t na, int64_t nb, int32_t* oa, int32_t* ob) {
 
 }  // namespace
 
+// The autotuner's choice of slots per build key for a one-pass hash join of one build and one probe
+// partition (keys: non-NULL build keys): the recorded one, or in tuning mode the fastest of 2, 3 and 4,
+// each timed (best of two) building its table and probing every row into scratch pair buffers.
+// 0: the default.
+static int joinSlotsChoice(ws_col_view build_key, int64_t nb, ws_col_view probe_key, int64_t np, int64_t keys) {
+  int lb = 0, lp = 0;
+  while (lb < 62 && ((int64_t)1 << (lb + 1)) <= keys) ++lb;
+  while (lp < 62 && ((int64_t)1 << (lp + 1)) <= np) ++lp;
+  const std::string key = "join:b" + std::to_string(lb) + ":p" + std::to_string(lp);
+  TuneChoice c;
+  if (tuneLookup(key, c)) return c.slotsPerKey;
+  if (tuneMode() != WS_TUNE_ON || np > INT32_MAX) return 0;
+  const int64_t maxC = joinTableSlots(keys, 4);
+  DBuf<u64> table(maxC / 4 * kJBucketWords);
+  DBuf<int> flags(1);
+  DBuf<int32_t> ob(std::max<int64_t>(np, 1)), op(std::max<int64_t>(np, 1));
+  DBuf<unsigned long long> ctr(1);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  WS_CK(cudaEventCreate(&e0));
+  WS_CK(cudaEventCreate(&e1));
+  int best = 0;
+  double bestMs = 1e300;
+  try {
+    for (int per : {2, 3, 4}) {
+      const int64_t cs = joinTableSlots(keys, per);
+      double ms = 1e300;
+      int full = 0;
+      for (int rep = 0; rep < 2; ++rep) {
+        WS_CK(cudaEventRecord(e0, stream()));
+        WS_CK(cudaMemsetAsync(table.p, 0, 8 * kJBucketWords * (cs / 4), stream()));
+        WS_CK(cudaMemsetAsync(flags.p, 0, 4, stream()));
+        WS_CK(cudaMemsetAsync(ctr.p, 0, 8, stream()));
+        WS_LAUNCH(kJoinBuild, gridFor(nb), 256, 0, build_key, (int64_t)0, nb, JPass{0, 0}, table.p,
+                  (int*)(table.p + 4), (u64)(cs / 4), flags.p, JFilter{nullptr, 0});
+        const JOut jo{ob.p, op.p, 0, np, ctr.p, 0, nullptr, 0};
+        WS_LAUNCH(kJoinProbe, gridFor((np + kJHashPer - 1) / kJHashPer, kJThreads), kJThreads, 0, probe_key,
+                  (int64_t)0, np, JPass{0, 0}, table.p, (const int*)(table.p + 4), (u64)(cs / 4), jo,
+                  JFilter{nullptr, 0});
+        WS_CK(cudaEventRecord(e1, stream()));
+        WS_CK(cudaEventSynchronize(e1));
+        float t = 0;
+        WS_CK(cudaEventElapsedTime(&t, e0, e1));
+        ms = std::min(ms, (double)t);
+      }
+      d2hSync(&full, flags.p, 4);
+      if (!full && ms < bestMs) bestMs = ms, best = per;
+    }
+  } catch (...) {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (!best) return 0;
+  TuneChoice t;
+  t.slotsPerKey = best;
+  tuneStore(key, t, bestMs * 1000);
+  return best;
+}
+
 // Inner (outer = 0) or outer equi join over build / probe partitions; see ws_hash_join_parts and
 // ws_hash_join_outer.  full: also the build rows that matched nothing, paired with probe row -1.
 // firstCap > 0 (an inner join of one partition): the pair buffers' capacity of the first attempt
@@ -867,6 +928,14 @@ static int joinImpl(ws_col_view build_key, const int64_t* boff, int pb, ws_col_v
         const int64_t c = joinTableSlots(bits[q] ? (int64_t)st[3 + p] : keys);
         cap[q].push_back(c);
         tableSlots = std::max(tableSlots, c);
+      }
+    }
+    // the tuner's table size for a one-pass hash join of one partition a side
+    if (pb == 1 && pp == 1 && boff[0] == 0 && poff[0] == 0 && !dense[0] && cap[0].size() == 1 && !bits[0]) {
+      const int per = joinSlotsChoice(build_key, nb, probe_key, np, (int64_t)hs[0]);
+      if (per) {
+        cap[0][0] = joinTableSlots((int64_t)hs[0], per);
+        tableSlots = std::max(tableSlots, cap[0][0]);
       }
     }
     bool anyDense = false, anyHash = false;

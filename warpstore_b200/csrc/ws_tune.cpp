@@ -3,12 +3,14 @@
 // interpreter: of the plan's shape), the size class log2 of the scan's tiles.  A choice is the CTAs
 // per SM of the persistent grid (0: as many as fit), for the hash scan the shared-memory budget of the
 // per-CTA table in KB (0: the default), and for compiled no-key and private-row scans the depth of the
-// TMA tile staging (0: direct loads, 2..4 stages, -1: the default).  In tuning mode a key seen for the
-// first time is tuned on the query's own batches (aggRun in ws_ops.cu times each candidate and keeps
-// the fastest); the table lives in memory and, once a plan-cache directory is set, in
-// <dir>/wsb200_tune.txt (one line per key: `key ctas smem_kb stages microseconds`; lines without the
-// stages field are read with the default), read back when the directory is set.  No counterpart in the
-// reference, whose launch shapes are fixed (src/gpu.cu:393-653).
+// TMA tile staging (0: direct loads, 2..4 stages, -1: the default); for a hash join (keys `join:b<log2
+// build keys>:p<log2 probe rows>`) the table's slots per build key (0: the default).  In tuning mode a
+// key seen for the first time is tuned on the query's own data (aggRun in ws_ops.cu and joinImpl in
+// ws_select_join.cu time each candidate and keep the fastest); the table lives in memory and, once a
+// plan-cache directory is set, in <dir>/wsb200_tune.txt (one line per key: `key ctas smem_kb stages
+// slots microseconds`; lines without the last fields are read with the defaults), read back when the
+// directory is set.  No counterpart in the reference, whose launch shapes are fixed
+// (src/gpu.cu:393-653).
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -45,21 +47,24 @@ bool parseLine(const std::string& line, std::string& key, Entry& e) {
   std::vector<double> v;
   double x;
   while (in >> x) v.push_back(x);
-  if (!in.eof() || (v.size() != 3 && v.size() != 4)) return false;
-  const int ctas = (int)v[0], smem = (int)v[1], stages = v.size() == 4 ? (int)v[2] : -1;
+  if (!in.eof() || v.size() < 3 || v.size() > 5) return false;
+  const int ctas = (int)v[0], smem = (int)v[1], stages = v.size() >= 4 ? (int)v[2] : -1;
+  const int slots = v.size() == 5 ? (int)v[3] : 0;
   if (v[0] != ctas || v[1] != smem || ctas < 0 || ctas > 64 || smem < 0 || smem > 228) return false;
   if (stages != -1 && stages != 0 && (stages < 2 || stages > 4)) return false;
+  if (slots != 0 && (slots < 2 || slots > 16)) return false;
   e.c.ctasPerSm = ctas;
   e.c.smemKB = smem;
   e.c.stages = stages;
+  e.c.slotsPerKey = slots;
   e.c.found = true;
   e.us = v.back();
   return true;
 }
 
 std::string formatLine(const std::string& key, const Entry& e) {
-  char b[80];
-  std::snprintf(b, sizeof(b), " %d %d %d %.1f\n", e.c.ctasPerSm, e.c.smemKB, e.c.stages, e.us);
+  char b[96];
+  std::snprintf(b, sizeof(b), " %d %d %d %d %.1f\n", e.c.ctasPerSm, e.c.smemKB, e.c.stages, e.c.slotsPerKey, e.us);
   return key + b;
 }
 

@@ -85,16 +85,16 @@ def tune_set_mode(mode: int):
 
 
 def tune_table() -> dict:
-    """{key: (ctas per SM, shared KB, tile stages, microseconds)} of the autotuner's table (stages -1:
-    the default)."""
+    """{key: (ctas per SM, shared KB, tile stages, join slots per key, microseconds)} of the autotuner's
+    table (stages -1 and slots 0: the defaults)."""
     need = C.c_size_t()
     lib().ws_tune_table(None, 0, C.byref(need))
     buf = C.create_string_buffer(need.value)
     check(lib().ws_tune_table(buf, need.value, C.byref(need)))
     out = {}
     for line in buf.value.decode().splitlines():
-        k, c, m, st, us = line.split()
-        out[k] = (int(c), int(m), int(st), float(us))
+        k, c, m, st, sl, us = line.split()
+        out[k] = (int(c), int(m), int(st), int(sl), float(us))
     return out
 
 
