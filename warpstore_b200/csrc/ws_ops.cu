@@ -87,10 +87,6 @@ __global__ void kScanExclusive(int64_t* counts, int64_t n) {
   if (t == T - 1) counts[n] = part[T - 1];
 }
 
-__global__ void kGatherI64(const int64_t* src, const int64_t* idx, int n, int64_t* dst) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = src[idx[i]];
-}
-
 // Occupied result rows: hash rows [0, cap) by their key word, the extra row (cap) by its claim flag,
 // dense rows by slot 0 (COUNT(*)) being non-zero.
 struct OccSpec {
