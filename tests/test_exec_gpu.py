@@ -263,3 +263,32 @@ def test_group_of_prepared_queries_equals_each_alone(kind):
         ops.jit_set_mode(-1)
         for t in tables:
             t.free_device()
+
+
+def test_group_refuses_mixed_plans_and_kinds(fg):
+    """A group needs one compiled plan and one scan kind with a multi-query form: executors of two
+    plans (hash and no-key) are refused before anything is captured, as is an executor given twice."""
+    e, aq = W.filter_groupby_1m_query(fg)
+    ops.jit_set_mode(abi.JIT_SYNC)
+    exs = []
+    try:
+        arrays = E.batch_arrays(fg.batches(True))
+        prog = ops.jit_get(e.env, e.ncols, aq.plan, abi.JF_GROUPED, "exec group")
+        exs.append(ops.Executor(aq.plan, 1024, None, e.env, e.ncols, arrays, prog, 64))
+        e2 = W.env_for(fg)
+        aq2 = q.AggQuery(e2, None, [], [q.Agg("COUNT")])
+        prog2 = ops.jit_get(e2.env, e2.ncols, aq2.plan, abi.JF_NOKEYS, "exec group")
+        exs.append(ops.Executor(aq2.plan, 1, None, e2.env, e2.ncols, arrays, prog2, 1))
+        for members in ([exs[0], exs[1]], [exs[0], exs[0]]):
+            with pytest.raises(ops.WsError) as ei:
+                ops.ExecGroup(members, prog)
+            assert ei.value.code == 1210
+        # the executors still run on their own
+        exs[0].run(e.env)
+        ops.sync()
+        _, _, st = exs[0].results()
+        assert st["error"] == 0 and st["groups"] > 0
+    finally:
+        for x in exs:
+            x.close()
+        ops.jit_set_mode(-1)
